@@ -1,0 +1,878 @@
+// gsc_api.cu -- the C ABI (include/gsc_b200.h) over the sm_100a kernels.
+//
+// Host-side work mirrors run_case_cuda_u32 (cuda/kernels.cu:492-875), split
+// into device-resident stages.  The only host arithmetic on the successor-box
+// path is the tabulation of cos/sin along theta trajectories and of the
+// theta / v trajectories themselves (model.hpp:26-46), done with the C
+// library the reference calls, in its operation order.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/gsc_b200.h"
+#include "gsc_kernels.cuh"
+
+using namespace gsc_b200;
+
+struct gsc_context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::string last_error;
+    uint64_t budget = 0;
+    uint64_t in_use = 0;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+};
+
+struct gsc_abstraction {
+    gsc_context* ctx = nullptr;
+    GridInfo g{};
+    gsc_model_desc model{};
+    double* xn = nullptr;
+    double* yn = nullptr;
+    double* thf = nullptr;
+    double* vf = nullptr;
+    uint64_t bytes = 0;
+    double build_ms = 0.0;
+};
+
+struct gsc_problem {
+    gsc_context* ctx = nullptr;
+    const gsc_abstraction* abs = nullptr;
+    GridInfo g{};
+    QueryInfo q{};
+    uint32_t method = 0;
+    std::vector<void*> allocs;
+    uint64_t bytes = 0;
+    // masks and tables
+    uint8_t* valid = nullptr;
+    uint8_t* cand = nullptr;
+    uint8_t* safe = nullptr;
+    int safe_rank = 0;
+    double* obstacles = nullptr;
+    unsigned long long* counts = nullptr;   // [0] valid [1] cand [2] cand-not-valid [3] valid pairs [4] valid!=safe
+    unsigned int* flags = nullptr;
+    uint32_t *xt = nullptr, *yt = nullptr, *zt = nullptr, *wt = nullptr;
+    int32_t* unsafe2 = nullptr;
+    int32_t* unsafe4 = nullptr;
+    int32_t* pvalid = nullptr;
+    // stored
+    uint2* boxes = nullptr;
+    uint64_t S_pad = 0;
+    int32_t* pd = nullptr;
+    uint8_t* reach8 = nullptr;
+    // fused
+    uint64_t *validb = nullptr, *unsafeb = nullptr, *srcb = nullptr, *candb = nullptr, *dp = nullptr;
+    uint64_t *reach0 = nullptr, *reach1 = nullptr, *active = nullptr;
+    int need_valid = 0;
+    // common fixpoint state
+    uint32_t* controller = nullptr;
+    uint32_t* reach_step = nullptr;
+    FixControl* fc = nullptr;
+    unsigned long long* stats = nullptr;
+    uint32_t stats_cap = 0;
+    uint64_t valid_count = 0, candidate_count = 0, valid_pairs = 0;
+    // graph
+    cudaGraphExec_t exec = nullptr;
+    cudaGraph_t graph = nullptr;
+    gsc_timings timings{};
+    ~gsc_problem();
+};
+
+namespace {
+
+constexpr uint32_t kStatsCapMax = 1u << 20;
+
+struct Fail {
+    int status;
+};
+
+int fail(gsc_context* ctx, int status, const std::string& msg) {
+    if (ctx) ctx->last_error = msg;
+    return status;
+}
+
+#define GSC_CU(ctx, expr)                                                                              \
+    do {                                                                                               \
+        cudaError_t e__ = (expr);                                                                      \
+        if (e__ != cudaSuccess) {                                                                      \
+            return fail((ctx), e__ == cudaErrorMemoryAllocation ? GSC_ERR_OUT_OF_MEMORY : GSC_ERR_CUDA, \
+                        std::string(#expr) + ": " + cudaGetErrorString(e__));                          \
+        }                                                                                              \
+    } while (0)
+
+// Reference wrap_angle (model.hpp:14-24).
+double wrap_angle(double x) {
+    constexpr double kPi = 3.14159265358979323846;
+    constexpr double kTwoPi = 2.0 * kPi;
+    while (x < -kPi) x += kTwoPi;
+    while (x >= kPi) x -= kTwoPi;
+    return x;
+}
+
+int grid_from_model(const gsc_model_desc* m, GridInfo* g, std::string* err) {
+    std::memset(g, 0, sizeof(*g));
+    uint64_t total = 1;
+    for (int d = 0; d < 4; ++d) {
+        if (!(m->state_eta[d] > 0.0)) {
+            *err = "state eta must be positive";
+            return GSC_ERR_INVALID_ARGUMENT;
+        }
+        const double width = m->state_ub[d] - m->state_lb[d];
+        if (!(width > 0.0)) {
+            *err = "state bounds must satisfy ub > lb";
+            return GSC_ERR_INVALID_ARGUMENT;
+        }
+        const double n = std::ceil(width / m->state_eta[d]);
+        if (!(n >= 1.0) || n > 65535.0) {
+            *err = "state grid dimension out of range (1..65535 cells)";
+            return GSC_ERR_UNSUPPORTED;
+        }
+        g->n[d] = static_cast<uint32_t>(n);
+        g->lb[d] = m->state_lb[d];
+        g->ub[d] = m->state_ub[d];
+        g->eta[d] = m->state_eta[d];
+        total *= g->n[d];
+    }
+    if (total > 0xFFFFFFFFull) {
+        *err = "state grid exceeds the selected state index type";
+        return GSC_ERR_UNSUPPORTED;
+    }
+    uint32_t ni[2];
+    for (int d = 0; d < 2; ++d) {
+        if (!(m->input_eta[d] > 0.0)) {
+            *err = "input eta must be positive";
+            return GSC_ERR_INVALID_ARGUMENT;
+        }
+        const double width = m->input_ub[d] - m->input_lb[d];
+        if (!(width > 0.0)) {
+            *err = "input bounds must satisfy ub > lb";
+            return GSC_ERR_INVALID_ARGUMENT;
+        }
+        const double n = std::ceil(width / m->input_eta[d]);
+        if (!(n >= 1.0) || n > 65535.0) {
+            *err = "input grid dimension out of range";
+            return GSC_ERR_UNSUPPORTED;
+        }
+        ni[d] = static_cast<uint32_t>(n);
+        g->ilb[d] = m->input_lb[d];
+        g->ieta[d] = m->input_eta[d];
+    }
+    if (m->wrap_dim != 2) {
+        *err = "only wrap_dim = 2 (theta) is supported";
+        return GSC_ERR_UNSUPPORTED;
+    }
+    if (m->integration_substeps == 0) {
+        *err = "integration_substeps must be positive";
+        return GSC_ERR_INVALID_ARGUMENT;
+    }
+    g->ma = ni[0];
+    g->mw = ni[1];
+    g->M = ni[0] * ni[1];
+    g->T = m->sample_time;
+    g->K = m->integration_substeps;
+    g->dt = m->sample_time / static_cast<double>(m->integration_substeps);
+    g->S = total;
+    g->ps[0] = 1;
+    for (int d = 1; d < 4; ++d) g->ps[d] = g->ps[d - 1] * (g->n[d - 1] + 1);
+    g->tsize = static_cast<uint64_t>(g->ps[3]) * (g->n[3] + 1);
+    if (g->tsize >= 0x7FFFFFFFull) {
+        *err = "padded prefix table exceeds int32 indexing";
+        return GSC_ERR_UNSUPPORTED;
+    }
+    g->W = (g->n[0] + 63) / 64;
+    g->rows = static_cast<uint64_t>(g->n[1]) * g->n[2] * g->n[3];
+    g->slices = g->n[2] * g->n[3];
+    return GSC_OK;
+}
+
+template <typename T>
+int dalloc(gsc_context* ctx, std::vector<void*>& allocs, uint64_t& bytes, T** p, uint64_t count) {
+    const uint64_t nbytes = count * sizeof(T);
+    if (ctx->budget && ctx->in_use + nbytes > ctx->budget)
+        return fail(ctx, GSC_ERR_OUT_OF_MEMORY, "device memory budget exceeded");
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, nbytes ? nbytes : 1);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(ctx, GSC_ERR_OUT_OF_MEMORY, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    }
+    allocs.push_back(q);
+    bytes += nbytes;
+    ctx->in_use += nbytes;
+    *p = static_cast<T*>(q);
+    return GSC_OK;
+}
+
+#define GSC_TRY(expr)              \
+    do {                           \
+        int s__ = (expr);          \
+        if (s__ != GSC_OK) return s__; \
+    } while (0)
+
+}  // namespace
+
+gsc_problem::~gsc_problem() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    for (void* p : allocs) cudaFree(p);
+    if (ctx) ctx->in_use -= bytes;
+}
+
+extern "C" {
+
+int gsc_cuda_backend_compiled(void) { return 1; }
+
+int gsc_abi_version(void) { return GSC_B200_ABI_VERSION; }
+
+const char* gsc_status_string(int status) {
+    switch (status) {
+        case GSC_OK: return "ok";
+        case GSC_ERR_INVALID_ARGUMENT: return "invalid argument";
+        case GSC_ERR_CUDA: return "CUDA error";
+        case GSC_ERR_OUT_OF_MEMORY: return "out of device memory";
+        case GSC_ERR_UNSUPPORTED: return "unsupported";
+        case GSC_ERR_NO_DEVICE: return "no CUDA device found";
+        case GSC_ERR_CANDIDATE_INVALID: return "candidate set contains invalid states";
+        case GSC_ERR_TIMEOUT: return "device wait timed out";
+        default: return "unknown status";
+    }
+}
+
+const char* gsc_message_string(int message) {
+    switch (message) {
+        case GSC_MSG_CONVERGED: return "all candidate states obtained a controller";
+        case GSC_MSG_STALLED: return "iteration stalled before candidate closure";
+        case GSC_MSG_MAX_ITERATIONS: return "maximum iterations reached";
+        default: return "";
+    }
+}
+
+int gsc_grid_shape(const gsc_model_desc* model, uint32_t shape[4], uint32_t input_shape[2]) {
+    if (!model || !shape || !input_shape) return GSC_ERR_INVALID_ARGUMENT;
+    GridInfo g;
+    std::string err;
+    const int s = grid_from_model(model, &g, &err);
+    if (s != GSC_OK) return s;
+    for (int d = 0; d < 4; ++d) shape[d] = g.n[d];
+    input_shape[0] = g.ma;
+    input_shape[1] = g.mw;
+    return GSC_OK;
+}
+
+int gsc_context_create(int device, void* cuda_stream, gsc_context** out) {
+    if (!out) return GSC_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count <= 0) {
+        cudaGetLastError();
+        return GSC_ERR_NO_DEVICE;
+    }
+    if (device < 0 || device >= count) return GSC_ERR_INVALID_ARGUMENT;
+    if (cudaSetDevice(device) != cudaSuccess) return GSC_ERR_CUDA;
+    gsc_context* ctx = new (std::nothrow) gsc_context();
+    if (!ctx) return GSC_ERR_OUT_OF_MEMORY;
+    ctx->device = device;
+    if (cuda_stream) {
+        ctx->stream = static_cast<cudaStream_t>(cuda_stream);
+    } else {
+        if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+            delete ctx;
+            return GSC_ERR_CUDA;
+        }
+        ctx->own_stream = true;
+    }
+    if (cudaEventCreate(&ctx->ev[0]) != cudaSuccess || cudaEventCreate(&ctx->ev[1]) != cudaSuccess) {
+        if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
+        delete ctx;
+        return GSC_ERR_CUDA;
+    }
+    *out = ctx;
+    return GSC_OK;
+}
+
+void gsc_context_destroy(gsc_context* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->ev[0]) cudaEventDestroy(ctx->ev[0]);
+    if (ctx->ev[1]) cudaEventDestroy(ctx->ev[1]);
+    if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+const char* gsc_last_error(const gsc_context* ctx) { return ctx ? ctx->last_error.c_str() : ""; }
+
+int gsc_context_set_memory_budget(gsc_context* ctx, uint64_t bytes) {
+    if (!ctx) return GSC_ERR_INVALID_ARGUMENT;
+    ctx->budget = bytes;
+    return GSC_OK;
+}
+
+uint64_t gsc_context_memory_in_use(const gsc_context* ctx) { return ctx ? ctx->in_use : 0; }
+
+int gsc_abstraction_create(gsc_context* ctx, const gsc_model_desc* model, gsc_abstraction** out) {
+    if (!ctx || !model || !out) return GSC_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    GSC_CU(ctx, cudaSetDevice(ctx->device));
+    std::unique_ptr<gsc_abstraction> a(new (std::nothrow) gsc_abstraction());
+    if (!a) return GSC_ERR_OUT_OF_MEMORY;
+    a->ctx = ctx;
+    a->model = *model;
+    std::string err;
+    const int s = grid_from_model(model, &a->g, &err);
+    if (s != GSC_OK) return fail(ctx, s, err);
+    const GridInfo& g = a->g;
+    const uint32_t K = g.K;
+
+    // Host tabulation of the theta and v trajectories (model.hpp:34-45).
+    std::vector<double> cosT(static_cast<size_t>(g.n[2]) * g.mw * K), sinT(cosT.size());
+    std::vector<double> thf(static_cast<size_t>(g.n[2]) * g.mw), vf(static_cast<size_t>(g.n[3]) * g.ma);
+    std::vector<double> vseq(static_cast<size_t>(g.n[3]) * g.ma * K);
+    for (uint32_t i2 = 0; i2 < g.n[2]; ++i2) {
+        for (uint32_t jw = 0; jw < g.mw; ++jw) {
+            double th = g.lb[2] + (static_cast<double>(i2) + 0.5) * g.eta[2];
+            const double omega = g.ilb[1] + (static_cast<double>(jw) + 0.5) * g.ieta[1];
+            const size_t base = (static_cast<size_t>(i2) * g.mw + jw) * K;
+            for (uint32_t k = 0; k < K; ++k) {
+                cosT[base + k] = std::cos(th);
+                sinT[base + k] = std::sin(th);
+                th = wrap_angle(th + g.dt * omega);
+            }
+            thf[static_cast<size_t>(i2) * g.mw + jw] = th;
+        }
+    }
+    for (uint32_t i3 = 0; i3 < g.n[3]; ++i3) {
+        for (uint32_t ja = 0; ja < g.ma; ++ja) {
+            double v = g.lb[3] + (static_cast<double>(i3) + 0.5) * g.eta[3];
+            const double acc = g.ilb[0] + (static_cast<double>(ja) + 0.5) * g.ieta[0];
+            const size_t base = (static_cast<size_t>(i3) * g.ma + ja) * K;
+            for (uint32_t k = 0; k < K; ++k) {
+                vseq[base + k] = v;
+                v += g.dt * acc;
+            }
+            vf[static_cast<size_t>(i3) * g.ma + ja] = v;
+        }
+    }
+    std::vector<void*> allocs;
+    uint64_t bytes = 0;
+    const uint64_t planes = static_cast<uint64_t>(g.slices) * g.M;
+    double *d_cos = nullptr, *d_sin = nullptr, *d_vseq = nullptr;
+    auto cleanup_tmp = [&]() {
+        cudaFree(d_cos);
+        cudaFree(d_sin);
+        cudaFree(d_vseq);
+    };
+    int st = dalloc(ctx, allocs, bytes, &a->xn, planes * g.n[0]);
+    if (st == GSC_OK) st = dalloc(ctx, allocs, bytes, &a->yn, planes * g.n[1]);
+    if (st == GSC_OK) st = dalloc(ctx, allocs, bytes, &a->thf, thf.size());
+    if (st == GSC_OK) st = dalloc(ctx, allocs, bytes, &a->vf, vf.size());
+    if (st != GSC_OK) {
+        for (void* p : allocs) cudaFree(p);
+        ctx->in_use -= bytes;
+        return st;
+    }
+    a->bytes = bytes;
+    cudaError_t e = cudaMalloc(&d_cos, cosT.size() * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&d_sin, sinT.size() * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&d_vseq, vseq.size() * sizeof(double));
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_cos, cosT.data(), cosT.size() * 8, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_sin, sinT.data(), sinT.size() * 8, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_vseq, vseq.data(), vseq.size() * 8, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(a->thf, thf.data(), thf.size() * 8, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(a->vf, vf.data(), vf.size() * 8, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(ctx->ev[0], ctx->stream);
+    if (e == cudaSuccess) e = launch_nominal_xy(g, d_cos, d_sin, d_vseq, a->xn, a->yn, ctx->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(ctx->ev[1], ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    float ms = 0.f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);
+    cleanup_tmp();
+    if (e != cudaSuccess) {
+        for (void* p : allocs) cudaFree(p);
+        ctx->in_use -= bytes;
+        return fail(ctx, e == cudaErrorMemoryAllocation ? GSC_ERR_OUT_OF_MEMORY : GSC_ERR_CUDA,
+                    std::string("abstraction: ") + cudaGetErrorString(e));
+    }
+    a->build_ms = ms;
+    *out = a.release();
+    return GSC_OK;
+}
+
+void gsc_abstraction_destroy(gsc_abstraction* a) {
+    if (!a) return;
+    cudaSetDevice(a->ctx->device);
+    cudaFree(a->xn);
+    cudaFree(a->yn);
+    cudaFree(a->thf);
+    cudaFree(a->vf);
+    a->ctx->in_use -= a->bytes;
+    delete a;
+}
+
+}  // extern "C"
+
+namespace {
+
+int build_problem(gsc_problem* p, const gsc_query_desc* qd, uint32_t method) {
+    gsc_context* ctx = p->ctx;
+    const GridInfo& g = p->g;
+    cudaStream_t st = ctx->stream;
+    auto& A = p->allocs;
+    auto& B = p->bytes;
+    QueryInfo& q = p->q;
+    std::memset(&q, 0, sizeof(q));
+    for (int d = 0; d < 4; ++d) {
+        q.dhw[d] = qd->disturbance_half_width[d];
+        q.cp[d] = qd->constraint_params[d];
+        q.map_lb[d] = qd->map_lb[d];
+        q.map_ub[d] = qd->map_ub[d];
+    }
+    if (qd->constraint_kind < 0 || qd->constraint_kind > 3)
+        return fail(ctx, GSC_ERR_INVALID_ARGUMENT, "unknown constraint kind");
+    if (qd->candidate_kind < 0 || qd->candidate_kind > 1)
+        return fail(ctx, GSC_ERR_INVALID_ARGUMENT, "unknown candidate kind");
+    if (qd->obstacle_count > 0 && !qd->obstacles) return fail(ctx, GSC_ERR_INVALID_ARGUMENT, "obstacles pointer");
+    if (qd->safe_mask && qd->safe_mask_rank != 2 && qd->safe_mask_rank != 4)
+        return fail(ctx, GSC_ERR_INVALID_ARGUMENT, "safe_mask_rank must be 2 or 4");
+    q.ckind = qd->constraint_kind;
+    q.n_obstacles = static_cast<int32_t>(qd->obstacle_count);
+    q.cand_kind = qd->candidate_kind;
+    for (int i = 0; i < 8; ++i) q.cand[i] = qd->candidate[i];
+    q.max_iterations = qd->max_iterations;
+
+    // Method selection.
+    bool stored_ok = g.n[0] <= 255 && g.n[1] <= 255 && g.n[2] <= 255 && g.n[3] <= 255;
+    bool fused_ok = g.n[0] <= 64 * kMaxWords;
+    if (method == GSC_METHOD_STORED && !stored_ok)
+        return fail(ctx, GSC_ERR_UNSUPPORTED, "stored method needs at most 255 cells per dimension");
+    if (method == GSC_METHOD_FUSED && !fused_ok)
+        return fail(ctx, GSC_ERR_UNSUPPORTED, "fused method needs at most 256 cells along x");
+    if (method > GSC_METHOD_FUSED) return fail(ctx, GSC_ERR_INVALID_ARGUMENT, "unknown method");
+
+    // Masks.
+    GSC_TRY(dalloc(ctx, A, B, &p->valid, g.S));
+    GSC_TRY(dalloc(ctx, A, B, &p->cand, g.S));
+    GSC_TRY(dalloc(ctx, A, B, &p->counts, 8));
+    GSC_TRY(dalloc(ctx, A, B, &p->flags, 1));
+    GSC_CU(ctx, cudaMemsetAsync(p->counts, 0, 8 * sizeof(unsigned long long), st));
+    GSC_CU(ctx, cudaMemsetAsync(p->flags, 0, sizeof(unsigned int), st));
+    if (qd->obstacle_count) {
+        GSC_TRY(dalloc(ctx, A, B, &p->obstacles, 8ull * qd->obstacle_count));
+        GSC_CU(ctx, cudaMemcpyAsync(p->obstacles, qd->obstacles, 64ull * qd->obstacle_count, cudaMemcpyHostToDevice, st));
+    }
+    if (qd->valid_mask) GSC_CU(ctx, cudaMemcpyAsync(p->valid, qd->valid_mask, g.S, cudaMemcpyHostToDevice, st));
+    if (qd->candidate_mask) GSC_CU(ctx, cudaMemcpyAsync(p->cand, qd->candidate_mask, g.S, cudaMemcpyHostToDevice, st));
+    if (qd->safe_mask) {
+        p->safe_rank = qd->safe_mask_rank;
+        const uint64_t n = (p->safe_rank == 4) ? g.S : static_cast<uint64_t>(g.n[0]) * g.n[1];
+        GSC_TRY(dalloc(ctx, A, B, &p->safe, n));
+        GSC_CU(ctx, cudaMemcpyAsync(p->safe, qd->safe_mask, n, cudaMemcpyHostToDevice, st));
+    } else if (q.ckind != GSC_CONSTRAINT_NONE) {
+        p->safe_rank = 2;
+        GSC_TRY(dalloc(ctx, A, B, &p->safe, static_cast<uint64_t>(g.n[0]) * g.n[1]));
+        GSC_CU(ctx, launch_safe2(g, q, p->safe, st));
+    }
+    MaskArgs ma{};
+    ma.obstacles = p->obstacles;
+    ma.valid = p->valid;
+    ma.cand = p->cand;
+    ma.build_valid = qd->valid_mask ? 0 : 1;
+    ma.build_cand = qd->candidate_mask ? 0 : 1;
+    ma.counts = p->counts;
+    GSC_CU(ctx, launch_masks(g, q, ma, st));
+
+    // Per-axis boxes.
+    const uint64_t planes = static_cast<uint64_t>(g.slices) * g.M;
+    GSC_TRY(dalloc(ctx, A, B, &p->xt, planes * g.n[0]));
+    GSC_TRY(dalloc(ctx, A, B, &p->yt, planes * g.n[1]));
+    GSC_TRY(dalloc(ctx, A, B, &p->zt, static_cast<uint64_t>(g.n[2]) * g.mw));
+    GSC_TRY(dalloc(ctx, A, B, &p->wt, static_cast<uint64_t>(g.n[3]) * g.ma));
+    GSC_CU(ctx, launch_axis_tables(g, q, p->abs->xn, p->abs->yn, p->abs->thf, p->abs->vf, p->xt, p->yt, p->zt, p->wt,
+                                   p->flags, st));
+    if (p->safe) GSC_CU(ctx, launch_valid_vs_safe(g, p->valid, p->safe, p->safe_rank, p->counts + 4, st));
+    unsigned long long hc[8];
+    unsigned int hflags = 0;
+    GSC_CU(ctx, cudaMemcpyAsync(hc, p->counts, sizeof(hc), cudaMemcpyDeviceToHost, st));
+    GSC_CU(ctx, cudaMemcpyAsync(&hflags, p->flags, sizeof(hflags), cudaMemcpyDeviceToHost, st));
+    GSC_CU(ctx, cudaStreamSynchronize(st));
+    if (hc[2] != 0) return fail(ctx, GSC_ERR_CANDIDATE_INVALID, "candidate set contains invalid states");
+    p->valid_count = hc[0];
+    p->candidate_count = hc[1];
+    if (hflags != 0) fused_ok = false;   // an empty or over-wide interval: only the stored count is exact
+    if (method == GSC_METHOD_AUTO) method = fused_ok ? GSC_METHOD_FUSED : (stored_ok ? GSC_METHOD_STORED : 0);
+    if (method == 0) return fail(ctx, GSC_ERR_UNSUPPORTED, "no method applies to this grid");
+    if (method == GSC_METHOD_FUSED && !fused_ok)
+        return fail(ctx, GSC_ERR_UNSUPPORTED, "fused method: an interval is empty or wider than 64 cells");
+    p->method = method;
+    // need the valid-cell test when some cell's validity is not its safety
+    p->need_valid = p->safe ? (hc[4] != 0) : (p->valid_count != g.S);
+
+    // Fixpoint state.
+    const uint64_t iter_bound = std::min<uint64_t>(q.max_iterations, g.S + 1);
+    if (iter_bound + 2 > kStatsCapMax)
+        return fail(ctx, GSC_ERR_UNSUPPORTED, "more than 2^20 fixpoint iterations requested");
+    p->stats_cap = static_cast<uint32_t>(iter_bound + 2);
+    GSC_TRY(dalloc(ctx, A, B, &p->controller, g.S));
+    GSC_TRY(dalloc(ctx, A, B, &p->reach_step, g.S));
+    GSC_TRY(dalloc(ctx, A, B, &p->fc, 1));
+    GSC_TRY(dalloc(ctx, A, B, &p->stats, 2ull * p->stats_cap));
+    GSC_TRY(dalloc(ctx, A, B, &p->reach8, g.S));
+
+    if (method == GSC_METHOD_STORED) {
+        GSC_TRY(dalloc(ctx, A, B, &p->pvalid, g.tsize));
+        GSC_CU(ctx, cudaMemsetAsync(p->pvalid, 0, g.tsize * 4, st));
+        GSC_CU(ctx, launch_prefix4(g, 0, p->valid, nullptr, p->pvalid, nullptr, st));
+        if (p->safe && p->safe_rank == 2) {
+            GSC_TRY(dalloc(ctx, A, B, &p->unsafe2, static_cast<uint64_t>(g.n[0] + 1) * (g.n[1] + 1)));
+            GSC_CU(ctx, launch_prefix2_unsafe(g, p->safe, p->unsafe2, st));
+        } else if (p->safe) {
+            GSC_TRY(dalloc(ctx, A, B, &p->unsafe4, g.tsize));
+            GSC_CU(ctx, cudaMemsetAsync(p->unsafe4, 0, g.tsize * 4, st));
+            GSC_CU(ctx, launch_prefix4(g, 2, p->safe, nullptr, p->unsafe4, nullptr, st));
+        }
+        p->S_pad = (g.S + 1) & ~1ull;
+        GSC_TRY(dalloc(ctx, A, B, &p->boxes, p->S_pad * g.M));
+        StoredBuildArgs sb{};
+        sb.xt = p->xt;
+        sb.yt = p->yt;
+        sb.zt = p->zt;
+        sb.wt = p->wt;
+        sb.safe = p->safe;
+        sb.safe_rank = p->safe_rank;
+        sb.unsafe2 = p->unsafe2;
+        sb.unsafe4 = p->unsafe4;
+        sb.pvalid = p->pvalid;
+        sb.boxes = p->boxes;
+        sb.S_pad = p->S_pad;
+        sb.valid_pairs = p->counts + 3;
+        GSC_CU(ctx, launch_stored_build(g, sb, st));
+        GSC_TRY(dalloc(ctx, A, B, &p->pd, g.tsize));
+        GSC_CU(ctx, cudaMemsetAsync(p->pd, 0, g.tsize * 4, st));
+    } else {
+        const uint64_t words = g.rows * g.W;
+        GSC_TRY(dalloc(ctx, A, B, &p->validb, words));
+        GSC_TRY(dalloc(ctx, A, B, &p->unsafeb, words));
+        GSC_TRY(dalloc(ctx, A, B, &p->srcb, words));
+        GSC_TRY(dalloc(ctx, A, B, &p->candb, words));
+        GSC_TRY(dalloc(ctx, A, B, &p->dp, words));
+        GSC_TRY(dalloc(ctx, A, B, &p->reach0, words));
+        GSC_TRY(dalloc(ctx, A, B, &p->reach1, words));
+        GSC_TRY(dalloc(ctx, A, B, &p->active, words));
+        GSC_CU(ctx, launch_pack_bits(g, 0, p->valid, nullptr, p->validb, st));
+        GSC_CU(ctx, launch_pack_bits(g, 0, p->cand, nullptr, p->candb, st));
+        if (!p->safe) {
+            GSC_CU(ctx, cudaMemsetAsync(p->unsafeb, 0, words * 8, st));
+            GSC_CU(ctx, cudaMemcpyAsync(p->srcb, p->validb, words * 8, cudaMemcpyDeviceToDevice, st));
+        } else if (p->safe_rank == 2) {
+            GSC_CU(ctx, launch_pack_bits(g, 2, nullptr, p->safe, p->unsafeb, st));
+            GSC_CU(ctx, launch_pack_bits(g, 3, p->valid, p->safe, p->srcb, st));
+        } else {
+            GSC_CU(ctx, launch_pack_bits(g, 1, p->safe, nullptr, p->unsafeb, st));
+            GSC_CU(ctx, launch_pack_bits(g, 4, p->valid, p->safe, p->srcb, st));
+        }
+    }
+    GSC_CU(ctx, cudaMemcpyAsync(hc, p->counts, sizeof(hc), cudaMemcpyDeviceToHost, st));
+    GSC_CU(ctx, cudaStreamSynchronize(st));
+    p->valid_pairs = hc[3];
+    return GSC_OK;
+}
+
+StoredFixArgs stored_args(gsc_problem* p, cudaGraphConditionalHandle cond, int use_cond) {
+    StoredFixArgs a{};
+    a.boxes = p->boxes;
+    a.S_pad = p->S_pad;
+    a.pd = p->pd;
+    a.valid = p->valid;
+    a.cand = p->cand;
+    a.reach = p->reach8;
+    a.controller = p->controller;
+    a.reach_step = p->reach_step;
+    a.fc = p->fc;
+    a.stats = p->stats;
+    a.cond = cond;
+    a.use_cond = use_cond;
+    return a;
+}
+
+FusedFixArgs fused_args(gsc_problem* p, cudaGraphConditionalHandle cond, int use_cond) {
+    FusedFixArgs a{};
+    a.xt = p->xt;
+    a.yt = p->yt;
+    a.zt = p->zt;
+    a.wt = p->wt;
+    a.validb = p->validb;
+    a.unsafeb = p->unsafeb;
+    a.srcb = p->srcb;
+    a.candb = p->candb;
+    a.dp = p->dp;
+    a.reach0 = p->reach0;
+    a.reach1 = p->reach1;
+    a.active = p->active;
+    a.controller = p->controller;
+    a.reach_step = p->reach_step;
+    a.fc = p->fc;
+    a.stats = p->stats;
+    a.need_valid = p->need_valid;
+    a.cond = cond;
+    a.use_cond = use_cond;
+    return a;
+}
+
+cudaError_t enqueue_init(gsc_problem* p) {
+    cudaStream_t st = p->ctx->stream;
+    cudaError_t e = launch_fix_init(p->fc, p->q.max_iterations, p->stats_cap, p->counts, p->stats, st);
+    if (e != cudaSuccess) return e;
+    if (p->method == GSC_METHOD_STORED) return launch_stored_init(p->g, stored_args(p, 0, 0), st);
+    return launch_fused_init(p->g, fused_args(p, 0, 0), p->cand, st);
+}
+
+cudaError_t enqueue_iteration(gsc_problem* p, cudaGraphConditionalHandle cond, int use_cond, uint32_t* launches) {
+    if (p->method == GSC_METHOD_STORED)
+        return launch_stored_iteration(p->g, stored_args(p, cond, use_cond), p->ctx->stream, launches);
+    return launch_fused_iteration(p->g, fused_args(p, cond, use_cond), p->ctx->stream, launches);
+}
+
+// Outer graph: [init kernels] -> while (condition) { one iteration }.  The
+// condition defaults to 1 at each launch; the control kernel at the end of
+// the body writes !stop.
+int build_graph(gsc_problem* p) {
+    gsc_context* ctx = p->ctx;
+    cudaStream_t st = ctx->stream;
+    cudaGraph_t g = nullptr, ginit = nullptr;
+    GSC_CU(ctx, cudaGraphCreate(&g, 0));
+    p->graph = g;
+    GSC_CU(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = enqueue_init(p);
+    cudaError_t e2 = cudaStreamEndCapture(st, &ginit);
+    GSC_CU(ctx, e);
+    GSC_CU(ctx, e2);
+    cudaGraphNode_t init_node;
+    e = cudaGraphAddChildGraphNode(&init_node, g, nullptr, 0, ginit);
+    cudaGraphDestroy(ginit);
+    GSC_CU(ctx, e);
+    cudaGraphConditionalHandle handle;
+    GSC_CU(ctx, cudaGraphConditionalHandleCreate(&handle, g, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+    cp.conditional.handle = handle;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t cnode;
+    GSC_CU(ctx, cudaGraphAddNode(&cnode, g, &init_node, 1, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    GSC_CU(ctx, cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    uint32_t launches = 0;
+    e = enqueue_iteration(p, handle, 1, &launches);
+    cudaGraph_t body_out = nullptr;
+    e2 = cudaStreamEndCapture(st, &body_out);
+    GSC_CU(ctx, e);
+    GSC_CU(ctx, e2);
+    GSC_CU(ctx, cudaGraphInstantiate(&p->exec, g, 0));
+    return GSC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gsc_problem_create(gsc_context* ctx, const gsc_abstraction* abs, const gsc_query_desc* query, uint32_t method,
+                       gsc_problem** out) {
+    if (!ctx || !abs || !query || !out) return GSC_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    if (abs->ctx != ctx) return fail(ctx, GSC_ERR_INVALID_ARGUMENT, "abstraction belongs to another context");
+    GSC_CU(ctx, cudaSetDevice(ctx->device));
+    std::unique_ptr<gsc_problem> p(new (std::nothrow) gsc_problem());
+    if (!p) return GSC_ERR_OUT_OF_MEMORY;
+    p->ctx = ctx;
+    p->abs = abs;
+    p->g = abs->g;
+    GSC_CU(ctx, cudaEventRecord(ctx->ev[0], ctx->stream));
+    const int s = build_problem(p.get(), query, method);
+    if (s != GSC_OK) return s;
+    GSC_CU(ctx, cudaEventRecord(ctx->ev[1], ctx->stream));
+    GSC_CU(ctx, cudaEventSynchronize(ctx->ev[1]));
+    float ms = 0.f;
+    GSC_CU(ctx, cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));
+    p->timings.prepare_ms = ms;
+    p->timings.abstraction_ms = abs->build_ms;
+    p->timings.device_bytes = p->bytes;
+    p->timings.method = p->method;
+    *out = p.release();
+    return GSC_OK;
+}
+
+void gsc_problem_destroy(gsc_problem* p) {
+    if (!p) return;
+    cudaSetDevice(p->ctx->device);
+    delete p;
+}
+
+int gsc_problem_solve(gsc_problem* p, uint32_t flags) {
+    if (!p) return GSC_ERR_INVALID_ARGUMENT;
+    gsc_context* ctx = p->ctx;
+    GSC_CU(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    GSC_CU(ctx, cudaEventRecord(ctx->ev[0], st));
+    uint32_t launches = 0;
+    if (flags & GSC_SOLVE_GRAPH) {
+        if (!p->exec) GSC_TRY(build_graph(p));
+        GSC_CU(ctx, cudaGraphLaunch(p->exec, st));
+        launches = 0;   // counted by the caller from the iteration count
+    } else {
+        GSC_CU(ctx, enqueue_init(p));
+        launches += 2;
+        uint32_t host_stop = 0, chunk = 4, done = 0;
+        FixControl hfc;
+        while (true) {
+            for (uint32_t i = 0; i < chunk; ++i) GSC_CU(ctx, enqueue_iteration(p, 0, 0, &launches));
+            done += chunk;
+            GSC_CU(ctx, cudaMemcpyAsync(&hfc, p->fc, sizeof(hfc), cudaMemcpyDeviceToHost, st));
+            GSC_CU(ctx, cudaStreamSynchronize(st));
+            host_stop = hfc.stop;
+            if (host_stop) break;
+            if (chunk < 64) chunk *= 2;
+        }
+        (void)done;
+    }
+    GSC_CU(ctx, cudaEventRecord(ctx->ev[1], st));
+    GSC_CU(ctx, cudaEventSynchronize(ctx->ev[1]));
+    float ms = 0.f;
+    GSC_CU(ctx, cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));
+    p->timings.solve_ms = ms;
+    p->timings.kernel_launches = launches;
+    return GSC_OK;
+}
+
+int gsc_problem_read(gsc_problem* p, gsc_result* r) {
+    if (!p || !r) return GSC_ERR_INVALID_ARGUMENT;
+    gsc_context* ctx = p->ctx;
+    GSC_CU(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    const GridInfo& g = p->g;
+    GSC_CU(ctx, cudaEventRecord(ctx->ev[0], st));
+    FixControl fc;
+    GSC_CU(ctx, cudaMemcpyAsync(&fc, p->fc, sizeof(fc), cudaMemcpyDeviceToHost, st));
+    GSC_CU(ctx, cudaStreamSynchronize(st));
+    for (int d = 0; d < 4; ++d) r->shape[d] = g.n[d];
+    r->input_shape[0] = g.ma;
+    r->input_shape[1] = g.mw;
+    r->states = g.S;
+    r->inputs = g.M;
+    r->pairs = g.S * g.M;
+    r->iterations = fc.iter;
+    r->converged = static_cast<int32_t>(fc.converged);
+    r->message = static_cast<int32_t>(fc.message ? fc.message : GSC_MSG_MAX_ITERATIONS);
+    r->certified_candidates = fc.certified;
+    r->reachable_states = fc.reachable;
+    r->candidate_count = fc.candidate_count;
+    r->valid_count = fc.valid_count;
+    if (r->valid_mask) GSC_CU(ctx, cudaMemcpyAsync(r->valid_mask, p->valid, g.S, cudaMemcpyDeviceToHost, st));
+    if (r->candidate_mask) GSC_CU(ctx, cudaMemcpyAsync(r->candidate_mask, p->cand, g.S, cudaMemcpyDeviceToHost, st));
+    if (r->reachable_mask) {
+        if (p->method == GSC_METHOD_FUSED)
+            GSC_CU(ctx, launch_unpack_bits(g, (fc.iter & 1) ? p->reach1 : p->reach0, p->reach8, st));
+        GSC_CU(ctx, cudaMemcpyAsync(r->reachable_mask, p->reach8, g.S, cudaMemcpyDeviceToHost, st));
+    }
+    if (r->controller)
+        GSC_CU(ctx, cudaMemcpyAsync(r->controller, p->controller, g.S * 4, cudaMemcpyDeviceToHost, st));
+    if (r->reach_step)
+        GSC_CU(ctx, cudaMemcpyAsync(r->reach_step, p->reach_step, g.S * 4, cudaMemcpyDeviceToHost, st));
+    const uint32_t n = std::min<uint32_t>(fc.iter, r->iter_capacity);
+    if (n && (r->iter_new_reachable || r->iter_new_certified)) {
+        std::vector<unsigned long long> hs(2ull * (n + 1));
+        GSC_CU(ctx, cudaMemcpyAsync(hs.data(), p->stats, hs.size() * 8, cudaMemcpyDeviceToHost, st));
+        GSC_CU(ctx, cudaStreamSynchronize(st));
+        for (uint32_t i = 0; i < n; ++i) {
+            if (r->iter_new_reachable) r->iter_new_reachable[i] = hs[2 * (i + 1)];
+            if (r->iter_new_certified) r->iter_new_certified[i] = hs[2 * (i + 1) + 1];
+        }
+    }
+    GSC_CU(ctx, cudaEventRecord(ctx->ev[1], st));
+    GSC_CU(ctx, cudaEventSynchronize(ctx->ev[1]));
+    float ms = 0.f;
+    GSC_CU(ctx, cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));
+    p->timings.readback_ms = ms;
+    return GSC_OK;
+}
+
+int gsc_problem_export_abstraction(gsc_problem* p, uint32_t* min_flat, uint32_t* max_flat, uint8_t* valid) {
+    if (!p || !min_flat || !max_flat || !valid) return GSC_ERR_INVALID_ARGUMENT;
+    gsc_context* ctx = p->ctx;
+    GSC_CU(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    const GridInfo& g = p->g;
+    // The export needs the unsafe prefix of the stored build; make it if the
+    // fused method skipped it.
+    if (p->safe && p->safe_rank == 2 && !p->unsafe2) {
+        GSC_TRY(dalloc(ctx, p->allocs, p->bytes, &p->unsafe2, static_cast<uint64_t>(g.n[0] + 1) * (g.n[1] + 1)));
+        GSC_CU(ctx, launch_prefix2_unsafe(g, p->safe, p->unsafe2, st));
+    } else if (p->safe && p->safe_rank == 4 && !p->unsafe4) {
+        GSC_TRY(dalloc(ctx, p->allocs, p->bytes, &p->unsafe4, g.tsize));
+        GSC_CU(ctx, cudaMemsetAsync(p->unsafe4, 0, g.tsize * 4, st));
+        GSC_CU(ctx, launch_prefix4(g, 2, p->safe, nullptr, p->unsafe4, nullptr, st));
+    }
+    const uint64_t P = g.S * g.M;
+    const uint64_t chunk = std::min<uint64_t>(P, 1ull << 26);
+    uint32_t *dmn = nullptr, *dmx = nullptr;
+    uint8_t* dv = nullptr;
+    cudaError_t e = cudaMalloc(&dmn, chunk * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&dmx, chunk * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&dv, chunk);
+    for (uint64_t b = 0; e == cudaSuccess && b < P; b += chunk) {
+        const uint64_t n = std::min<uint64_t>(chunk, P - b);
+        ExportArgs ea{};
+        ea.xt = p->xt;
+        ea.yt = p->yt;
+        ea.zt = p->zt;
+        ea.wt = p->wt;
+        ea.safe = p->safe;
+        ea.safe_rank = p->safe_rank;
+        ea.unsafe2 = p->unsafe2;
+        ea.unsafe4 = p->unsafe4;
+        ea.min_flat = dmn;
+        ea.max_flat = dmx;
+        ea.valid = dv;
+        ea.pair_begin = b;
+        ea.pair_count = n;
+        e = launch_export(g, ea, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(min_flat + b, dmn, n * 4, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(max_flat + b, dmx, n * 4, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(valid + b, dv, n, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    }
+    cudaFree(dmn);
+    cudaFree(dmx);
+    cudaFree(dv);
+    GSC_CU(ctx, e);
+    return GSC_OK;
+}
+
+int gsc_problem_timings(const gsc_problem* p, gsc_timings* out) {
+    if (!p || !out) return GSC_ERR_INVALID_ARGUMENT;
+    *out = p->timings;
+    return GSC_OK;
+}
+
+int gsc_run_case(int device, const gsc_model_desc* model, const gsc_query_desc* query, uint32_t method,
+                 uint32_t flags, gsc_result* out, gsc_timings* timings) {
+    if (!model || !query || !out) return GSC_ERR_INVALID_ARGUMENT;
+    gsc_context* ctx = nullptr;
+    int s = gsc_context_create(device, nullptr, &ctx);
+    if (s != GSC_OK) return s;
+    gsc_abstraction* abs = nullptr;
+    gsc_problem* p = nullptr;
+    s = gsc_abstraction_create(ctx, model, &abs);
+    if (s == GSC_OK) s = gsc_problem_create(ctx, abs, query, method, &p);
+    if (s == GSC_OK) s = gsc_problem_solve(p, flags);
+    if (s == GSC_OK) s = gsc_problem_read(p, out);
+    if (s == GSC_OK && timings) gsc_problem_timings(p, timings);
+    gsc_problem_destroy(p);
+    gsc_abstraction_destroy(abs);
+    gsc_context_destroy(ctx);
+    return s;
+}
+
+}  // extern "C"

@@ -1,0 +1,128 @@
+// gsc_kernels.cuh -- launch wrappers shared between the kernel files and the C ABI layer.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "gsc_common.cuh"
+
+namespace gsc_b200 {
+
+// ---- abstraction (resident nominal successors) ------------------------------------------
+// xn[((i2*n3 + i3)*M + j)*n0 + i0] = nominal x after K Euler substeps (model.hpp:26-46),
+// yn likewise over i1.  cosT/sinT[(i2*mw + jw)*K + k], vseq[(i3*ma + ja)*K + k].
+cudaError_t launch_nominal_xy(const GridInfo& g, const double* cosT, const double* sinT, const double* vseq,
+                              double* xn, double* yn, cudaStream_t st);
+
+// ---- query preparation ------------------------------------------------------------------
+struct MaskArgs {
+    const double* obstacles;  // [n][8] device
+    uint8_t* valid;           // [S]
+    uint8_t* cand;            // [S]
+    int build_valid;          // 0: valid already filled by the caller's mask
+    int build_cand;
+    unsigned long long* counts;  // [0] valid, [1] candidate, [2] candidate-not-valid
+};
+cudaError_t launch_masks(const GridInfo& g, const QueryInfo& q, const MaskArgs& a, cudaStream_t st);
+cudaError_t launch_safe2(const GridInfo& g, const QueryInfo& q, uint8_t* safe2, cudaStream_t st);
+
+// Per-axis quantised boxes.  xt/yt: [n2][n3][M][n0|n1], zt: [n2][mw], wt: [n3][ma], packed
+// lo | hi << 16 or kReject.  flags |= 1 if an accepted non-wrap interval is empty (hi < lo),
+// |= 2 if one is wider than 64 cells.
+cudaError_t launch_axis_tables(const GridInfo& g, const QueryInfo& q, const double* xn, const double* yn,
+                               const double* thf, const double* vf, uint32_t* xt, uint32_t* yt, uint32_t* zt,
+                               uint32_t* wt, unsigned int* flags, cudaStream_t st);
+
+// Bit-sliced sets: bit i0 of word w of x-row r is state r*n0 + 64*w + i0.
+// mode 0: bit = src[s] != 0; 1: bit = src[s] == 0; 2: bit = src2d[i1*n0 + i0] == 0;
+// 3: bit = src[s] != 0 && src2d[i1*n0+i0] != 0; 4: bit = src[s] != 0 && src[s] (4-D second) != 0
+cudaError_t launch_pack_bits(const GridInfo& g, int mode, const uint8_t* src, const uint8_t* src2, uint64_t* out,
+                             cudaStream_t st);
+cudaError_t launch_unpack_bits(const GridInfo& g, const uint64_t* bits, uint8_t* out, cudaStream_t st);
+
+// Counts cells with valid != safe (safe rank 2 or 4) into *count.
+cudaError_t launch_valid_vs_safe(const GridInfo& g, const uint8_t* valid, const uint8_t* safe, int safe_rank,
+                                 unsigned long long* count, cudaStream_t st);
+
+// ---- 4-D inclusive prefix tables (int32, zero first plane per dimension) -----------------
+// mode 0: valid; 1: valid && !reach (b = reach); 2: !safe (4-D safe mask).
+cudaError_t launch_prefix4(const GridInfo& g, int mode, const uint8_t* a, const uint8_t* b, int32_t* table,
+                           const FixControl* ctl, cudaStream_t st);
+// 2-D prefix of !safe2 over (x, y): (n0+1)*(n1+1) entries, stride n0+1.
+cudaError_t launch_prefix2_unsafe(const GridInfo& g, const uint8_t* safe2, int32_t* table, cudaStream_t st);
+
+// ---- stored per-pair boxes --------------------------------------------------------------
+struct StoredBuildArgs {
+    const uint32_t *xt, *yt, *zt, *wt;
+    const uint8_t* safe;      // rank 2 or 4
+    int safe_rank;
+    const int32_t* unsafe2;   // rank 2 prefix
+    const int32_t* unsafe4;   // rank 4 prefix
+    const int32_t* pvalid;    // 4-D valid prefix
+    uint2* boxes;             // [M][S_pad]
+    uint64_t S_pad;
+    unsigned long long* valid_pairs;   // abstraction-valid pairs (before the V(box) > 0 fold)
+};
+cudaError_t launch_stored_build(const GridInfo& g, const StoredBuildArgs& a, cudaStream_t st);
+
+// Reference-format abstraction (pair = s * M + j), abstraction.hpp:161-209.
+struct ExportArgs {
+    const uint32_t *xt, *yt, *zt, *wt;
+    const uint8_t* safe;
+    int safe_rank;
+    const int32_t* unsafe2;
+    const int32_t* unsafe4;
+    uint32_t* min_flat;
+    uint32_t* max_flat;
+    uint8_t* valid;
+    uint64_t pair_begin, pair_count;
+};
+cudaError_t launch_export(const GridInfo& g, const ExportArgs& a, cudaStream_t st);
+
+// ---- fixpoint ---------------------------------------------------------------------------
+struct StoredFixArgs {
+    const uint2* boxes;
+    uint64_t S_pad;
+    int32_t* pd;              // D-prefix table
+    const uint8_t* valid;
+    const uint8_t* cand;
+    uint8_t* reach;
+    uint32_t* controller;
+    uint32_t* reach_step;
+    FixControl* fc;
+    unsigned long long* stats;   // [stats_cap][2]
+    cudaGraphConditionalHandle cond;
+    int use_cond;
+};
+cudaError_t launch_stored_init(const GridInfo& g, const StoredFixArgs& a, cudaStream_t st);
+cudaError_t launch_stored_iteration(const GridInfo& g, const StoredFixArgs& a, cudaStream_t st, uint32_t* launches);
+
+struct FusedFixArgs {
+    const uint32_t *xt, *yt, *zt, *wt;
+    const uint64_t* validb;
+    const uint64_t* unsafeb;
+    const uint64_t* srcb;      // valid && source-safe
+    const uint64_t* candb;
+    uint64_t* dp;
+    uint64_t* reach0;
+    uint64_t* reach1;
+    uint64_t* active;
+    uint32_t* controller;
+    uint32_t* reach_step;
+    FixControl* fc;
+    unsigned long long* stats;
+    int need_valid;
+    cudaGraphConditionalHandle cond;
+    int use_cond;
+};
+cudaError_t launch_fused_init(const GridInfo& g, const FusedFixArgs& a, const uint8_t* cand, cudaStream_t st);
+cudaError_t launch_fused_iteration(const GridInfo& g, const FusedFixArgs& a, cudaStream_t st, uint32_t* launches);
+
+// Resets the control block and zeroes the per-iteration counters.
+cudaError_t launch_fix_init(FixControl* fc, uint32_t max_iterations, uint32_t stats_cap,
+                            const unsigned long long* counts, unsigned long long* stats, cudaStream_t st);
+
+// Sets the graph condition from the control block (first node of a graph solve).
+cudaError_t launch_set_condition(const FixControl* fc, cudaGraphConditionalHandle cond, cudaStream_t st);
+
+}  // namespace gsc_b200

@@ -1,0 +1,449 @@
+// gsc_tables.cu -- abstraction and query-preparation kernels.
+//
+// The reference builds one (min_flat, max_flat, valid) triple per (state,
+// input) pair in abstraction_kernel (cuda/kernels.cu:164-217), evaluating the
+// Euler successor and enumerating every cell of the box.  Here the same boxes
+// come from the structure of the unicycle model (model.hpp:26-46): theta
+// evolves from (theta cell, omega) alone, v from (v cell, a) alone, x from
+// (x, theta, v, input) and y from (y, theta, v, input).  Each coordinate of the
+// nominal successor is therefore a per-axis table, bit-identical to the
+// reference's per-pair value because it is the same sequence of rounded
+// operations.  The box test over cells is a prefix-count (or bit-sliced OR)
+// instead of an enumeration.
+#include "gsc_kernels.cuh"
+
+namespace gsc_b200 {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+inline unsigned int blocks_for(uint64_t n, int threads = kThreads) {
+    uint64_t b = (n + threads - 1) / threads;
+    if (b > 0x7FFFFFFFull) b = 0x7FFFFFFFull;
+    if (b == 0) b = 1;
+    return static_cast<unsigned int>(b);
+}
+
+__device__ __forceinline__ void unflatten(const GridInfo& g, uint64_t s, uint32_t idx[4]) {
+    uint64_t r = s / g.n[0];
+    idx[0] = static_cast<uint32_t>(s - r * g.n[0]);
+    uint64_t r2 = r / g.n[1];
+    idx[1] = static_cast<uint32_t>(r - r2 * g.n[1]);
+    idx[3] = static_cast<uint32_t>(r2 / g.n[2]);
+    idx[2] = static_cast<uint32_t>(r2 - static_cast<uint64_t>(idx[3]) * g.n[2]);
+}
+
+__device__ __forceinline__ bool in_rect(const double* lb, const double* ub, const double x[4]) {
+    for (int d = 0; d < 4; ++d)
+        if (x[d] < lb[d] || x[d] > ub[d]) return false;
+    return true;
+}
+
+// ---- nominal successors -----------------------------------------------------------------
+
+// One thread per (plane, i) entry.  plane = (i2*n3 + i3)*M + j.
+__global__ void k_nominal_xy(GridInfo g, const double* __restrict__ cosT, const double* __restrict__ sinT,
+                             const double* __restrict__ vseq, double* __restrict__ xn, double* __restrict__ yn) {
+    const uint64_t planes = static_cast<uint64_t>(g.slices) * g.M;
+    const uint64_t nx = planes * g.n[0];
+    const uint64_t total = nx + planes * g.n[1];
+    for (uint64_t e = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; e < total;
+         e += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const bool is_x = e < nx;
+        const uint64_t ee = is_x ? e : e - nx;
+        const uint32_t n = is_x ? g.n[0] : g.n[1];
+        const uint64_t plane = ee / n;
+        const uint32_t i = static_cast<uint32_t>(ee - plane * n);
+        const uint32_t j = static_cast<uint32_t>(plane % g.M);
+        const uint64_t q = plane / g.M;
+        const uint32_t i3 = static_cast<uint32_t>(q % g.n[3]);
+        const uint32_t i2 = static_cast<uint32_t>(q / g.n[3]);
+        const uint32_t ja = j % g.ma, jw = j / g.ma;
+        const double* trig = (is_x ? cosT : sinT) + static_cast<uint64_t>(i2 * g.mw + jw) * g.K;
+        const double* vs = vseq + static_cast<uint64_t>(i3 * g.ma + ja) * g.K;
+        // out[d] += dt * (v * cos(theta)) per substep (model.hpp:34-45).
+        double c = centre(g, is_x ? 0 : 1, i);
+        for (uint32_t k = 0; k < g.K; ++k) c = dadd(c, dmul(g.dt, dmul(vs[k], trig[k])));
+        (is_x ? xn : yn)[ee] = c;
+    }
+}
+
+// ---- masks ------------------------------------------------------------------------------
+
+// build_valid_mask / build_candidate_mask (abstraction.hpp:65-106) plus the
+// ellipse candidate; counts valid, candidate and candidate-but-invalid cells.
+__global__ void k_masks(GridInfo g, QueryInfo q, MaskArgs a) {
+    unsigned long long nv = 0, nc = 0, nbad = 0;
+    for (uint64_t s = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; s < g.S;
+         s += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        uint32_t idx[4];
+        unflatten(g, s, idx);
+        double x[4];
+        for (int d = 0; d < 4; ++d) x[d] = centre(g, d, idx[d]);
+        bool v;
+        if (a.build_valid) {
+            v = in_rect(q.map_lb, q.map_ub, x);
+            if (v) {
+                for (int o = 0; o < q.n_obstacles; ++o) {
+                    if (in_rect(a.obstacles + 8 * o, a.obstacles + 8 * o + 4, x)) {
+                        v = false;
+                        break;
+                    }
+                }
+            }
+            if (v && q.ckind != 0) v = satisfies(q, x[0], x[1]);
+            a.valid[s] = v ? 1 : 0;
+        } else {
+            v = a.valid[s] != 0;
+        }
+        bool k;
+        if (a.build_cand) {
+            if (q.cand_kind == 0) {
+                k = in_rect(q.cand, q.cand + 4, x);
+            } else {
+                const double dx = dsub(x[0], q.cand[0]);
+                const double dy = dsub(x[1], q.cand[1]);
+                k = v && (dadd(dmul(dmul(dx, dx), q.cand[2]), dmul(dmul(dy, dy), q.cand[3])) <= q.cand[4]);
+            }
+            a.cand[s] = k ? 1 : 0;
+        } else {
+            k = a.cand[s] != 0;
+        }
+        nv += v;
+        nc += k;
+        nbad += (k && !v);
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        nv += __shfl_down_sync(0xFFFFFFFFu, nv, off);
+        nc += __shfl_down_sync(0xFFFFFFFFu, nc, off);
+        nbad += __shfl_down_sync(0xFFFFFFFFu, nbad, off);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (nv) atomicAdd(&a.counts[0], nv);
+        if (nc) atomicAdd(&a.counts[1], nc);
+        if (nbad) atomicAdd(&a.counts[2], nbad);
+    }
+}
+
+// The state constraint at the centres of the (x, y) plane: every built-in
+// constraint reads only x and y (config.cpp:62-75).
+__global__ void k_safe2(GridInfo g, QueryInfo q, uint8_t* safe2) {
+    const uint32_t n = g.n[0] * g.n[1];
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+        const uint32_t i1 = e / g.n[0];
+        const uint32_t i0 = e - i1 * g.n[0];
+        safe2[e] = satisfies(q, centre(g, 0, i0), centre(g, 1, i1)) ? 1 : 0;
+    }
+}
+
+// ---- per-axis boxes ---------------------------------------------------------------------
+
+__global__ void k_axis_tables(GridInfo g, QueryInfo q, const double* __restrict__ xn, const double* __restrict__ yn,
+                              const double* __restrict__ thf, const double* __restrict__ vf, uint32_t* xt,
+                              uint32_t* yt, uint32_t* zt, uint32_t* wt, unsigned int* flags) {
+    const uint64_t planes = static_cast<uint64_t>(g.slices) * g.M;
+    const uint64_t nx = planes * g.n[0];
+    const uint64_t ny = planes * g.n[1];
+    const uint64_t nz = static_cast<uint64_t>(g.n[2]) * g.mw;
+    const uint64_t nw = static_cast<uint64_t>(g.n[3]) * g.ma;
+    const uint64_t total = nx + ny + nz + nw;
+    unsigned int fl = 0;
+    for (uint64_t e = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; e < total;
+         e += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        if (e < nx + ny) {
+            const bool is_x = e < nx;
+            const uint64_t ee = is_x ? e : e - nx;
+            const uint32_t n = is_x ? g.n[0] : g.n[1];
+            const uint64_t plane = ee / n;
+            const uint32_t i3 = static_cast<uint32_t>((plane / g.M) % g.n[3]);
+            const int d = is_x ? 0 : 1;
+            const double r = box_radius(g, q, d, centre(g, 3, i3));
+            uint32_t lo, hi;
+            const bool ok = axis_box(g, d, (is_x ? xn : yn)[ee], r, &lo, &hi);
+            (is_x ? xt : yt)[ee] = ok ? pack16(lo, hi) : kReject;
+            if (ok && hi < lo) fl |= 1u;
+            if (ok && hi >= lo && hi - lo >= 64) fl |= 2u;
+        } else if (e < nx + ny + nz) {
+            const uint32_t ee = static_cast<uint32_t>(e - nx - ny);   // i2 * mw + jw
+            const double r = box_radius(g, q, 2, 0.0);
+            uint32_t lo, hi;
+            wrap_box(g, thf[ee], r, &lo, &hi);
+            zt[ee] = pack16(lo, hi);
+        } else {
+            const uint32_t ee = static_cast<uint32_t>(e - nx - ny - nz);   // i3 * ma + ja
+            const double r = box_radius(g, q, 3, 0.0);
+            uint32_t lo, hi;
+            const bool ok = axis_box(g, 3, vf[ee], r, &lo, &hi);
+            wt[ee] = ok ? pack16(lo, hi) : kReject;
+            if (ok && hi < lo) fl |= 1u;
+        }
+    }
+    if (fl) atomicOr(flags, fl);
+}
+
+// ---- bit-sliced sets --------------------------------------------------------------------
+
+__global__ void k_pack_bits(GridInfo g, int mode, const uint8_t* __restrict__ src, const uint8_t* __restrict__ src2,
+                            uint64_t* __restrict__ out) {
+    const uint64_t words = g.rows * g.W;
+    for (uint64_t e = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; e < words;
+         e += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint64_t r = e / g.W;
+        const uint32_t w = static_cast<uint32_t>(e - r * g.W);
+        const uint32_t i1 = static_cast<uint32_t>(r % g.n[1]);
+        const uint64_t base = r * g.n[0];
+        uint64_t word = 0;
+        for (uint32_t b = 0; b < 64; ++b) {
+            const uint32_t i0 = w * 64 + b;
+            if (i0 >= g.n[0]) break;
+            bool bit;
+            switch (mode) {
+                case 0: bit = src[base + i0] != 0; break;
+                case 1: bit = src[base + i0] == 0; break;
+                case 2: bit = src2[i1 * g.n[0] + i0] == 0; break;
+                case 3: bit = src[base + i0] != 0 && src2[i1 * g.n[0] + i0] != 0; break;
+                default: bit = src[base + i0] != 0 && src2[base + i0] != 0; break;
+            }
+            word |= static_cast<uint64_t>(bit) << b;
+        }
+        out[e] = word;
+    }
+}
+
+__global__ void k_unpack_bits(GridInfo g, const uint64_t* __restrict__ bits, uint8_t* __restrict__ out) {
+    for (uint64_t s = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; s < g.S;
+         s += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint64_t r = s / g.n[0];
+        const uint32_t i0 = static_cast<uint32_t>(s - r * g.n[0]);
+        out[s] = static_cast<uint8_t>((bits[r * g.W + (i0 >> 6)] >> (i0 & 63)) & 1u);
+    }
+}
+
+__global__ void k_valid_vs_safe(GridInfo g, const uint8_t* __restrict__ valid, const uint8_t* __restrict__ safe,
+                                int rank, unsigned long long* count) {
+    unsigned long long c = 0;
+    for (uint64_t s = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; s < g.S;
+         s += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        uint8_t sf;
+        if (rank == 4) {
+            sf = safe[s];
+        } else {
+            const uint64_t r = s / g.n[0];
+            const uint32_t i0 = static_cast<uint32_t>(s - r * g.n[0]);
+            sf = safe[(r % g.n[1]) * g.n[0] + i0];
+        }
+        c += ((valid[s] != 0) != (sf != 0));
+    }
+    for (int off = 16; off > 0; off >>= 1) c += __shfl_down_sync(0xFFFFFFFFu, c, off);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, c);
+}
+
+// ---- box counts on prefix tables --------------------------------------------------------
+
+// 16-corner inclusion-exclusion of one box [l, r) on a padded int32 table
+// (prefix_sum.hpp:65-85): even-popcount corners add.  Exact modulo 2^32.
+__device__ __forceinline__ uint32_t count16(const int32_t* __restrict__ P, const GridInfo& g, uint32_t l0,
+                                            uint32_t l1, uint32_t l2, uint32_t l3, uint32_t r0, uint32_t r1,
+                                            uint32_t r2, uint32_t r3) {
+    const uint32_t X[2] = {r0, l0};
+    const uint32_t Y[2] = {r1 * g.ps[1], l1 * g.ps[1]};
+    const uint32_t Z[2] = {r2 * g.ps[2], l2 * g.ps[2]};
+    const uint32_t Wd[2] = {r3 * g.ps[3], l3 * g.ps[3]};
+    uint32_t v[16];
+#pragma unroll
+    for (int m = 0; m < 16; ++m)
+        v[m] = static_cast<uint32_t>(__ldg(P + (X[m & 1] + Y[(m >> 1) & 1] + Z[(m >> 2) & 1] + Wd[(m >> 3) & 1])));
+    uint32_t t = 0;
+#pragma unroll
+    for (int m = 0; m < 16; ++m) t = (__popc(m) & 1) ? t - v[m] : t + v[m];
+    return t;
+}
+
+// query_box_count (prefix_sum.hpp:87-105): a box crossing the theta seam is split.
+__device__ __forceinline__ uint32_t count_box(const int32_t* __restrict__ P, const GridInfo& g, const uint32_t lo[4],
+                                              const uint32_t hi[4]) {
+    if (lo[2] <= hi[2]) return count16(P, g, lo[0], lo[1], lo[2], lo[3], hi[0] + 1, hi[1] + 1, hi[2] + 1, hi[3] + 1);
+    return count16(P, g, lo[0], lo[1], lo[2], lo[3], hi[0] + 1, hi[1] + 1, g.n[2], hi[3] + 1) +
+           count16(P, g, lo[0], lo[1], 0, lo[3], hi[0] + 1, hi[1] + 1, hi[2] + 1, hi[3] + 1);
+}
+
+// box_satisfies_constraint (abstraction.hpp:108-159) as a count of unsafe
+// centres: an empty non-wrap range enumerates no cell and passes.
+__device__ __forceinline__ bool box_safe(const GridInfo& g, const uint8_t* __restrict__ safe, int rank,
+                                         const int32_t* __restrict__ u2, const int32_t* __restrict__ u4,
+                                         const uint32_t lo[4], const uint32_t hi[4]) {
+    if (!safe) return true;
+    if (hi[0] < lo[0] || hi[1] < lo[1] || hi[3] < lo[3]) return true;
+    if (rank == 2) {
+        const uint32_t s1 = g.n[0] + 1;
+        const uint32_t a = static_cast<uint32_t>(__ldg(u2 + (hi[0] + 1) + (hi[1] + 1) * s1));
+        const uint32_t b = static_cast<uint32_t>(__ldg(u2 + lo[0] + (hi[1] + 1) * s1));
+        const uint32_t c = static_cast<uint32_t>(__ldg(u2 + (hi[0] + 1) + lo[1] * s1));
+        const uint32_t d = static_cast<uint32_t>(__ldg(u2 + lo[0] + lo[1] * s1));
+        return a - b - c + d == 0;
+    }
+    return count_box(u4, g, lo, hi) == 0;
+}
+
+struct PairBox {
+    bool ok;        // source safe, inside bounds (abstraction validity before the box test)
+    uint32_t lo[4], hi[4];
+};
+
+__device__ __forceinline__ PairBox pair_box(const GridInfo& g, const uint32_t* __restrict__ xt,
+                                            const uint32_t* __restrict__ yt, const uint32_t* __restrict__ zt,
+                                            const uint32_t* __restrict__ wt, const uint8_t* __restrict__ safe,
+                                            int rank, uint64_t s, uint32_t j) {
+    PairBox b;
+    uint32_t idx[4];
+    unflatten(g, s, idx);
+    const uint32_t ja = j % g.ma, jw = j / g.ma;
+    const uint64_t plane = (static_cast<uint64_t>(idx[2]) * g.n[3] + idx[3]) * g.M + j;
+    const uint32_t xe = __ldg(xt + plane * g.n[0] + idx[0]);
+    const uint32_t ye = __ldg(yt + plane * g.n[1] + idx[1]);
+    const uint32_t ze = __ldg(zt + idx[2] * g.mw + jw);
+    const uint32_t we = __ldg(wt + idx[3] * g.ma + ja);
+    bool src = true;
+    if (safe) src = (rank == 4) ? safe[s] != 0 : safe[idx[1] * g.n[0] + idx[0]] != 0;
+    b.ok = src && xe != kReject && ye != kReject && we != kReject;
+    b.lo[0] = lo16(xe);
+    b.hi[0] = hi16(xe);
+    b.lo[1] = lo16(ye);
+    b.hi[1] = hi16(ye);
+    b.lo[2] = lo16(ze);
+    b.hi[2] = hi16(ze);
+    b.lo[3] = lo16(we);
+    b.hi[3] = hi16(we);
+    return b;
+}
+
+// Stored layout: boxes[j * S_pad + s] = {pack8(lo), pack8(hi)}, or the
+// sentinel when the pair can never satisfy: abstraction-invalid, or a box
+// with no valid cell (the iteration-invariant valid_count == 0 test of
+// reachability.hpp:78-84).
+__global__ void k_stored_build(GridInfo g, StoredBuildArgs a) {
+    const uint64_t total = a.S_pad * g.M;
+    unsigned long long nvp = 0;
+    for (uint64_t e = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; e < total;
+         e += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint32_t j = static_cast<uint32_t>(e / a.S_pad);
+        const uint64_t s = e - static_cast<uint64_t>(j) * a.S_pad;
+        uint2 out = make_uint2(kBoxSentinel, kBoxSentinel);
+        if (s < g.S) {
+            const PairBox b = pair_box(g, a.xt, a.yt, a.zt, a.wt, a.safe, a.safe_rank, s, j);
+            if (b.ok && box_safe(g, a.safe, a.safe_rank, a.unsafe2, a.unsafe4, b.lo, b.hi)) {
+                ++nvp;
+                if (count_box(a.pvalid, g, b.lo, b.hi) != 0)
+                    out = make_uint2(pack8(b.lo[0], b.lo[1], b.lo[2], b.lo[3]), pack8(b.hi[0], b.hi[1], b.hi[2], b.hi[3]));
+            }
+        }
+        a.boxes[e] = out;
+    }
+    for (int off = 16; off > 0; off >>= 1) nvp += __shfl_down_sync(0xFFFFFFFFu, nvp, off);
+    if ((threadIdx.x & 31) == 0 && nvp) atomicAdd(a.valid_pairs, nvp);
+}
+
+__global__ void k_export(GridInfo g, ExportArgs a) {
+    for (uint64_t e = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; e < a.pair_count;
+         e += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint64_t pair = a.pair_begin + e;
+        const uint64_t s = pair / g.M;
+        const uint32_t j = static_cast<uint32_t>(pair - s * g.M);
+        const PairBox b = pair_box(g, a.xt, a.yt, a.zt, a.wt, a.safe, a.safe_rank, s, j);
+        const bool v = b.ok && box_safe(g, a.safe, a.safe_rank, a.unsafe2, a.unsafe4, b.lo, b.hi);
+        // grid.hpp:22-28 (flatten), x-fastest strides.
+        uint32_t mn = 0, mx = 0;
+        if (v) {
+            mn = b.lo[0] + g.n[0] * (b.lo[1] + g.n[1] * (b.lo[2] + g.n[2] * b.lo[3]));
+            mx = b.hi[0] + g.n[0] * (b.hi[1] + g.n[1] * (b.hi[2] + g.n[2] * b.hi[3]));
+        }
+        a.min_flat[e] = mn;
+        a.max_flat[e] = mx;
+        a.valid[e] = v ? 1 : 0;
+    }
+}
+
+// 2-D prefix of unsafe (x, y) centres; one block: rows, then columns.
+__global__ void k_prefix2(GridInfo g, const uint8_t* __restrict__ safe2, int32_t* __restrict__ t) {
+    const uint32_t s1 = g.n[0] + 1;
+    for (uint32_t y = threadIdx.x; y <= g.n[1]; y += blockDim.x) {
+        int32_t acc = 0;
+        t[y * s1] = 0;
+        for (uint32_t x = 1; x <= g.n[0]; ++x) {
+            if (y > 0) acc += safe2[(y - 1) * g.n[0] + (x - 1)] == 0;
+            t[y * s1 + x] = acc;
+        }
+    }
+    __syncthreads();
+    for (uint32_t x = threadIdx.x; x <= g.n[0]; x += blockDim.x) {
+        int32_t acc = 0;
+        for (uint32_t y = 1; y <= g.n[1]; ++y) {
+            acc += t[y * s1 + x];
+            t[y * s1 + x] = acc;
+        }
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_nominal_xy(const GridInfo& g, const double* cosT, const double* sinT, const double* vseq,
+                              double* xn, double* yn, cudaStream_t st) {
+    const uint64_t total = static_cast<uint64_t>(g.slices) * g.M * (g.n[0] + g.n[1]);
+    k_nominal_xy<<<blocks_for(total), kThreads, 0, st>>>(g, cosT, sinT, vseq, xn, yn);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_masks(const GridInfo& g, const QueryInfo& q, const MaskArgs& a, cudaStream_t st) {
+    k_masks<<<blocks_for(g.S), kThreads, 0, st>>>(g, q, a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_safe2(const GridInfo& g, const QueryInfo& q, uint8_t* safe2, cudaStream_t st) {
+    k_safe2<<<blocks_for(static_cast<uint64_t>(g.n[0]) * g.n[1]), kThreads, 0, st>>>(g, q, safe2);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_axis_tables(const GridInfo& g, const QueryInfo& q, const double* xn, const double* yn,
+                               const double* thf, const double* vf, uint32_t* xt, uint32_t* yt, uint32_t* zt,
+                               uint32_t* wt, unsigned int* flags, cudaStream_t st) {
+    const uint64_t planes = static_cast<uint64_t>(g.slices) * g.M;
+    const uint64_t total = planes * (g.n[0] + g.n[1]) + static_cast<uint64_t>(g.n[2]) * g.mw +
+                           static_cast<uint64_t>(g.n[3]) * g.ma;
+    k_axis_tables<<<blocks_for(total), kThreads, 0, st>>>(g, q, xn, yn, thf, vf, xt, yt, zt, wt, flags);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pack_bits(const GridInfo& g, int mode, const uint8_t* src, const uint8_t* src2, uint64_t* out,
+                             cudaStream_t st) {
+    k_pack_bits<<<blocks_for(g.rows * g.W), kThreads, 0, st>>>(g, mode, src, src2, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_unpack_bits(const GridInfo& g, const uint64_t* bits, uint8_t* out, cudaStream_t st) {
+    k_unpack_bits<<<blocks_for(g.S), kThreads, 0, st>>>(g, bits, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_valid_vs_safe(const GridInfo& g, const uint8_t* valid, const uint8_t* safe, int safe_rank,
+                                 unsigned long long* count, cudaStream_t st) {
+    k_valid_vs_safe<<<blocks_for(g.S), kThreads, 0, st>>>(g, valid, safe, safe_rank, count);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_prefix2_unsafe(const GridInfo& g, const uint8_t* safe2, int32_t* table, cudaStream_t st) {
+    k_prefix2<<<1, 256, 0, st>>>(g, safe2, table);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_stored_build(const GridInfo& g, const StoredBuildArgs& a, cudaStream_t st) {
+    k_stored_build<<<blocks_for(a.S_pad * g.M), kThreads, 0, st>>>(g, a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_export(const GridInfo& g, const ExportArgs& a, cudaStream_t st) {
+    k_export<<<blocks_for(a.pair_count), kThreads, 0, st>>>(g, a);
+    return cudaGetLastError();
+}
+
+}  // namespace gsc_b200

@@ -1,0 +1,357 @@
+"""Python binding of the B200 grid symbolic-control library (include/gsc_b200.h).
+
+The functions here mirror the reference's entry points
+(include/gsc/cuda_api.hpp:87-88: ``cuda_backend_compiled`` and
+``run_case_cuda_u32``) over the C ABI of ``libgsc_b200.so``.  There is no
+CPU fallback: if the library is missing, or no CUDA device is present, the
+calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgsc_b200.so")
+
+METHOD_AUTO, METHOD_STORED, METHOD_FUSED = 0, 1, 2
+SOLVE_GRAPH = 1
+CONSTRAINTS = {"none": 0, "hyperbolic": 1, "elliptic": 2, "quadric": 3}
+MESSAGES = {
+    0: "",
+    1: "all candidate states obtained a controller",
+    2: "iteration stalled before candidate closure",
+    3: "maximum iterations reached",
+}
+STATUS = {
+    0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "out of device memory", 4: "unsupported",
+    5: "no CUDA device found", 6: "candidate set contains invalid states", 7: "device wait timed out",
+}
+INVALID32 = 0xFFFFFFFF
+
+
+class GscError(RuntimeError):
+    def __init__(self, status, detail=""):
+        self.status = status
+        super().__init__(f"{STATUS.get(status, status)}" + (f": {detail}" if detail else ""))
+
+
+class ModelDesc(ctypes.Structure):
+    _fields_ = [
+        ("state_lb", ctypes.c_double * 4), ("state_ub", ctypes.c_double * 4), ("state_eta", ctypes.c_double * 4),
+        ("wrap_dim", ctypes.c_int32),
+        ("input_lb", ctypes.c_double * 2), ("input_ub", ctypes.c_double * 2), ("input_eta", ctypes.c_double * 2),
+        ("sample_time", ctypes.c_double), ("integration_substeps", ctypes.c_uint32),
+    ]
+
+
+class QueryDesc(ctypes.Structure):
+    _fields_ = [
+        ("disturbance_half_width", ctypes.c_double * 4),
+        ("constraint_kind", ctypes.c_int32), ("constraint_params", ctypes.c_double * 4),
+        ("map_lb", ctypes.c_double * 4), ("map_ub", ctypes.c_double * 4),
+        ("obstacle_count", ctypes.c_uint32), ("obstacles", ctypes.c_void_p),
+        ("candidate_kind", ctypes.c_int32), ("candidate", ctypes.c_double * 8),
+        ("max_iterations", ctypes.c_uint32),
+        ("safe_mask", ctypes.c_void_p), ("safe_mask_rank", ctypes.c_int32),
+        ("valid_mask", ctypes.c_void_p), ("candidate_mask", ctypes.c_void_p),
+    ]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [
+        ("valid_mask", ctypes.c_void_p), ("candidate_mask", ctypes.c_void_p), ("reachable_mask", ctypes.c_void_p),
+        ("controller", ctypes.c_void_p), ("reach_step", ctypes.c_void_p),
+        ("iter_new_reachable", ctypes.c_void_p), ("iter_new_certified", ctypes.c_void_p),
+        ("iter_capacity", ctypes.c_uint32),
+        ("shape", ctypes.c_uint32 * 4), ("input_shape", ctypes.c_uint32 * 2),
+        ("states", ctypes.c_uint64), ("inputs", ctypes.c_uint64), ("pairs", ctypes.c_uint64),
+        ("iterations", ctypes.c_uint32), ("converged", ctypes.c_int32), ("message", ctypes.c_int32),
+        ("reachable_states", ctypes.c_uint64), ("certified_candidates", ctypes.c_uint64),
+        ("candidate_count", ctypes.c_uint64), ("valid_count", ctypes.c_uint64),
+    ]
+
+
+class Timings(ctypes.Structure):
+    _fields_ = [
+        ("abstraction_ms", ctypes.c_double), ("prepare_ms", ctypes.c_double), ("solve_ms", ctypes.c_double),
+        ("readback_ms", ctypes.c_double), ("device_bytes", ctypes.c_uint64), ("method", ctypes.c_uint32),
+        ("kernel_launches", ctypes.c_uint32),
+    ]
+
+
+# Every symbol include/gsc_b200.h declares, with its ctypes signature.
+_P = ctypes.c_void_p
+SIGNATURES = {
+    "gsc_cuda_backend_compiled": (ctypes.c_int, []),
+    "gsc_abi_version": (ctypes.c_int, []),
+    "gsc_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+    "gsc_message_string": (ctypes.c_char_p, [ctypes.c_int]),
+    "gsc_grid_shape": (ctypes.c_int, [ctypes.POINTER(ModelDesc), _P, _P]),
+    "gsc_context_create": (ctypes.c_int, [ctypes.c_int, _P, ctypes.POINTER(_P)]),
+    "gsc_context_destroy": (None, [_P]),
+    "gsc_last_error": (ctypes.c_char_p, [_P]),
+    "gsc_context_set_memory_budget": (ctypes.c_int, [_P, ctypes.c_uint64]),
+    "gsc_context_memory_in_use": (ctypes.c_uint64, [_P]),
+    "gsc_abstraction_create": (ctypes.c_int, [_P, ctypes.POINTER(ModelDesc), ctypes.POINTER(_P)]),
+    "gsc_abstraction_destroy": (None, [_P]),
+    "gsc_problem_create": (ctypes.c_int, [_P, _P, ctypes.POINTER(QueryDesc), ctypes.c_uint32, ctypes.POINTER(_P)]),
+    "gsc_problem_destroy": (None, [_P]),
+    "gsc_problem_solve": (ctypes.c_int, [_P, ctypes.c_uint32]),
+    "gsc_problem_read": (ctypes.c_int, [_P, ctypes.POINTER(Result)]),
+    "gsc_problem_export_abstraction": (ctypes.c_int, [_P, _P, _P, _P]),
+    "gsc_problem_timings": (ctypes.c_int, [_P, ctypes.POINTER(Timings)]),
+    "gsc_run_case": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ModelDesc), ctypes.POINTER(QueryDesc),
+                                    ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(Result),
+                                    ctypes.POINTER(Timings)]),
+}
+
+_lib = None
+
+
+def lib():
+    """Load libgsc_b200.so; raises when it was not built (no fallback path)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `make -C {HERE}`")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def cuda_backend_compiled() -> bool:
+    return bool(lib().gsc_cuda_backend_compiled())
+
+
+def _ptr(a):
+    return ctypes.c_void_p(a.ctypes.data) if a is not None else None
+
+
+def model_desc(case) -> ModelDesc:
+    m = ModelDesc()
+    m.state_lb[:] = [float(v) for v in case["state_lb"]]
+    m.state_ub[:] = [float(v) for v in case["state_ub"]]
+    m.state_eta[:] = [float(v) for v in case["state_eta"]]
+    m.wrap_dim = int(case.get("wrap_dim", 2))
+    m.input_lb[:] = [float(v) for v in case["input_lb"]]
+    m.input_ub[:] = [float(v) for v in case["input_ub"]]
+    m.input_eta[:] = [float(v) for v in case["input_eta"]]
+    m.sample_time = float(case["sample_time"])
+    m.integration_substeps = int(case["integration_substeps"])
+    return m
+
+
+class _Query:
+    """A QueryDesc plus the host arrays it points to (kept alive with it)."""
+
+    def __init__(self, case, safe_mask=None, safe_rank=0, valid_mask=None, candidate_mask=None):
+        q = QueryDesc()
+        q.disturbance_half_width[:] = [float(v) for v in case["disturbance_half_width"]]
+        q.constraint_kind = CONSTRAINTS[case.get("constraint", "none")]
+        cp = list(case.get("constraint_params", [0.0] * 4)) + [0.0] * 4
+        q.constraint_params[:] = [float(v) for v in cp[:4]]
+        q.map_lb[:] = [float(v) for v in case.get("map_lb", case["state_lb"])]
+        q.map_ub[:] = [float(v) for v in case.get("map_ub", case["state_ub"])]
+        obs = case.get("obstacles", [])
+        self.obstacles = np.ascontiguousarray(np.array(obs, dtype=np.float64).reshape(-1, 8)) if obs else None
+        q.obstacle_count = len(obs)
+        q.obstacles = _ptr(self.obstacles)
+        if case.get("candidate", "rect") == "rect":
+            q.candidate_kind = 0
+            q.candidate[:] = [float(v) for v in list(case["candidate_lb"]) + list(case["candidate_ub"])]
+        else:
+            q.candidate_kind = 1
+            e = list(case["candidate_ellipse"]) + [0.0] * 8
+            q.candidate[:] = [float(v) for v in e[:8]]
+        q.max_iterations = int(case["max_iterations"])
+        self.safe = np.ascontiguousarray(safe_mask, dtype=np.uint8) if safe_mask is not None else None
+        self.valid = np.ascontiguousarray(valid_mask, dtype=np.uint8) if valid_mask is not None else None
+        self.cand = np.ascontiguousarray(candidate_mask, dtype=np.uint8) if candidate_mask is not None else None
+        q.safe_mask = _ptr(self.safe)
+        q.safe_mask_rank = int(safe_rank) if self.safe is not None else 0
+        q.valid_mask = _ptr(self.valid)
+        q.candidate_mask = _ptr(self.cand)
+        self.desc = q
+
+
+def grid_shape(case):
+    s = (ctypes.c_uint32 * 4)()
+    u = (ctypes.c_uint32 * 2)()
+    m = model_desc(case)
+    st = lib().gsc_grid_shape(ctypes.byref(m), s, u)
+    if st != 0:
+        raise GscError(st)
+    return tuple(s), tuple(u)
+
+
+class Context:
+    def __init__(self, device=0, stream=None):
+        self._h = ctypes.c_void_p()
+        st = lib().gsc_context_create(int(device), ctypes.c_void_p(stream) if stream else None, ctypes.byref(self._h))
+        if st != 0:
+            raise GscError(st)
+
+    def error(self):
+        return lib().gsc_last_error(self._h).decode()
+
+    def check(self, st):
+        if st != 0:
+            raise GscError(st, self.error())
+
+    def set_memory_budget(self, nbytes):
+        self.check(lib().gsc_context_set_memory_budget(self._h, int(nbytes)))
+
+    def memory_in_use(self):
+        return int(lib().gsc_context_memory_in_use(self._h))
+
+    def close(self):
+        if self._h:
+            lib().gsc_context_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Abstraction:
+    def __init__(self, ctx: Context, case):
+        self.ctx = ctx
+        self._h = ctypes.c_void_p()
+        self.model = model_desc(case)
+        ctx.check(lib().gsc_abstraction_create(ctx._h, ctypes.byref(self.model), ctypes.byref(self._h)))
+
+    def close(self):
+        if self._h:
+            lib().gsc_abstraction_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Problem:
+    def __init__(self, ctx: Context, abs_: Abstraction, case, method=METHOD_AUTO, **masks):
+        self.ctx = ctx
+        self.abs = abs_
+        self._h = ctypes.c_void_p()
+        self.query = _Query(case, **masks)
+        ctx.check(lib().gsc_problem_create(ctx._h, abs_._h, ctypes.byref(self.query.desc), int(method),
+                                           ctypes.byref(self._h)))
+
+    def solve(self, graph=False):
+        self.ctx.check(lib().gsc_problem_solve(self._h, SOLVE_GRAPH if graph else 0))
+
+    def timings(self) -> dict:
+        t = Timings()
+        self.ctx.check(lib().gsc_problem_timings(self._h, ctypes.byref(t)))
+        return {k: getattr(t, k) for k, _ in Timings._fields_}
+
+    def read(self, iter_capacity=4096, masks=True) -> dict:
+        r = Result()
+        probe = Result()
+        self.ctx.check(lib().gsc_problem_read(self._h, ctypes.byref(probe)))
+        S = int(probe.states)
+        out = {}
+        if masks:
+            out = {
+                "valid_mask": np.zeros(S, np.uint8), "candidate_mask": np.zeros(S, np.uint8),
+                "reachable_mask": np.zeros(S, np.uint8), "controller": np.zeros(S, np.uint32),
+                "reach_step": np.zeros(S, np.uint32),
+            }
+            for k, v in out.items():
+                setattr(r, k, _ptr(v))
+        nr = np.zeros(iter_capacity, np.uint64)
+        nc = np.zeros(iter_capacity, np.uint64)
+        r.iter_new_reachable = _ptr(nr)
+        r.iter_new_certified = _ptr(nc)
+        r.iter_capacity = iter_capacity
+        self.ctx.check(lib().gsc_problem_read(self._h, ctypes.byref(r)))
+        it = int(r.iterations)
+        out.update({
+            "shape": tuple(r.shape), "input_shape": tuple(r.input_shape), "states": int(r.states),
+            "inputs": int(r.inputs), "pairs": int(r.pairs), "iterations": it, "converged": bool(r.converged),
+            "message": MESSAGES[int(r.message)], "reachable_states": int(r.reachable_states),
+            "certified_candidates": int(r.certified_candidates), "candidate_count": int(r.candidate_count),
+            "valid_count": int(r.valid_count), "iter_new_reachable": nr[:min(it, iter_capacity)].copy(),
+            "iter_new_certified": nc[:min(it, iter_capacity)].copy(),
+        })
+        return out
+
+    def export_abstraction(self):
+        probe = Result()
+        self.ctx.check(lib().gsc_problem_read(self._h, ctypes.byref(probe)))
+        P = int(probe.pairs)
+        mn = np.zeros(P, np.uint32)
+        mx = np.zeros(P, np.uint32)
+        v = np.zeros(P, np.uint8)
+        self.ctx.check(lib().gsc_problem_export_abstraction(self._h, _ptr(mn), _ptr(mx), _ptr(v)))
+        return mn, mx, v
+
+    def close(self):
+        if self._h:
+            lib().gsc_problem_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def run_case(case, method=METHOD_AUTO, graph=False, device=0, iter_capacity=4096, **masks) -> dict:
+    """One-shot run through ``gsc_run_case`` (the run_case_cuda_u32 replacement):
+    host description in, host arrays out."""
+    L = lib()
+    m = model_desc(case)
+    q = _Query(case, **masks)
+    s, u = grid_shape(case)
+    S = int(np.prod(s, dtype=np.uint64))
+    out = {
+        "valid_mask": np.zeros(S, np.uint8), "candidate_mask": np.zeros(S, np.uint8),
+        "reachable_mask": np.zeros(S, np.uint8), "controller": np.zeros(S, np.uint32),
+        "reach_step": np.zeros(S, np.uint32),
+    }
+    r = Result()
+    for k, v in out.items():
+        setattr(r, k, _ptr(v))
+    nr = np.zeros(iter_capacity, np.uint64)
+    nc = np.zeros(iter_capacity, np.uint64)
+    r.iter_new_reachable = _ptr(nr)
+    r.iter_new_certified = _ptr(nc)
+    r.iter_capacity = iter_capacity
+    t = Timings()
+    st = L.gsc_run_case(int(device), ctypes.byref(m), ctypes.byref(q.desc), int(method),
+                        SOLVE_GRAPH if graph else 0, ctypes.byref(r), ctypes.byref(t))
+    if st != 0:
+        raise GscError(st)
+    it = int(r.iterations)
+    out.update({
+        "shape": tuple(r.shape), "input_shape": tuple(r.input_shape), "states": int(r.states),
+        "inputs": int(r.inputs), "pairs": int(r.pairs), "iterations": it, "converged": bool(r.converged),
+        "message": MESSAGES[int(r.message)], "reachable_states": int(r.reachable_states),
+        "certified_candidates": int(r.certified_candidates), "candidate_count": int(r.candidate_count),
+        "valid_count": int(r.valid_count), "iter_new_reachable": nr[:min(it, iter_capacity)].copy(),
+        "iter_new_certified": nc[:min(it, iter_capacity)].copy(),
+        "timings": {k: getattr(t, k) for k, _ in Timings._fields_},
+    })
+    return out

@@ -1,0 +1,228 @@
+/*
+ * gsc_b200.h -- C ABI of the B200 (sm_100a) grid symbolic-control library.
+ *
+ * The reference (zzx-ur/gpu-inner-outer, namespace gsc) exposes its CUDA
+ * backend as two C++ functions, include/gsc/cuda_api.hpp:87-88:
+ *
+ *     bool gsc::cuda_backend_compiled();
+ *     gsc::GpuRunReport gsc::run_case_cuda_u32(const gsc::CaseConfig&);
+ *
+ * run_case_cuda_u32 (cuda/kernels.cu:492-875) builds the masks on the host,
+ * launches abstraction_kernel (:164-217), then loops over fixpoint iterations
+ * (:654-767) of build_prefix_on_device (:403-484), pair_satisfaction_kernel
+ * (:310-336) and reduce_inputs_kernel (:338-393), and copies everything back.
+ *
+ * This header splits that call into device-resident stages behind plain C
+ * types (no C++ or torch types cross the boundary):
+ *
+ *   gsc_abstraction_*  the dynamics part of abstraction_kernel: nominal Euler
+ *                      successors of every (cell, input), kept on the device;
+ *   gsc_problem_*      one K-invariance query against a resident abstraction:
+ *                      masks, quantised successor boxes, and the fixpoint;
+ *   gsc_run_case       the whole reference call in one step.
+ *
+ * Every entry point returns a gsc_status.  Results go to caller-provided host
+ * buffers.  Device memory is owned by the handles.  There is no CPU fallback:
+ * without a usable CUDA device the calls fail with GSC_ERR_NO_DEVICE.
+ */
+#ifndef GSC_B200_H
+#define GSC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GSC_B200_ABI_VERSION 1
+
+typedef enum {
+    GSC_OK = 0,
+    GSC_ERR_INVALID_ARGUMENT = 1,   /* bad grid, bad pointer, bad option          */
+    GSC_ERR_CUDA = 2,               /* a CUDA runtime call failed                 */
+    GSC_ERR_OUT_OF_MEMORY = 3,      /* device allocation failed or over budget    */
+    GSC_ERR_UNSUPPORTED = 4,        /* valid input outside what a method handles  */
+    GSC_ERR_NO_DEVICE = 5,          /* no CUDA device (kernels.cu:497-502)        */
+    GSC_ERR_CANDIDATE_INVALID = 6,  /* candidate set contains invalid states
+                                       (abstraction.hpp:268-272)                  */
+    GSC_ERR_TIMEOUT = 7             /* a bounded device-side wait ran out         */
+} gsc_status;
+
+/* Fixpoint outcome, reachability.hpp:133-152 (messages kept verbatim by
+ * gsc_message_string). */
+enum {
+    GSC_MSG_NONE = 0,
+    GSC_MSG_CONVERGED = 1,          /* "all candidate states obtained a controller"  */
+    GSC_MSG_STALLED = 2,            /* "iteration stalled before candidate closure"  */
+    GSC_MSG_MAX_ITERATIONS = 3      /* "maximum iterations reached"                  */
+};
+
+/* State constraint kinds: ConstraintType (config.hpp:19-24) plus the quadric
+ * safe set (x*x)*qa - (y*y)*qb <= c && fabs(y) <= ymax, which the reference can
+ * only state as kCustom. */
+enum {
+    GSC_CONSTRAINT_NONE = 0,        /* params unused                              */
+    GSC_CONSTRAINT_HYPERBOLIC = 1,  /* a, b, c: x^2 - y^2 <= a && b*y^2 - x^2 <= c */
+    GSC_CONSTRAINT_ELLIPTIC = 2,    /* a, b: (x/a)^2 + (y/b)^2 <= 1                */
+    GSC_CONSTRAINT_QUADRIC = 3      /* qa, qb, c, ymax                             */
+};
+
+enum {
+    GSC_CANDIDATE_RECT = 0,         /* candidate[0..3] lb, [4..7] ub, inclusive     */
+    GSC_CANDIDATE_ELLIPSE = 1       /* cx, cy, wx, wy, r2; intersected with valid  */
+};
+
+/* Solve methods.  Both give bit-identical results. */
+enum {
+    GSC_METHOD_AUTO = 0,            /* FUSED when it applies, else STORED          */
+    GSC_METHOD_STORED = 1,          /* per-pair int32 index boxes in HBM, int32 4-D
+                                       prefix scan, 16-corner box count            */
+    GSC_METHOD_FUSED = 2            /* boxes recomputed from per-axis tables inside
+                                       the satisfaction kernel, bit-sliced sets    */
+};
+
+/* Solve flags. */
+enum {
+    GSC_SOLVE_GRAPH = 1u << 0       /* run the fixpoint as one CUDA graph with a
+                                       device-side while condition                 */
+};
+
+/* The grid and dynamics (CaseConfig fields that the successor boxes' nominal
+ * part depends on, config.hpp:41-66; grids grid.hpp:103-168; model
+ * model.hpp:8-112). */
+typedef struct {
+    double state_lb[4];
+    double state_ub[4];
+    double state_eta[4];
+    int32_t wrap_dim;               /* must be 2 (theta), as in all reference cases */
+    double input_lb[2];
+    double input_ub[2];
+    double input_eta[2];
+    double sample_time;
+    uint32_t integration_substeps;
+} gsc_model_desc;
+
+/* One K-invariance query (the rest of CaseConfig). */
+typedef struct {
+    double disturbance_half_width[4];
+    int32_t constraint_kind;
+    double constraint_params[4];
+    double map_lb[4];
+    double map_ub[4];
+    uint32_t obstacle_count;
+    const double* obstacles;        /* obstacle_count x {lb[4], ub[4]}            */
+    int32_t candidate_kind;
+    double candidate[8];
+    uint32_t max_iterations;
+    /* Optional host masks replacing the ones built from the description above
+     * (NULL = build on the device).  safe_mask is the state constraint
+     * evaluated at cell centres: rank 2 = [ny][nx] over (x, y), rank 4 = one
+     * byte per state.  A custom constraint (ConstraintType::kCustom) is passed
+     * this way. */
+    const uint8_t* safe_mask;
+    int32_t safe_mask_rank;
+    const uint8_t* valid_mask;      /* one byte per state                         */
+    const uint8_t* candidate_mask;  /* one byte per state                         */
+} gsc_query_desc;
+
+/* Outputs.  Buffers are caller-owned host memory; any may be NULL. */
+typedef struct {
+    uint8_t* valid_mask;            /* [states]                                   */
+    uint8_t* candidate_mask;        /* [states]                                   */
+    uint8_t* reachable_mask;        /* [states]                                   */
+    uint32_t* controller;           /* [states], 0xFFFFFFFF = none (types.hpp:22)  */
+    uint32_t* reach_step;           /* [states], 0xFFFFFFFF = unreachable         */
+    uint64_t* iter_new_reachable;   /* [iter_capacity]                            */
+    uint64_t* iter_new_certified;   /* [iter_capacity]                            */
+    uint32_t iter_capacity;
+    /* Filled by the library. */
+    uint32_t shape[4];
+    uint32_t input_shape[2];
+    uint64_t states;
+    uint64_t inputs;
+    uint64_t pairs;
+    uint32_t iterations;
+    int32_t converged;
+    int32_t message;                /* GSC_MSG_*                                  */
+    uint64_t reachable_states;
+    uint64_t certified_candidates;
+    uint64_t candidate_count;
+    uint64_t valid_count;
+} gsc_result;
+
+/* Device timings of the last solve, CUDA events on the library's stream. */
+typedef struct {
+    double abstraction_ms;          /* gsc_abstraction_create kernels             */
+    double prepare_ms;              /* masks + boxes (gsc_problem_create)         */
+    double solve_ms;                /* the fixpoint                               */
+    double readback_ms;             /* gsc_problem_read copies                    */
+    uint64_t device_bytes;          /* device memory held by the problem          */
+    uint32_t method;                /* method actually used                       */
+    uint32_t kernel_launches;       /* kernels launched by the last solve         */
+} gsc_timings;
+
+typedef struct gsc_context gsc_context;
+typedef struct gsc_abstraction gsc_abstraction;
+typedef struct gsc_problem gsc_problem;
+
+/* Replaces gsc::cuda_backend_compiled() (cuda_api.hpp:87). */
+int gsc_cuda_backend_compiled(void);
+
+int gsc_abi_version(void);
+const char* gsc_status_string(int status);
+/* reachability.hpp:135,140,151 */
+const char* gsc_message_string(int message);
+
+/* Grid shapes exactly as build_state_grid / build_input_grid
+ * (grid.hpp:103-168): shape = (uint32_t)ceil(width / eta). */
+int gsc_grid_shape(const gsc_model_desc* model, uint32_t shape[4], uint32_t input_shape[2]);
+
+/* A context binds a device and a stream (NULL stream = a private stream).
+ * Mirrors the device checks of kernels.cu:496-502. */
+int gsc_context_create(int device, void* cuda_stream, gsc_context** out);
+void gsc_context_destroy(gsc_context* ctx);
+const char* gsc_last_error(const gsc_context* ctx);
+/* Device memory the context may hold in problems and abstractions (0 = no
+ * limit).  Creation fails with GSC_ERR_OUT_OF_MEMORY beyond it. */
+int gsc_context_set_memory_budget(gsc_context* ctx, uint64_t bytes);
+uint64_t gsc_context_memory_in_use(const gsc_context* ctx);
+
+/* The nominal successor tables of abstraction_kernel (kernels.cu:164-217,
+ * model.hpp:26-46) for every (cell, input), built once and kept resident. */
+int gsc_abstraction_create(gsc_context* ctx, const gsc_model_desc* model, gsc_abstraction** out);
+void gsc_abstraction_destroy(gsc_abstraction* abs);
+
+/* Prepare a query: masks (abstraction.hpp:65-106), quantised successor boxes
+ * with constraint and bounds validity (abstraction.hpp:161-209,
+ * grid.hpp:181-251), and the fixpoint state (reachability.hpp:36-51).
+ * method = GSC_METHOD_*. */
+int gsc_problem_create(gsc_context* ctx, const gsc_abstraction* abs, const gsc_query_desc* query,
+                       uint32_t method, gsc_problem** out);
+void gsc_problem_destroy(gsc_problem* p);
+
+/* Run the fixpoint (kernels.cu:650-767 / reachability.hpp:53-153) on the
+ * device.  Resets the fixpoint state first, so a problem can be solved again.
+ * Stream-ordered; returns after enqueueing unless the host-driven loop needs
+ * to read the stop flag (flags without GSC_SOLVE_GRAPH). */
+int gsc_problem_solve(gsc_problem* p, uint32_t flags);
+
+/* Copy the results into caller buffers (kernels.cu:776-832).  Synchronises. */
+int gsc_problem_read(gsc_problem* p, gsc_result* out);
+
+/* The reference's abstraction arrays (cuda_api.hpp:82-84: min_flat, max_flat,
+ * valid; pair = state * inputs + input), produced on demand.  Synchronises. */
+int gsc_problem_export_abstraction(gsc_problem* p, uint32_t* min_flat, uint32_t* max_flat, uint8_t* valid);
+
+int gsc_problem_timings(const gsc_problem* p, gsc_timings* out);
+
+/* Replaces gsc::run_case_cuda_u32 (cuda_api.hpp:88, kernels.cu:492-875):
+ * abstraction, query, fixpoint and readback in one call on `device`. */
+int gsc_run_case(int device, const gsc_model_desc* model, const gsc_query_desc* query, uint32_t method,
+                 uint32_t flags, gsc_result* out, gsc_timings* timings);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GSC_B200_H */
