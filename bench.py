@@ -1,0 +1,377 @@
+#!/usr/bin/env python
+"""Benchmark of the grid symbolic-control fixpoint on B200.
+
+Metric: nominal pair-checks per second = states x inputs x iterations / fixpoint
+time (the reference tests every pair every iteration, cuda/kernels.cu:668), on
+the 65x65x38x25-state x 10x10-input unicycle workload (seeded synthetic grid,
+no dataset).  One step = one full backward-reachability fixpoint from the
+candidate set, with the abstraction and masks resident in HBM.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Under torchrun (N > 1) every rank solves its own replica of the workload
+(independent K-invariance queries shard without any exchange), the step time is
+the max over ranks, and value = the pair-checks of all ranks / that time.
+
+`--impl reference` times the reference's own CPU method (oracle/_ref/gsc_ref,
+compiled from its sources) on the host cores, on a seeded sample of states of
+the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "gpu-inner-outer_b200")
+ORACLE = os.path.join(ROOT, "oracle")
+sys.path.insert(0, PKG)
+
+import gsc_cases as C  # noqa: E402
+
+REF_BIN = os.path.join(ORACLE, "_ref", "gsc_ref")
+PUBLISHED_DEMO_SOLVE_MS = 214.936   # README.md:69, RTX 4090, 12 iterations
+PUBLISHED_DEMO_PAIRS = 401310000
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(C.PRESETS), default="demo_scale")
+    ap.add_argument("--method", choices=["auto", "stored", "fused"], default="auto")
+    ap.add_argument("--cpu-sample-states", type=int, default=160000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    return ap.parse_args()
+
+
+# ---- CPU: the reference's own method on a sample of states ------------------------------
+
+def reference_sample(case, n_states, seed, threads):
+    """One run of `gsc_ref sample`: the reference's abstraction rows and
+    iteration-1 state bodies for n_states seeded states, split over threads.
+    Returns the nominal pair-checks/s of a full fixpoint iteration, computed as
+    states x inputs / (prefix build + per-state loop scaled to all states)."""
+    sys.path.insert(0, ORACLE)
+    import oracle as O
+
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "case.bin")
+        with open(path, "wb") as f:
+            f.write(bytes(O.to_struct(case)))
+        out = subprocess.run([REF_BIN, "sample", path, str(n_states), str(seed), str(threads)], check=True,
+                             capture_output=True, text=True).stdout
+    line = [ln for ln in out.splitlines() if ln.startswith("SAMPLE")][0]
+    kv = dict(t.split("=") for t in line.split()[1:])
+    S, M = int(kv["grid_states"]), int(kv["inputs"])
+    n = int(kv["states"])
+    iter_ms = float(kv["prefix_ms"]) + float(kv["iteration_ms"]) * S / n
+    full_ms = iter_ms + float(kv["abstraction_ms"]) * S / n
+    return {
+        "pair_checks_per_s": S * M / (iter_ms * 1e-3),
+        "iteration_ms_full_grid": iter_ms,
+        "abstraction_plus_iteration_ms_full_grid": full_ms,
+        "sample_states": n,
+        "threads": threads,
+        "raw": kv,
+    }
+
+
+def cpu_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def run_reference_arm(args, case):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    metric = "fixpoint pair-checks/s"
+    if not os.path.exists(REF_BIN):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/gsc_ref was not built"}))
+        return
+    threads = cpu_threads()
+    vals = []
+    for i in range(args.warmup + args.steps):
+        r = reference_sample(case, args.cpu_sample_states, 1000 + i, threads)
+        if i >= args.warmup:
+            vals.append(r)
+    v = statistics.median(x["pair_checks_per_s"] for x in vals)
+    it_ms = statistics.median(x["iteration_ms_full_grid"] for x in vals)
+    S, M = C.grid_shape(case)
+    sample = (f"{args.cpu_sample_states} seeded states per step of the {case['name']} grid: the reference's "
+              f"abstraction rows and iteration-1 bodies (abstraction.hpp:168-208, reachability.hpp:59-109) on "
+              f"{threads} threads, plus one full-grid build_prefix_sum_cpu; scaled to all states")
+    line = {
+        "impl": "reference", "metric": metric, "value": v, "unit": "pair-checks/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": it_ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+        "config": {"workload": case["name"], "states": vals[0]["raw"]["grid_states"],
+                   "inputs": vals[0]["raw"]["inputs"], "sample": sample},
+        "cpu_baseline": {"value": v, "unit": "pair-checks/s", "cores": threads, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": v, "unit": "pair-checks/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+# ---- GPU --------------------------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid):
+        self.uuid = uuid
+        self.lines = []
+        self.proc = None
+
+    def __enter__(self):
+        cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100"]
+        if self.uuid:
+            cmd += ["-i", self.uuid]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        time.sleep(0.15)
+        return self
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.15)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel, workload):
+    """DRAM bytes per launch of `kernel` on `workload` from a committed ncu
+    summary (profiles/*.txt lines 'traffic kernel=<k> workload=<w> bytes_per_launch=<n>')."""
+    pdir = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(pdir):
+        return None
+    for fn in sorted(os.listdir(pdir)):
+        if not fn.endswith((".txt", ".md")):
+            continue
+        with open(os.path.join(pdir, fn)) as f:
+            for ln in f:
+                if ln.startswith("traffic ") and f"kernel={kernel} " in ln and f"workload={workload} " in ln:
+                    for tok in ln.split():
+                        if tok.startswith("bytes_per_launch="):
+                            return float(tok.split("=")[1])
+    return None
+
+
+def algorithmic_bytes(method, g, timings):
+    """Bytes one satisfaction launch must move, from the counters of a profiled
+    solve.  stored: 8 B per streamed (state, input) box + valid, candidate,
+    reachable (1 B each) and controller (4 B) per state.  fused: the x and y
+    box-table rows of every processed (slice, input) plane task (4 B per entry)
+    + four passes over the bit-sliced sets (active, previous and next reachable,
+    D') per launch."""
+    n0, n1, n2, n3 = g["shape"]
+    S = n0 * n1 * n2 * n3
+    L = max(timings["sat_launches"], 1)
+    if method == 1:
+        return (8.0 * timings["pair_tests"] + 7.0 * S * L) / L
+    W = (n0 + 63) // 64
+    words = n1 * n2 * n3 * W
+    return (4.0 * (n0 + n1) * timings["aux_count"] + 32.0 * words * L) / L
+
+
+def main():
+    args = parse()
+    case = C.checked(C.PRESETS[args.workload]())
+    if args.impl == "reference":
+        run_reference_arm(args, case)
+        return
+
+    import numpy as np
+    import torch
+    import gsc_b200 as G
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    method = {"auto": G.METHOD_AUTO, "stored": G.METHOD_STORED, "fused": G.METHOD_FUSED}[args.method]
+
+    ctx = G.Context(local, stream.cuda_stream)
+    absn = G.Abstraction(ctx, case)
+    prob = G.Problem(ctx, absn, case, method)
+    shape, ishape = G.grid_shape(case)
+    S = int(np.prod(shape))
+    M = ishape[0] * ishape[1]
+    P = S * M
+
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)   # > 126 MB L2
+    for _ in range(args.warmup):
+        flush.fill_(1)
+        prob.solve(graph=True)
+    torch.cuda.synchronize(dev)
+    iters = prob.timings()["iterations"]
+
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:
+        pass
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    launches = 0
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    with ClockSampler(uuid) as clocks:
+        t_wall = time.perf_counter()
+        for k in range(args.steps):
+            flush.fill_(k & 0xFF)
+            evs[k][0].record(stream)
+            prob.solve(graph=True)
+            evs[k][1].record(stream)
+            launches += prob.timings()["kernel_launches"]
+        torch.cuda.synchronize(dev)
+        t_wall = time.perf_counter() - t_wall
+    if dist:
+        dist.barrier()
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    total_ms = sum(step_ms)
+    if dist:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    value = world * P * iters / (ms_per_step * 1e-3)
+
+    # Dominant kernel: one profiled solve (events around each satisfaction launch).
+    prob.solve(profile=True)
+    tp = prob.timings()
+    used = tp["method"]
+    kname = "k_sat_stored" if used == G.METHOD_STORED else "k_sat_fused"
+    per_launch_ms = tp["sat_kernel_ms"] / max(tp["sat_launches"], 1)
+    alg = algorithmic_bytes(used, {"shape": shape}, tp)
+    peak, peak_kind = measured_peak()
+    achieved = alg / (per_launch_ms * 1e-3) / 1e9
+    traffic = ncu_traffic(kname, case["name"])
+
+    # End to end through the public one-shot call: host description in, pinned host arrays out.
+    e2e_ms = []
+    pin = {k: torch.empty(S * sz, dtype=torch.uint8, pin_memory=True)
+           for k, sz in (("valid_mask", 1), ("candidate_mask", 1), ("reachable_mask", 1), ("controller", 4),
+                         ("reach_step", 4))}
+    outs = {k: (v.numpy() if k.endswith("mask") else v.numpy().view(np.uint32)) for k, v in pin.items()}
+    for k in range(args.e2e_steps + 1):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        r = G.run_case(case, method=method, graph=True, device=local, out=outs)
+        torch.cuda.synchronize(dev)
+        if k > 0:
+            e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    e2e_step = statistics.median(e2e_ms)
+    if dist:
+        t = torch.tensor([e2e_step], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_step = float(t.item())
+    K = case["integration_substeps"]
+    h2d = 8 * (2 * shape[2] * ishape[1] * K + shape[3] * ishape[0] * K + shape[2] * ishape[1] +
+               shape[3] * ishape[0]) + 64 * len(case.get("obstacles", []))
+    d2h = 11 * S + 16 * r["iterations"]
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(REF_BIN):
+        threads = cpu_threads()
+        rs = reference_sample(case, args.cpu_sample_states, 7, threads)
+        cpu = {"value": rs["pair_checks_per_s"], "unit": "pair-checks/s", "cores": threads, "kind": "reference",
+               "sample": f"{args.cpu_sample_states} seeded states of the same grid, the reference's "
+                         f"iteration-1 state bodies on {threads} threads plus one full-grid prefix build, "
+                         f"scaled to all states"}
+
+    vs = None
+    if args.workload == "hyperbolic_demo":
+        vs = value / (PUBLISHED_DEMO_PAIRS * 12 / (PUBLISHED_DEMO_SOLVE_MS * 1e-3))
+    line = {
+        "metric": "fixpoint pair-checks/s", "value": value, "unit": "pair-checks/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": vs, "dtype": "u64 bit-sliced sets / int32 counts (f64 boxes)",
+        "data": "synthetic",
+        "config": {"workload": case["name"], "states": S, "inputs": M, "pairs": P, "iterations": iters,
+                   "method": {1: "stored", 2: "fused"}[used], "fixpoint_ms": ms_per_step,
+                   "l2": "flushed before every step (256 MiB write)", "wall_s": t_wall,
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic, "kernel": kname,
+                     "kernel_ms_per_launch": per_launch_ms, "algorithmic_bytes_per_launch": alg,
+                     "peak_kind": peak_kind},
+        "cpu_baseline": cpu,
+        "e2e": {"value": world * P * r["iterations"] / (e2e_step * 1e-3), "unit": "pair-checks/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_step},
+        "gpu_launches": launches,
+        "clocks": clocks.summary(),
+    }
+    if rank == 0:
+        print(json.dumps(line))
+    prob.close()
+    absn.close()
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

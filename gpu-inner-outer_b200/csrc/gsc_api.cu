@@ -68,6 +68,8 @@ struct gsc_problem {
     // fused
     uint64_t *validb = nullptr, *unsafeb = nullptr, *srcb = nullptr, *candb = nullptr, *dp = nullptr;
     uint64_t *reach0 = nullptr, *reach1 = nullptr, *active = nullptr;
+    uint64_t* xcls = nullptr;
+    uint32_t ez_rows = 0;
     int need_valid = 0;
     // common fixpoint state
     uint32_t* controller = nullptr;
@@ -503,6 +505,25 @@ int build_problem(gsc_problem* p, const gsc_query_desc* qd, uint32_t method) {
     p->valid_count = hc[0];
     p->candidate_count = hc[1];
     if (hflags != 0) fused_ok = false;   // an empty or over-wide interval: only the stored count is exact
+    // The fused kernel stages, per v cell, every v row its inputs can reach.
+    {
+        std::vector<uint32_t> hw(static_cast<size_t>(g.n[3]) * g.ma);
+        GSC_CU(ctx, cudaMemcpy(hw.data(), p->wt, hw.size() * 4, cudaMemcpyDeviceToHost));
+        uint32_t rows = 1;
+        for (uint32_t i3 = 0; i3 < g.n[3]; ++i3) {
+            int lo = 1 << 30, hi = -1;
+            for (uint32_t ja = 0; ja < g.ma; ++ja) {
+                const uint32_t we = hw[static_cast<size_t>(i3) * g.ma + ja];
+                if (we == kReject) continue;
+                lo = std::min(lo, static_cast<int>(lo16(we)));
+                hi = std::max(hi, static_cast<int>(hi16(we)));
+            }
+            if (hi >= lo) rows = std::max<uint32_t>(rows, static_cast<uint32_t>(hi - lo + 1));
+        }
+        p->ez_rows = rows;
+        const int nv = p->safe ? (hc[4] != 0) : (hc[0] != g.S);
+        if (fused_smem_bytes(g, rows, class_words(g), nv) > kFusedSmemMax) fused_ok = false;
+    }
     if (method == GSC_METHOD_AUTO) method = fused_ok ? GSC_METHOD_FUSED : (stored_ok ? GSC_METHOD_STORED : 0);
     if (method == 0) return fail(ctx, GSC_ERR_UNSUPPORTED, "no method applies to this grid");
     if (method == GSC_METHOD_FUSED && !fused_ok)
@@ -519,7 +540,7 @@ int build_problem(gsc_problem* p, const gsc_query_desc* qd, uint32_t method) {
     GSC_TRY(dalloc(ctx, A, B, &p->controller, g.S));
     GSC_TRY(dalloc(ctx, A, B, &p->reach_step, g.S));
     GSC_TRY(dalloc(ctx, A, B, &p->fc, 1));
-    GSC_TRY(dalloc(ctx, A, B, &p->stats, 2ull * p->stats_cap));
+    GSC_TRY(dalloc(ctx, A, B, &p->stats, static_cast<uint64_t>(kStatsCols) * p->stats_cap));
     GSC_TRY(dalloc(ctx, A, B, &p->reach8, g.S));
 
     if (method == GSC_METHOD_STORED) {
@@ -562,6 +583,8 @@ int build_problem(gsc_problem* p, const gsc_query_desc* qd, uint32_t method) {
         GSC_TRY(dalloc(ctx, A, B, &p->reach0, words));
         GSC_TRY(dalloc(ctx, A, B, &p->reach1, words));
         GSC_TRY(dalloc(ctx, A, B, &p->active, words));
+        GSC_TRY(dalloc(ctx, A, B, &p->xcls, static_cast<uint64_t>(g.slices) * g.M * class_words(g)));
+        GSC_CU(ctx, launch_x_classes(g, p->xt, p->xcls, st));
         GSC_CU(ctx, launch_pack_bits(g, 0, p->valid, nullptr, p->validb, st));
         GSC_CU(ctx, launch_pack_bits(g, 0, p->cand, nullptr, p->candb, st));
         if (!p->safe) {
@@ -617,6 +640,9 @@ FusedFixArgs fused_args(gsc_problem* p, cudaGraphConditionalHandle cond, int use
     a.fc = p->fc;
     a.stats = p->stats;
     a.need_valid = p->need_valid;
+    a.xcls = p->xcls;
+    a.cls_words = class_words(p->g);
+    a.ez_rows = p->ez_rows;
     a.cond = cond;
     a.use_cond = use_cond;
     return a;
@@ -630,10 +656,11 @@ cudaError_t enqueue_init(gsc_problem* p) {
     return launch_fused_init(p->g, fused_args(p, 0, 0), p->cand, st);
 }
 
-cudaError_t enqueue_iteration(gsc_problem* p, cudaGraphConditionalHandle cond, int use_cond, uint32_t* launches) {
+cudaError_t enqueue_iteration(gsc_problem* p, cudaGraphConditionalHandle cond, int use_cond, uint32_t* launches,
+                              cudaEvent_t* ev = nullptr) {
     if (p->method == GSC_METHOD_STORED)
-        return launch_stored_iteration(p->g, stored_args(p, cond, use_cond), p->ctx->stream, launches);
-    return launch_fused_iteration(p->g, fused_args(p, cond, use_cond), p->ctx->stream, launches);
+        return launch_stored_iteration(p->g, stored_args(p, cond, use_cond), p->ctx->stream, launches, ev);
+    return launch_fused_iteration(p->g, fused_args(p, cond, use_cond), p->ctx->stream, launches, ev);
 }
 
 // Outer graph: [init kernels] -> while (condition) { one iteration }.  The
@@ -717,10 +744,33 @@ int gsc_problem_solve(gsc_problem* p, uint32_t flags) {
     cudaStream_t st = ctx->stream;
     GSC_CU(ctx, cudaEventRecord(ctx->ev[0], st));
     uint32_t launches = 0;
-    if (flags & GSC_SOLVE_GRAPH) {
+    double sat_ms = 0.0, scan_ms = 0.0;
+    uint32_t sat_launches = 0;
+    const uint32_t per_iter = (p->method == GSC_METHOD_STORED) ? 6 : 3;
+    if (flags & GSC_SOLVE_PROFILE) {
+        GSC_CU(ctx, enqueue_init(p));
+        launches += 2;
+        cudaEvent_t ev[3];
+        for (auto& e : ev) GSC_CU(ctx, cudaEventCreate(&e));
+        FixControl hfc;
+        cudaError_t err = cudaSuccess;
+        while (err == cudaSuccess) {
+            err = enqueue_iteration(p, 0, 0, &launches, ev);
+            if (err == cudaSuccess) err = cudaMemcpyAsync(&hfc, p->fc, sizeof(hfc), cudaMemcpyDeviceToHost, st);
+            if (err == cudaSuccess) err = cudaStreamSynchronize(st);
+            float a = 0.f, b = 0.f;
+            if (err == cudaSuccess) err = cudaEventElapsedTime(&a, ev[0], ev[1]);
+            if (err == cudaSuccess) err = cudaEventElapsedTime(&b, ev[1], ev[2]);
+            scan_ms += a;
+            sat_ms += b;
+            ++sat_launches;
+            if (hfc.stop) break;
+        }
+        for (auto& e : ev) cudaEventDestroy(e);
+        GSC_CU(ctx, err);
+    } else if (flags & GSC_SOLVE_GRAPH) {
         if (!p->exec) GSC_TRY(build_graph(p));
         GSC_CU(ctx, cudaGraphLaunch(p->exec, st));
-        launches = 0;   // counted by the caller from the iteration count
     } else {
         GSC_CU(ctx, enqueue_init(p));
         launches += 2;
@@ -742,7 +792,29 @@ int gsc_problem_solve(gsc_problem* p, uint32_t flags) {
     float ms = 0.f;
     GSC_CU(ctx, cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));
     p->timings.solve_ms = ms;
+    // Iteration count and per-iteration counters of this solve.
+    FixControl hfc;
+    GSC_CU(ctx, cudaMemcpyAsync(&hfc, p->fc, sizeof(hfc), cudaMemcpyDeviceToHost, st));
+    GSC_CU(ctx, cudaStreamSynchronize(st));
+    std::vector<unsigned long long> hs(static_cast<size_t>(kStatsCols) * (hfc.iter + 1));
+    GSC_CU(ctx, cudaMemcpyAsync(hs.data(), p->stats, hs.size() * 8, cudaMemcpyDeviceToHost, st));
+    GSC_CU(ctx, cudaStreamSynchronize(st));
+    uint64_t tests = 0, aux = 0;
+    for (uint32_t i = 1; i <= hfc.iter; ++i) {
+        tests += hs[kStatsCols * i + 2];
+        aux += hs[kStatsCols * i + 3];
+    }
+    p->timings.iterations = hfc.iter;
+    p->timings.pair_tests = tests;
+    p->timings.aux_count = aux;
+    if (flags & GSC_SOLVE_GRAPH && !(flags & GSC_SOLVE_PROFILE))
+        launches = 2 + per_iter * std::max<uint32_t>(hfc.iter, 1);   // init child graph + loop bodies
     p->timings.kernel_launches = launches;
+    if (flags & GSC_SOLVE_PROFILE) {
+        p->timings.sat_kernel_ms = sat_ms;
+        p->timings.scan_kernel_ms = scan_ms;
+        p->timings.sat_launches = sat_launches;
+    }
     return GSC_OK;
 }
 
@@ -782,12 +854,12 @@ int gsc_problem_read(gsc_problem* p, gsc_result* r) {
         GSC_CU(ctx, cudaMemcpyAsync(r->reach_step, p->reach_step, g.S * 4, cudaMemcpyDeviceToHost, st));
     const uint32_t n = std::min<uint32_t>(fc.iter, r->iter_capacity);
     if (n && (r->iter_new_reachable || r->iter_new_certified)) {
-        std::vector<unsigned long long> hs(2ull * (n + 1));
+        std::vector<unsigned long long> hs(static_cast<size_t>(kStatsCols) * (n + 1));
         GSC_CU(ctx, cudaMemcpyAsync(hs.data(), p->stats, hs.size() * 8, cudaMemcpyDeviceToHost, st));
         GSC_CU(ctx, cudaStreamSynchronize(st));
         for (uint32_t i = 0; i < n; ++i) {
-            if (r->iter_new_reachable) r->iter_new_reachable[i] = hs[2 * (i + 1)];
-            if (r->iter_new_certified) r->iter_new_certified[i] = hs[2 * (i + 1) + 1];
+            if (r->iter_new_reachable) r->iter_new_reachable[i] = hs[kStatsCols * (i + 1)];
+            if (r->iter_new_certified) r->iter_new_certified[i] = hs[kStatsCols * (i + 1) + 1];
         }
     }
     GSC_CU(ctx, cudaEventRecord(ctx->ev[1], st));

@@ -22,6 +22,10 @@ constexpr uint32_t kInvalid32 = 0xFFFFFFFFu;   // kInvalidInput / kUnreachableSt
 constexpr uint32_t kReject = 0xFFFFFFFFu;      // axis-table entry of a bounds-rejected pair
 constexpr uint32_t kBoxSentinel = 0xFFFFFFFFu; // stored-box entry of an invalid pair
 constexpr int kMaxWords = 4;                   // bit-sliced rows: n0 <= 256
+// Per-iteration counters: [0] newly reachable, [1] newly certified candidates,
+// [2] pair tests performed (stored: boxes streamed; fused: (state, input)
+// tests), [3] stored: box counts evaluated; fused: (slice, input) plane tasks.
+constexpr int kStatsCols = 4;
 
 // Geometry shared by all kernels (by value in kernel parameters).
 struct GridInfo {

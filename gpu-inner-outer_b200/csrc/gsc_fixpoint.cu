@@ -147,7 +147,7 @@ __global__ void __launch_bounds__(256) k_sat_stored(GridInfo g, StoredFixArgs a)
     const uint32_t it = fc->iter + 1;
     const uint64_t half = a.S_pad >> 1;
     const uint64_t t = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
-    unsigned long long nr = 0, nc = 0;
+    unsigned long long nr = 0, nc = 0, nload = 0, ncount = 0;
     if (t < half) {
         bool act[2], isc[2], rch[2], cert[2], found[2] = {false, false};
         uint32_t chosen[2] = {0, 0};
@@ -168,14 +168,21 @@ __global__ void __launch_bounds__(256) k_sat_stored(GridInfo g, StoredFixArgs a)
             uint4 nb = ld_stream(bx);
             for (uint32_t j = 0; j < g.M; ++j) {
                 const uint4 b = nb;
+                nload += 2;   // one 16-byte load carries two pairs' boxes
                 if (j + 1 < g.M) nb = ld_stream(bx + static_cast<uint64_t>(j + 1) * half);
-                if (act[0] && !found[0] && b.x != kBoxSentinel && dcount(a.pd, g, b.x, b.y) == 0) {
-                    found[0] = true;
-                    chosen[0] = j;
+                if (act[0] && !found[0] && b.x != kBoxSentinel) {
+                    ++ncount;
+                    if (dcount(a.pd, g, b.x, b.y) == 0) {
+                        found[0] = true;
+                        chosen[0] = j;
+                    }
                 }
-                if (act[1] && !found[1] && b.z != kBoxSentinel && dcount(a.pd, g, b.z, b.w) == 0) {
-                    found[1] = true;
-                    chosen[1] = j;
+                if (act[1] && !found[1] && b.z != kBoxSentinel) {
+                    ++ncount;
+                    if (dcount(a.pd, g, b.z, b.w) == 0) {
+                        found[1] = true;
+                        chosen[1] = j;
+                    }
                 }
                 if ((!act[0] || found[0]) && (!act[1] || found[1])) break;
             }
@@ -200,10 +207,15 @@ __global__ void __launch_bounds__(256) k_sat_stored(GridInfo g, StoredFixArgs a)
     for (int off = 16; off > 0; off >>= 1) {
         nr += __shfl_down_sync(0xFFFFFFFFu, nr, off);
         nc += __shfl_down_sync(0xFFFFFFFFu, nc, off);
+        nload += __shfl_down_sync(0xFFFFFFFFu, nload, off);
+        ncount += __shfl_down_sync(0xFFFFFFFFu, ncount, off);
     }
     if ((threadIdx.x & 31) == 0) {
-        if (nr) atomicAdd(&a.stats[2 * it], nr);
-        if (nc) atomicAdd(&a.stats[2 * it + 1], nc);
+        unsigned long long* row = a.stats + kStatsCols * it;
+        if (nr) atomicAdd(row, nr);
+        if (nc) atomicAdd(row + 1, nc);
+        if (nload) atomicAdd(row + 2, nload);
+        if (ncount) atomicAdd(row + 3, ncount);
     }
 }
 
@@ -211,7 +223,7 @@ __global__ void __launch_bounds__(256) k_sat_stored(GridInfo g, StoredFixArgs a)
 
 __global__ void k_fix_init(FixControl* fc, uint32_t max_iterations, uint32_t stats_cap,
                            const unsigned long long* counts, unsigned long long* stats) {
-    const uint32_t n = 2 * stats_cap;
+    const uint32_t n = kStatsCols * stats_cap;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) stats[i] = 0;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         fc->iter = 0;
@@ -231,8 +243,8 @@ __global__ void k_control(FixControl* fc, const unsigned long long* stats, cudaG
                           int use_cond) {
     if (!fc->stop) {
         const uint32_t it = fc->iter + 1;
-        const unsigned long long nr = stats[2 * it];
-        const unsigned long long nc = stats[2 * it + 1];
+        const unsigned long long nr = stats[kStatsCols * it];
+        const unsigned long long nc = stats[kStatsCols * it + 1];
         fc->certified += nc;
         fc->reachable += nr;
         fc->iter = it;
@@ -296,30 +308,66 @@ __device__ __forceinline__ uint64_t extract_bits(const uint64_t (&F)[W], uint32_
     return v & mask;
 }
 
-// One block per (theta, v) slice, all (x, y) states of the slice, inputs in
-// order.  For input j the slice shares one (theta, v) box; E[y] is the OR of
-// the D' rows over that box, F[i1] the OR of E over the y-range of row i1, and
-// state (i0, i1) is satisfied when F has no bit in its x-range.
+// acc |= F shifted so that bit i of the result is bit i + d of F (|d| < 64).
 template <int W>
-__global__ void __launch_bounds__(128) k_sat_fused(GridInfo g, FusedFixArgs a) {
-    extern __shared__ uint64_t smem[];
+__device__ __forceinline__ void or_shifted(const uint64_t (&F)[W], int d, uint64_t (&acc)[W]) {
+    if (d >= 0) {
+        const uint32_t r = static_cast<uint32_t>(d);
+#pragma unroll
+        for (int w = 0; w < W; ++w) {
+            uint64_t v = F[w] >> r;
+            if (w + 1 < W && r) v |= F[w + 1] << (64 - r);
+            acc[w] |= v;
+        }
+    } else {
+        const uint32_t r = static_cast<uint32_t>(-d);
+#pragma unroll
+        for (int w = 0; w < W; ++w) {
+            uint64_t v = F[w] << r;
+            if (w > 0) v |= F[w - 1] >> (64 - r);
+            acc[w] |= v;
+        }
+    }
+}
+
+// One block per (theta, v) slice, all (x, y) states of the slice.
+//
+// Inputs are visited omega-column by omega-column (j = ja + ma * jw).  For one
+// column every input shares the theta range of its box, so the block first ORs
+// the D' rows over that theta range for every v row the column can reach
+// (Ez, shared memory).  Then each warp takes one acceleration ja: E[y] = OR of
+// Ez over the v range of input j, F[i1] = OR of E over the y range of row i1,
+// and the x test runs 64 states at a time: the x boxes of a plane fall into a
+// few classes (lo - i0, hi - i0) = (a, b), and a state in class c is blocked
+// when F has a bit in [i0 + a, i0 + b], i.e. when bit i0 of
+// OR_{d=a..b} (F >> d) is set.  A plane with more than kClassMax classes uses
+// the per-state test.  The block then resolves the column in input order, so
+// every state records the lowest satisfied input.
+template <int W, bool NV>
+__global__ void __launch_bounds__(kFusedWarps * 32) k_sat_fused(GridInfo g, FusedFixArgs a) {
+    extern __shared__ __align__(16) uint64_t smem[];
+    __shared__ int s_wlo, s_whi;
     const FixControl* fc = a.fc;
     if (fc->stop) return;
     const uint32_t it = fc->iter + 1;
-    const uint64_t* rprev = (fc->iter & 1) ? a.reach1 : a.reach0;
-    uint64_t* rnext = (fc->iter & 1) ? a.reach0 : a.reach1;
-    const uint32_t n0 = g.n[0], n1 = g.n[1], n2 = g.n[2];
+    const uint64_t* __restrict__ rprev = (fc->iter & 1) ? a.reach1 : a.reach0;
+    uint64_t* __restrict__ rnext = (fc->iter & 1) ? a.reach0 : a.reach1;
+    const uint32_t n0 = g.n[0], n1 = g.n[1], n2 = g.n[2], ma = g.ma;
     const uint32_t nw = n1 * W;
-    uint64_t* E = smem;
-    uint64_t* EV = E + nw;
-    uint64_t* act = EV + nw;
-    uint64_t* fnd = act + nw;
-    uint32_t* xs = reinterpret_cast<uint32_t*>(fnd + nw);
-    uint32_t* ys = xs + n0;
     const uint32_t slice = blockIdx.x;
     const uint32_t i2 = slice % n2, i3 = slice / n2;
     const uint64_t wbase = static_cast<uint64_t>(slice) * nw;
     const uint32_t tid = threadIdx.x, bd = blockDim.x;
+    const uint32_t warp = tid >> 5, lane = tid & 31;
+    const uint32_t nv = NV ? 2u : 1u;
+
+    uint64_t* act = smem;
+    uint64_t* fnd = act + nw;
+    uint64_t* Ez = fnd + nw;                       // ez_rows * nw (+ the same for valid)
+    uint64_t* sat = Ez + a.ez_rows * nw * nv;      // ma * nw
+    uint64_t* mine = sat + ma * nw + warp * (nw * nv + a.cls_words);
+    uint64_t* E = mine;                            // nw (+ nw valid)
+    uint64_t* cls = mine + nw * nv;                // class record of the warp's plane
 
     int any = 0;
     for (uint32_t e = tid; e < nw; e += bd) {
@@ -328,79 +376,168 @@ __global__ void __launch_bounds__(128) k_sat_fused(GridInfo g, FusedFixArgs a) {
         fnd[e] = 0;
         any |= (v != 0);
     }
-    if (!__syncthreads_or(any)) {
+    if (tid == 0) {
+        int lo = 1 << 30, hi = -1;
+        for (uint32_t ja = 0; ja < ma; ++ja) {
+            const uint32_t we = a.wt[i3 * ma + ja];
+            if (we == kReject) continue;
+            lo = min(lo, static_cast<int>(lo16(we)));
+            hi = max(hi, static_cast<int>(hi16(we)));
+        }
+        s_wlo = lo;
+        s_whi = hi;
+    }
+    any = __syncthreads_or(any);
+    const int wlo = s_wlo, whi = s_whi;
+    if (!any || whi < wlo) {
         for (uint32_t e = tid; e < nw; e += bd) rnext[wbase + e] = rprev[wbase + e];
         return;
     }
-    for (uint32_t j = 0; j < g.M; ++j) {
-        const uint32_t ja = j % g.ma, jw = j / g.ma;
-        const uint32_t we = a.wt[i3 * g.ma + ja];
-        if (we == kReject) continue;
+    const uint32_t nwu = static_cast<uint32_t>(whi - wlo + 1);
+    unsigned long long ntest = 0, nplane = 0;
+    for (uint32_t jw = 0; jw < g.mw; ++jw) {
         const uint32_t ze = a.zt[i2 * g.mw + jw];
-        const uint64_t plane = (static_cast<uint64_t>(i2) * g.n[3] + i3) * g.M + j;
-        for (uint32_t e = tid; e < n0; e += bd) xs[e] = a.xt[plane * n0 + e];
-        for (uint32_t e = tid; e < n1; e += bd) ys[e] = a.yt[plane * n1 + e];
-        const uint32_t lw = lo16(we), hw = hi16(we), lz = lo16(ze), hz = hi16(ze);
-        for (uint32_t e = tid; e < nw; e += bd) {
-            const uint32_t y = e / W, w = e - y * W;
+        const uint32_t lz = lo16(ze), hz = hi16(ze);
+        for (uint32_t e = tid; e < nwu * nw; e += bd) {
+            const uint32_t wr = e / nw, rem = e - wr * nw;
+            const uint32_t y = rem / W, w = rem - y * W;
+            const uint64_t wv = static_cast<uint64_t>(wlo) + wr;
             uint64_t acc = 0, accv = 0;
-            for (uint32_t wv = lw; wv <= hw; ++wv) {
-                uint32_t z = lz;
-                for (;;) {
-                    const uint64_t r = y + static_cast<uint64_t>(n1) * (z + static_cast<uint64_t>(n2) * wv);
-                    acc |= a.dp[r * W + w];
-                    if (a.need_valid) accv |= a.validb[r * W + w];
-                    if (z == hz) break;
-                    z = (z + 1 == n2) ? 0 : z + 1;
-                }
+            uint32_t z = lz;
+            for (;;) {
+                const uint64_t r = y + static_cast<uint64_t>(n1) * (z + static_cast<uint64_t>(n2) * wv);
+                acc |= __ldg(a.dp + r * W + w);
+                if (NV) accv |= __ldg(a.validb + r * W + w);
+                if (z == hz) break;
+                z = (z + 1 == n2) ? 0 : z + 1;
             }
-            E[e] = acc;
-            EV[e] = accv;
+            Ez[e] = acc;
+            if (NV) Ez[nwu * nw + e] = accv;
         }
         __syncthreads();
-        for (uint32_t i1 = tid; i1 < n1; i1 += bd) {
-            uint64_t cm[W];
-            bool anyc = false;
-#pragma unroll
-            for (int w = 0; w < W; ++w) {
-                cm[w] = act[i1 * W + w] & ~fnd[i1 * W + w];
-                anyc |= cm[w] != 0;
+        for (uint32_t ja = warp; ja < ma; ja += kFusedWarps) {
+            const uint32_t j = ja + ma * jw;
+            uint64_t* Sj = sat + ja * nw;
+            const uint32_t we = a.wt[i3 * ma + ja];
+            if (we == kReject) {
+                for (uint32_t e = lane; e < nw; e += 32) Sj[e] = 0;
+                continue;
             }
-            const uint32_t ye = ys[i1];
-            if (!anyc || ye == kReject) continue;
-            uint64_t F[W], FV[W];
+            nplane += (lane == 0);
+            const uint32_t lw = lo16(we) - wlo, hw = hi16(we) - wlo;
+            const uint64_t plane = (static_cast<uint64_t>(i2) * g.n[3] + i3) * g.M + j;
+            for (uint32_t e = lane; e < a.cls_words; e += 32) cls[e] = __ldg(a.xcls + plane * a.cls_words + e);
+            for (uint32_t e = lane; e < nw; e += 32) {
+                uint64_t acc = 0, accv = 0;
+                for (uint32_t wr = lw; wr <= hw; ++wr) {
+                    acc |= Ez[wr * nw + e];
+                    if (NV) accv |= Ez[(nwu + wr) * nw + e];
+                }
+                E[e] = acc;
+                if (NV) E[nw + e] = accv;
+            }
+            __syncwarp();
+            const uint64_t h0 = cls[0], h1 = cls[1];
+            const uint32_t ncls = static_cast<uint32_t>(h0 & 0xFFu);
+            uint64_t okm[W];
 #pragma unroll
-            for (int w = 0; w < W; ++w) F[w] = FV[w] = 0;
-            for (uint32_t y = lo16(ye); y <= hi16(ye); ++y) {
+            for (int w = 0; w < W; ++w) okm[w] = 0;
+            if (ncls != 0xFFu) {
+                for (uint32_t c = 0; c < ncls; ++c) {
 #pragma unroll
-                for (int w = 0; w < W; ++w) {
-                    F[w] |= E[y * W + w];
-                    FV[w] |= EV[y * W + w];
+                    for (int w = 0; w < W; ++w) okm[w] |= cls[2 + c * W + w];
                 }
             }
-            const uint64_t srow = (static_cast<uint64_t>(slice) * n1 + i1) * n0;
+            for (uint32_t i1 = lane; i1 < n1; i1 += 32) {
+                uint64_t cm[W], sw[W];
+                bool anyc = false;
 #pragma unroll
-            for (int w = 0; w < W; ++w) {
-                uint64_t m = cm[w], nb = 0;
+                for (int w = 0; w < W; ++w) {
+                    cm[w] = act[i1 * W + w] & ~fnd[i1 * W + w];
+                    sw[w] = 0;
+                    anyc |= cm[w] != 0;
+                }
+                const uint32_t ye = anyc ? __ldg(a.yt + plane * n1 + i1) : kReject;
+                if (ye != kReject) {
+#pragma unroll
+                    for (int w = 0; w < W; ++w) ntest += __popcll(cm[w]);
+                    uint64_t F[W], FV[W];
+#pragma unroll
+                    for (int w = 0; w < W; ++w) F[w] = FV[w] = 0;
+                    for (uint32_t y = lo16(ye); y <= hi16(ye); ++y) {
+#pragma unroll
+                        for (int w = 0; w < W; ++w) {
+                            F[w] |= E[y * W + w];
+                            if (NV) FV[w] |= E[nw + y * W + w];
+                        }
+                    }
+                    if (ncls != 0xFFu) {
+                        uint64_t U[W], VA[W];
+#pragma unroll
+                        for (int w = 0; w < W; ++w) U[w] = VA[w] = 0;
+                        for (uint32_t c = 0; c < ncls; ++c) {
+                            const int ca = static_cast<int8_t>((h0 >> (8 * (c + 1))) & 0xFFu);
+                            const int cb = static_cast<int8_t>((h1 >> (8 * c)) & 0xFFu);
+                            uint64_t win[W], winv[W];
+#pragma unroll
+                            for (int w = 0; w < W; ++w) win[w] = winv[w] = 0;
+                            for (int d = ca; d <= cb; ++d) {
+                                or_shifted<W>(F, d, win);
+                                if (NV) or_shifted<W>(FV, d, winv);
+                            }
+#pragma unroll
+                            for (int w = 0; w < W; ++w) {
+                                const uint64_t m = cls[2 + c * W + w];
+                                U[w] |= win[w] & m;
+                                VA[w] |= winv[w] & m;
+                            }
+                        }
+#pragma unroll
+                        for (int w = 0; w < W; ++w) sw[w] = cm[w] & okm[w] & ~U[w] & (NV ? VA[w] : ~0ull);
+                    } else {
+                        const uint32_t* xrow = a.xt + plane * n0;
+#pragma unroll
+                        for (int w = 0; w < W; ++w) {
+                            uint64_t m = cm[w];
+                            while (m) {
+                                const uint32_t b = __ffsll(static_cast<long long>(m)) - 1;
+                                m &= m - 1;
+                                const uint32_t xe = __ldg(xrow + w * 64 + b);
+                                if (xe == kReject) continue;
+                                const uint32_t lx = lo16(xe), hx = hi16(xe);
+                                bool ok = extract_bits<W>(F, lx, hx) == 0;
+                                if (NV) ok = ok && extract_bits<W>(FV, lx, hx) != 0;
+                                if (ok) sw[w] |= 1ull << b;
+                            }
+                        }
+                    }
+                }
+#pragma unroll
+                for (int w = 0; w < W; ++w) Sj[i1 * W + w] = sw[w];
+            }
+        }
+        __syncthreads();
+        // Resolve the column in input order: the lowest satisfied input wins.
+        int left = 0;
+        for (uint32_t e = tid; e < nw; e += bd) {
+            uint64_t f = fnd[e];
+            uint64_t open = act[e] & ~f;
+            const uint64_t srow = (static_cast<uint64_t>(slice) * n1 + e / W) * n0 + (e % W) * 64;
+            for (uint32_t ja = 0; ja < ma && open; ++ja) {
+                const uint64_t nb = sat[ja * nw + e] & open;
+                if (!nb) continue;
+                open &= ~nb;
+                f |= nb;
+                uint64_t m = nb;
                 while (m) {
                     const uint32_t b = __ffsll(static_cast<long long>(m)) - 1;
                     m &= m - 1;
-                    const uint32_t i0 = w * 64 + b;
-                    const uint32_t xe = xs[i0];
-                    if (xe == kReject) continue;
-                    const uint32_t lx = lo16(xe), hx = hi16(xe);
-                    bool ok = extract_bits<W>(F, lx, hx) == 0;
-                    if (a.need_valid) ok = ok && extract_bits<W>(FV, lx, hx) != 0;
-                    if (ok) {
-                        nb |= 1ull << b;
-                        a.controller[srow + i0] = j;
-                    }
+                    a.controller[srow + b] = ja + ma * jw;
                 }
-                fnd[i1 * W + w] |= nb;
             }
+            fnd[e] = f;
+            left |= (open != 0);
         }
-        int left = 0;
-        for (uint32_t e = tid; e < nw; e += bd) left |= (act[e] & ~fnd[e]) != 0;
         if (!__syncthreads_or(left)) break;
     }
     unsigned long long nr = 0, nc = 0;
@@ -426,17 +563,44 @@ __global__ void __launch_bounds__(128) k_sat_fused(GridInfo g, FusedFixArgs a) {
     for (int off = 16; off > 0; off >>= 1) {
         nr += __shfl_down_sync(0xFFFFFFFFu, nr, off);
         nc += __shfl_down_sync(0xFFFFFFFFu, nc, off);
+        ntest += __shfl_down_sync(0xFFFFFFFFu, ntest, off);
+        nplane += __shfl_down_sync(0xFFFFFFFFu, nplane, off);
     }
     if ((tid & 31) == 0) {
-        if (nr) atomicAdd(&a.stats[2 * it], nr);
-        if (nc) atomicAdd(&a.stats[2 * it + 1], nc);
+        unsigned long long* row = a.stats + kStatsCols * it;
+        if (nr) atomicAdd(row, nr);
+        if (nc) atomicAdd(row + 1, nc);
+        if (ntest) atomicAdd(row + 2, ntest);
+        if (nplane) atomicAdd(row + 3, nplane);
     }
 }
 
-size_t fused_smem(const GridInfo& g) {
-    return static_cast<size_t>(g.n[1]) * g.W * 8 * 4 + static_cast<size_t>(g.n[0] + g.n[1]) * 4;
+template <int W, bool NV>
+cudaError_t launch_sat_fused_t(const GridInfo& g, const FusedFixArgs& a, size_t sm, cudaStream_t st) {
+    // The opt-in above 48 KB is a per-device function attribute: set it once per device.
+    static bool configured[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64 || !configured[dev]) {
+        e = cudaFuncSetAttribute(k_sat_fused<W, NV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(kFusedSmemMax));
+        if (e != cudaSuccess) return e;
+        if (dev >= 0 && dev < 64) configured[dev] = true;
+    }
+    k_sat_fused<W, NV><<<g.slices, kFusedWarps * 32, sm, st>>>(g, a);
+    return cudaGetLastError();
 }
 
+}  // namespace
+
+size_t fused_smem_bytes(const GridInfo& g, uint32_t ez_rows, uint32_t cls_words, int need_valid) {
+    const size_t nw = static_cast<size_t>(g.n[1]) * g.W;
+    const size_t nv = need_valid ? 2 : 1;
+    return 8 * (2 * nw + ez_rows * nw * nv + g.ma * nw + kFusedWarps * (nw * nv + cls_words));
+}
+
+namespace {
 }  // namespace
 
 cudaError_t launch_prefix4(const GridInfo& g, int mode, const uint8_t* a, const uint8_t* b, int32_t* table,
@@ -456,10 +620,14 @@ cudaError_t launch_stored_init(const GridInfo& g, const StoredFixArgs& a, cudaSt
     return cudaGetLastError();
 }
 
-cudaError_t launch_stored_iteration(const GridInfo& g, const StoredFixArgs& a, cudaStream_t st, uint32_t* launches) {
+cudaError_t launch_stored_iteration(const GridInfo& g, const StoredFixArgs& a, cudaStream_t st, uint32_t* launches,
+                                    cudaEvent_t* ev) {
+    if (ev) cudaEventRecord(ev[0], st);
     cudaError_t e = launch_prefix4(g, 1, a.valid, a.reach, a.pd, a.fc, st);
     if (e != cudaSuccess) return e;
+    if (ev) cudaEventRecord(ev[1], st);
     k_sat_stored<<<blocks_for(a.S_pad / 2, 256), 256, 0, st>>>(g, a);
+    if (ev) cudaEventRecord(ev[2], st);
     k_control<<<1, 1, 0, st>>>(a.fc, a.stats, a.cond, a.use_cond);
     if (launches) *launches += 6;
     return cudaGetLastError();
@@ -470,15 +638,30 @@ cudaError_t launch_fused_init(const GridInfo& g, const FusedFixArgs& a, const ui
     return cudaGetLastError();
 }
 
-cudaError_t launch_fused_iteration(const GridInfo& g, const FusedFixArgs& a, cudaStream_t st, uint32_t* launches) {
+cudaError_t launch_fused_iteration(const GridInfo& g, const FusedFixArgs& a, cudaStream_t st, uint32_t* launches,
+                                   cudaEvent_t* ev) {
+    if (ev) cudaEventRecord(ev[0], st);
     k_fused_dp<<<blocks_for(g.rows * g.W, 256), 256, 0, st>>>(g, a);
-    const size_t sm = fused_smem(g);
-    switch (g.W) {
-        case 1: k_sat_fused<1><<<g.slices, 128, sm, st>>>(g, a); break;
-        case 2: k_sat_fused<2><<<g.slices, 128, sm, st>>>(g, a); break;
-        case 3: k_sat_fused<3><<<g.slices, 128, sm, st>>>(g, a); break;
-        default: k_sat_fused<4><<<g.slices, 128, sm, st>>>(g, a); break;
+    if (ev) cudaEventRecord(ev[1], st);
+    const size_t sm = fused_smem_bytes(g, a.ez_rows, a.cls_words, a.need_valid);
+    cudaError_t err;
+    if (a.need_valid) {
+        switch (g.W) {
+            case 1: err = launch_sat_fused_t<1, true>(g, a, sm, st); break;
+            case 2: err = launch_sat_fused_t<2, true>(g, a, sm, st); break;
+            case 3: err = launch_sat_fused_t<3, true>(g, a, sm, st); break;
+            default: err = launch_sat_fused_t<4, true>(g, a, sm, st); break;
+        }
+    } else {
+        switch (g.W) {
+            case 1: err = launch_sat_fused_t<1, false>(g, a, sm, st); break;
+            case 2: err = launch_sat_fused_t<2, false>(g, a, sm, st); break;
+            case 3: err = launch_sat_fused_t<3, false>(g, a, sm, st); break;
+            default: err = launch_sat_fused_t<4, false>(g, a, sm, st); break;
+        }
     }
+    if (err != cudaSuccess) return err;
+    if (ev) cudaEventRecord(ev[2], st);
     k_control<<<1, 1, 0, st>>>(a.fc, a.stats, a.cond, a.use_cond);
     if (launches) *launches += 3;
     return cudaGetLastError();
@@ -486,7 +669,7 @@ cudaError_t launch_fused_iteration(const GridInfo& g, const FusedFixArgs& a, cud
 
 cudaError_t launch_fix_init(FixControl* fc, uint32_t max_iterations, uint32_t stats_cap,
                             const unsigned long long* counts, unsigned long long* stats, cudaStream_t st) {
-    k_fix_init<<<blocks_for(2ull * stats_cap, 256), 256, 0, st>>>(fc, max_iterations, stats_cap, counts, stats);
+    k_fix_init<<<blocks_for(static_cast<uint64_t>(kStatsCols) * stats_cap, 256), 256, 0, st>>>(fc, max_iterations, stats_cap, counts, stats);
     return cudaGetLastError();
 }
 

@@ -90,12 +90,14 @@ struct StoredFixArgs {
     uint32_t* controller;
     uint32_t* reach_step;
     FixControl* fc;
-    unsigned long long* stats;   // [stats_cap][2]
+    unsigned long long* stats;   // [stats_cap][kStatsCols]
     cudaGraphConditionalHandle cond;
     int use_cond;
 };
 cudaError_t launch_stored_init(const GridInfo& g, const StoredFixArgs& a, cudaStream_t st);
-cudaError_t launch_stored_iteration(const GridInfo& g, const StoredFixArgs& a, cudaStream_t st, uint32_t* launches);
+// ev (optional, 3 events): recorded before the scan, before and after the satisfaction kernel.
+cudaError_t launch_stored_iteration(const GridInfo& g, const StoredFixArgs& a, cudaStream_t st, uint32_t* launches,
+                                    cudaEvent_t* ev = nullptr);
 
 struct FusedFixArgs {
     const uint32_t *xt, *yt, *zt, *wt;
@@ -112,11 +114,25 @@ struct FusedFixArgs {
     FixControl* fc;
     unsigned long long* stats;
     int need_valid;
+    const uint64_t* xcls;      // per-plane x-box classes (launch_x_classes)
+    uint32_t cls_words;        // 64-bit words per class record
+    uint32_t ez_rows;          // max number of v rows reachable from one v cell
     cudaGraphConditionalHandle cond;
     int use_cond;
 };
+constexpr int kFusedWarps = 4;
+constexpr int kClassMax = 6;
+constexpr size_t kFusedSmemMax = 200 * 1024;
+// Dynamic shared memory of the fused satisfaction kernel.
+size_t fused_smem_bytes(const GridInfo& g, uint32_t ez_rows, uint32_t cls_words, int need_valid);
+// Class record words per plane: 2 header words + kClassMax * W masks.
+inline uint32_t class_words(const GridInfo& g) { return 2 + kClassMax * g.W; }
+// Per (slice, input) plane: the classes (lo - i0, hi - i0) of its x boxes
+// (header word 0: count (0xFF = irregular) | a[c] << 8(c+1); word 1: b[c] << 8c).
+cudaError_t launch_x_classes(const GridInfo& g, const uint32_t* xt, uint64_t* xcls, cudaStream_t st);
 cudaError_t launch_fused_init(const GridInfo& g, const FusedFixArgs& a, const uint8_t* cand, cudaStream_t st);
-cudaError_t launch_fused_iteration(const GridInfo& g, const FusedFixArgs& a, cudaStream_t st, uint32_t* launches);
+cudaError_t launch_fused_iteration(const GridInfo& g, const FusedFixArgs& a, cudaStream_t st, uint32_t* launches,
+                                   cudaEvent_t* ev = nullptr);
 
 // Resets the control block and zeroes the per-iteration counters.
 cudaError_t launch_fix_init(FixControl* fc, uint32_t max_iterations, uint32_t stats_cap,

@@ -364,6 +364,56 @@ __global__ void k_export(GridInfo g, ExportArgs a) {
     }
 }
 
+// Classes of the x boxes of one (slice, input) plane: states whose box is
+// [i0 + a, i0 + b] share the class (a, b).  Up to kClassMax classes, else the
+// plane is marked irregular (0xFF) and tested state by state.
+__global__ void k_x_classes(GridInfo g, const uint32_t* __restrict__ xt, uint64_t* __restrict__ out) {
+    const uint32_t cw = 2 + kClassMax * g.W;
+    const uint64_t planes = static_cast<uint64_t>(g.slices) * g.M;
+    for (uint64_t plane = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; plane < planes;
+         plane += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        int cnt = 0, A[kClassMax], B[kClassMax];
+        uint64_t masks[kClassMax][kMaxWords];
+        for (int c = 0; c < kClassMax; ++c)
+            for (int w = 0; w < kMaxWords; ++w) masks[c][w] = 0;
+        bool irregular = false;
+        for (uint32_t i0 = 0; i0 < g.n[0] && !irregular; ++i0) {
+            const uint32_t xe = xt[plane * g.n[0] + i0];
+            if (xe == kReject) continue;
+            const int a = static_cast<int>(lo16(xe)) - static_cast<int>(i0);
+            const int b = static_cast<int>(hi16(xe)) - static_cast<int>(i0);
+            if (a < -63 || a > 63 || b < -63 || b > 63 || b < a) {
+                irregular = true;
+                break;
+            }
+            int c = 0;
+            while (c < cnt && !(A[c] == a && B[c] == b)) ++c;
+            if (c == cnt) {
+                if (cnt == kClassMax) {
+                    irregular = true;
+                    break;
+                }
+                A[cnt] = a;
+                B[cnt] = b;
+                ++cnt;
+            }
+            masks[c][i0 >> 6] |= 1ull << (i0 & 63);
+        }
+        uint64_t h0 = irregular ? 0xFFull : static_cast<uint64_t>(cnt), h1 = 0;
+        if (!irregular) {
+            for (int c = 0; c < cnt; ++c) {
+                h0 |= static_cast<uint64_t>(static_cast<uint8_t>(A[c])) << (8 * (c + 1));
+                h1 |= static_cast<uint64_t>(static_cast<uint8_t>(B[c])) << (8 * c);
+            }
+        }
+        uint64_t* o = out + plane * cw;
+        o[0] = h0;
+        o[1] = h1;
+        for (int c = 0; c < kClassMax; ++c)
+            for (uint32_t w = 0; w < g.W; ++w) o[2 + c * g.W + w] = irregular ? 0 : masks[c][w];
+    }
+}
+
 // 2-D prefix of unsafe (x, y) centres; one block: rows, then columns.
 __global__ void k_prefix2(GridInfo g, const uint8_t* __restrict__ safe2, int32_t* __restrict__ t) {
     const uint32_t s1 = g.n[0] + 1;
@@ -438,6 +488,11 @@ cudaError_t launch_prefix2_unsafe(const GridInfo& g, const uint8_t* safe2, int32
 
 cudaError_t launch_stored_build(const GridInfo& g, const StoredBuildArgs& a, cudaStream_t st) {
     k_stored_build<<<blocks_for(a.S_pad * g.M), kThreads, 0, st>>>(g, a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_x_classes(const GridInfo& g, const uint32_t* xt, uint64_t* xcls, cudaStream_t st) {
+    k_x_classes<<<blocks_for(static_cast<uint64_t>(g.slices) * g.M, 128), 128, 0, st>>>(g, xt, xcls);
     return cudaGetLastError();
 }
 

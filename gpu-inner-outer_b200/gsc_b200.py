@@ -18,6 +18,7 @@ LIB_PATH = os.path.join(HERE, "libgsc_b200.so")
 
 METHOD_AUTO, METHOD_STORED, METHOD_FUSED = 0, 1, 2
 SOLVE_GRAPH = 1
+SOLVE_PROFILE = 2
 CONSTRAINTS = {"none": 0, "hyperbolic": 1, "elliptic": 2, "quadric": 3}
 MESSAGES = {
     0: "",
@@ -78,7 +79,9 @@ class Timings(ctypes.Structure):
     _fields_ = [
         ("abstraction_ms", ctypes.c_double), ("prepare_ms", ctypes.c_double), ("solve_ms", ctypes.c_double),
         ("readback_ms", ctypes.c_double), ("device_bytes", ctypes.c_uint64), ("method", ctypes.c_uint32),
-        ("kernel_launches", ctypes.c_uint32),
+        ("kernel_launches", ctypes.c_uint32), ("iterations", ctypes.c_uint32), ("sat_launches", ctypes.c_uint32),
+        ("sat_kernel_ms", ctypes.c_double), ("scan_kernel_ms", ctypes.c_double), ("pair_tests", ctypes.c_uint64),
+        ("aux_count", ctypes.c_uint64),
     ]
 
 
@@ -257,8 +260,9 @@ class Problem:
         ctx.check(lib().gsc_problem_create(ctx._h, abs_._h, ctypes.byref(self.query.desc), int(method),
                                            ctypes.byref(self._h)))
 
-    def solve(self, graph=False):
-        self.ctx.check(lib().gsc_problem_solve(self._h, SOLVE_GRAPH if graph else 0))
+    def solve(self, graph=False, profile=False):
+        flags = (SOLVE_GRAPH if graph else 0) | (SOLVE_PROFILE if profile else 0)
+        self.ctx.check(lib().gsc_problem_solve(self._h, flags))
 
     def timings(self) -> dict:
         t = Timings()
@@ -318,19 +322,28 @@ class Problem:
             pass
 
 
-def run_case(case, method=METHOD_AUTO, graph=False, device=0, iter_capacity=4096, **masks) -> dict:
+def run_case(case, method=METHOD_AUTO, graph=False, device=0, iter_capacity=4096, out=None, **masks) -> dict:
     """One-shot run through ``gsc_run_case`` (the run_case_cuda_u32 replacement):
-    host description in, host arrays out."""
+    host description in, host arrays out.  ``out`` may supply the five output
+    arrays (e.g. views of pinned memory)."""
     L = lib()
     m = model_desc(case)
     q = _Query(case, **masks)
     s, u = grid_shape(case)
     S = int(np.prod(s, dtype=np.uint64))
-    out = {
-        "valid_mask": np.zeros(S, np.uint8), "candidate_mask": np.zeros(S, np.uint8),
-        "reachable_mask": np.zeros(S, np.uint8), "controller": np.zeros(S, np.uint32),
-        "reach_step": np.zeros(S, np.uint32),
-    }
+    if out is None:
+        out = {
+            "valid_mask": np.zeros(S, np.uint8), "candidate_mask": np.zeros(S, np.uint8),
+            "reachable_mask": np.zeros(S, np.uint8), "controller": np.zeros(S, np.uint32),
+            "reach_step": np.zeros(S, np.uint32),
+        }
+    else:
+        for k, dt in (("valid_mask", np.uint8), ("candidate_mask", np.uint8), ("reachable_mask", np.uint8),
+                      ("controller", np.uint32), ("reach_step", np.uint32)):
+            a = out[k]
+            if a.dtype != dt or a.size != S or not a.flags["C_CONTIGUOUS"]:
+                raise ValueError(f"out[{k}] must be a contiguous {np.dtype(dt).name} array of {S} elements")
+        out = dict(out)
     r = Result()
     for k, v in out.items():
         setattr(r, k, _ptr(v))

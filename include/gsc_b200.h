@@ -84,8 +84,11 @@ enum {
 
 /* Solve flags. */
 enum {
-    GSC_SOLVE_GRAPH = 1u << 0       /* run the fixpoint as one CUDA graph with a
+    GSC_SOLVE_GRAPH = 1u << 0,      /* run the fixpoint as one CUDA graph with a
                                        device-side while condition                 */
+    GSC_SOLVE_PROFILE = 1u << 1     /* host loop, one iteration at a time, CUDA
+                                       events around the scan and satisfaction
+                                       kernels (gsc_timings.*_kernel_ms)           */
 };
 
 /* The grid and dynamics (CaseConfig fields that the successor boxes' nominal
@@ -160,6 +163,14 @@ typedef struct {
     uint64_t device_bytes;          /* device memory held by the problem          */
     uint32_t method;                /* method actually used                       */
     uint32_t kernel_launches;       /* kernels launched by the last solve         */
+    uint32_t iterations;            /* fixpoint iterations of the last solve      */
+    uint32_t sat_launches;          /* satisfaction-kernel launches timed         */
+    double sat_kernel_ms;           /* GSC_SOLVE_PROFILE: satisfaction kernels    */
+    double scan_kernel_ms;          /* GSC_SOLVE_PROFILE: set / prefix rebuilds   */
+    uint64_t pair_tests;            /* stored: boxes streamed; fused: (state,
+                                       input) tests, summed over iterations       */
+    uint64_t aux_count;             /* stored: box counts evaluated; fused:
+                                       (slice, input) plane tasks                 */
 } gsc_timings;
 
 typedef struct gsc_context gsc_context;

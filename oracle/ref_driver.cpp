@@ -191,15 +191,32 @@ int run_sample(const orc_case& c, std::uint64_t n, std::uint64_t seed, unsigned 
     const auto t_pre1 = Clock::now();
     const double prefix_ms = std::chrono::duration<double, std::milli>(t_pre1 - t_pre0).count() / 2.0;
 
+    // The sample is made of contiguous runs of states (as the reference's own
+    // loop visits them, so its caches see the same access pattern), one run
+    // per thread, each starting at a seeded offset.
     std::mt19937_64 rng(seed);
-    std::vector<std::uint64_t> states(n);
-    for (auto& s : states) s = rng() % grid.total_size;
+    std::vector<std::uint64_t> states;
+    states.reserve(n);
+    const std::uint64_t run = std::max<std::uint64_t>(1, n / threads);
+    while (states.size() < n) {
+        const std::uint64_t len = std::min<std::uint64_t>(run, n - states.size());
+        const std::uint64_t start = rng() % (grid.total_size - std::min<std::uint64_t>(len, grid.total_size) + 1);
+        for (std::uint64_t k = 0; k < len && start + k < grid.total_size; ++k) states.push_back(start + k);
+        if (len == 0) break;
+    }
+    n = states.size();
     const std::uint64_t M = igrid.total_size;
 
     std::vector<std::uint32_t> mnf(n * M), mxf(n * M);
     std::vector<std::uint8_t> pv(n * M);
+    auto range_of = [&](unsigned t, std::uint64_t* b, std::uint64_t* e) {
+        *b = n * t / threads;
+        *e = n * (t + 1) / threads;
+    };
     auto worker_abs = [&](unsigned t) {
-        for (std::uint64_t k = t; k < n; k += threads) {
+        std::uint64_t kb, ke;
+        range_of(t, &kb, &ke);
+        for (std::uint64_t k = kb; k < ke; ++k) {
             const std::uint64_t state = states[k];
             double x[4];
             grid.center(static_cast<std::uint32_t>(state), x);
@@ -220,7 +237,9 @@ int run_sample(const orc_case& c, std::uint64_t n, std::uint64_t seed, unsigned 
     std::atomic<std::uint64_t> hits{0};
     auto worker_fix = [&](unsigned t) {
         std::uint64_t local = 0;
-        for (std::uint64_t k = t; k < n; k += threads) {
+        std::uint64_t kb, ke;
+        range_of(t, &kb, &ke);
+        for (std::uint64_t k = kb; k < ke; ++k) {
             const std::uint64_t state = states[k];
             if (!valid[state]) continue;
             for (std::uint64_t input = 0; input < M; ++input) {
