@@ -318,6 +318,7 @@ uint64_t gsc_context_memory_in_use(const gsc_context* ctx) { return ctx ? ctx->i
 
 int gsc_abstraction_create(gsc_context* ctx, const gsc_model_desc* model, gsc_abstraction** out) {
     if (!ctx || !model || !out) return GSC_ERR_INVALID_ARGUMENT;
+    cudaGetLastError();   // a failure of an unrelated earlier call must not be reported here
     *out = nullptr;
     GSC_CU(ctx, cudaSetDevice(ctx->device));
     std::unique_ptr<gsc_abstraction> a(new (std::nothrow) gsc_abstraction());
@@ -710,6 +711,7 @@ int gsc_problem_create(gsc_context* ctx, const gsc_abstraction* abs, const gsc_q
     if (!ctx || !abs || !query || !out) return GSC_ERR_INVALID_ARGUMENT;
     *out = nullptr;
     if (abs->ctx != ctx) return fail(ctx, GSC_ERR_INVALID_ARGUMENT, "abstraction belongs to another context");
+    cudaGetLastError();   // a failure of an unrelated earlier call must not be reported here
     GSC_CU(ctx, cudaSetDevice(ctx->device));
     std::unique_ptr<gsc_problem> p(new (std::nothrow) gsc_problem());
     if (!p) return GSC_ERR_OUT_OF_MEMORY;
@@ -739,6 +741,7 @@ void gsc_problem_destroy(gsc_problem* p) {
 
 int gsc_problem_solve(gsc_problem* p, uint32_t flags) {
     if (!p) return GSC_ERR_INVALID_ARGUMENT;
+    cudaGetLastError();   // a failure of an unrelated earlier call must not be reported here
     gsc_context* ctx = p->ctx;
     GSC_CU(ctx, cudaSetDevice(ctx->device));
     cudaStream_t st = ctx->stream;
@@ -820,6 +823,7 @@ int gsc_problem_solve(gsc_problem* p, uint32_t flags) {
 
 int gsc_problem_read(gsc_problem* p, gsc_result* r) {
     if (!p || !r) return GSC_ERR_INVALID_ARGUMENT;
+    cudaGetLastError();   // a failure of an unrelated earlier call must not be reported here
     gsc_context* ctx = p->ctx;
     GSC_CU(ctx, cudaSetDevice(ctx->device));
     cudaStream_t st = ctx->stream;
@@ -872,6 +876,7 @@ int gsc_problem_read(gsc_problem* p, gsc_result* r) {
 
 int gsc_problem_export_abstraction(gsc_problem* p, uint32_t* min_flat, uint32_t* max_flat, uint8_t* valid) {
     if (!p || !min_flat || !max_flat || !valid) return GSC_ERR_INVALID_ARGUMENT;
+    cudaGetLastError();   // a failure of an unrelated earlier call must not be reported here
     gsc_context* ctx = p->ctx;
     GSC_CU(ctx, cudaSetDevice(ctx->device));
     cudaStream_t st = ctx->stream;

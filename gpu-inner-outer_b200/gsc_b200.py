@@ -10,6 +10,7 @@ from __future__ import annotations
 
 import ctypes
 import os
+import weakref
 
 import numpy as np
 
@@ -195,7 +196,12 @@ def grid_shape(case):
 
 
 class Context:
+    """A device + stream.  Abstractions and problems made from it are closed
+    (problems first) when the context closes, since the library requires a
+    context to outlive everything created from it."""
+
     def __init__(self, device=0, stream=None):
+        self._children = weakref.WeakSet()
         self._h = ctypes.c_void_p()
         st = lib().gsc_context_create(int(device), ctypes.c_void_p(stream) if stream else None, ctypes.byref(self._h))
         if st != 0:
@@ -216,6 +222,12 @@ class Context:
 
     def close(self):
         if self._h:
+            kids = list(self._children)
+            for k in kids:
+                if isinstance(k, Problem):
+                    k.close()
+            for k in kids:
+                k.close()
             lib().gsc_context_destroy(self._h)
             self._h = ctypes.c_void_p()
 
@@ -238,6 +250,7 @@ class Abstraction:
         self._h = ctypes.c_void_p()
         self.model = model_desc(case)
         ctx.check(lib().gsc_abstraction_create(ctx._h, ctypes.byref(self.model), ctypes.byref(self._h)))
+        ctx._children.add(self)
 
     def close(self):
         if self._h:
@@ -259,6 +272,7 @@ class Problem:
         self.query = _Query(case, **masks)
         ctx.check(lib().gsc_problem_create(ctx._h, abs_._h, ctypes.byref(self.query.desc), int(method),
                                            ctypes.byref(self._h)))
+        ctx._children.add(self)
 
     def solve(self, graph=False, profile=False):
         flags = (SOLVE_GRAPH if graph else 0) | (SOLVE_PROFILE if profile else 0)

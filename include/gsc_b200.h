@@ -192,6 +192,7 @@ int gsc_grid_shape(const gsc_model_desc* model, uint32_t shape[4], uint32_t inpu
 /* A context binds a device and a stream (NULL stream = a private stream).
  * Mirrors the device checks of kernels.cu:496-502. */
 int gsc_context_create(int device, void* cuda_stream, gsc_context** out);
+/* Destroy every problem and abstraction of a context before the context. */
 void gsc_context_destroy(gsc_context* ctx);
 const char* gsc_last_error(const gsc_context* ctx);
 /* Device memory the context may hold in problems and abstractions (0 = no
