@@ -110,6 +110,9 @@ SIGNATURES = {
     "gsc_run_case": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ModelDesc), ctypes.POINTER(QueryDesc),
                                     ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(Result),
                                     ctypes.POINTER(Timings)]),
+    "gsc_fixpoint_noalloc": (ctypes.c_int, [ctypes.POINTER(ctypes.c_uint32), ctypes.c_uint32, ctypes.c_int32,
+                                            _P, _P, _P, _P, _P, ctypes.c_uint32, _P, _P, _P,
+                                            ctypes.POINTER(Result), _P]),
 }
 
 _lib = None

@@ -233,6 +233,35 @@ int gsc_problem_timings(const gsc_problem* p, gsc_timings* out);
 int gsc_run_case(int device, const gsc_model_desc* model, const gsc_query_desc* query, uint32_t method,
                  uint32_t flags, gsc_result* out, gsc_timings* timings);
 
+/* No counterpart in the reference.
+ *
+ * The backward-reachability fixpoint over an abstraction the caller already
+ * holds in device memory, in the reference's layout (min_flat, max_flat and
+ * valid per pair, pair = state * inputs + input), without allocating any
+ * memory.  It is meant for callers that may not call cudaMalloc when they
+ * need a solve: a process whose device memory is already carved into its own
+ * pools, a plugin whose host owns every allocation, or a latency-critical path
+ * that must not enter the driver's allocator (which can synchronise the device
+ * and can fail).
+ *
+ * Every pointer except `summary` is device memory owned by the caller:
+ * inputs min_flat, max_flat, pair_valid ([states * inputs]), valid_mask and
+ * candidate_mask ([states]); outputs reachable_mask, controller, reach_step
+ * ([states]).  `summary` (host, optional) receives the iteration count, stop
+ * message and set sizes.  The working tables live in one fixed device array
+ * inside the library (about 40 MiB, held by every GPU that loads the library
+ * until the process exits).  Grids whose padded table
+ * (nx+1)(ny+1)(ntheta+1)(nv+1) has more than 4,718,592 entries, or that could
+ * need more than 4,094 iterations, are refused with GSC_ERR_OUT_OF_MEMORY
+ * before any device work.  All calls share that array, so calls that overlap
+ * on the GPU race: serialise them.  The first call on a device looks the
+ * array's address up (cudaGetSymbolAddress); make that first call before any
+ * stream capture.  Returns after synchronising `cuda_stream`. */
+int gsc_fixpoint_noalloc(const uint32_t shape[4], uint32_t inputs, int32_t wrap_dim, const uint32_t* min_flat,
+                         const uint32_t* max_flat, const uint8_t* pair_valid, const uint8_t* valid_mask,
+                         const uint8_t* candidate_mask, uint32_t max_iterations, uint8_t* reachable_mask,
+                         uint32_t* controller, uint32_t* reach_step, gsc_result* summary, void* cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif
