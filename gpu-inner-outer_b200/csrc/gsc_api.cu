@@ -485,6 +485,8 @@ int build_problem(gsc_problem* p, const gsc_query_desc* qd, uint32_t method) {
     ma.cand = p->cand;
     ma.build_valid = qd->valid_mask ? 0 : 1;
     ma.build_cand = qd->candidate_mask ? 0 : 1;
+    ma.safe = qd->safe_mask ? p->safe : nullptr;
+    ma.safe_rank = p->safe_rank;
     ma.counts = p->counts;
     GSC_CU(ctx, launch_masks(g, q, ma, st));
 

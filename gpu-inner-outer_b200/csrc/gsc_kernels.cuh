@@ -21,6 +21,8 @@ struct MaskArgs {
     uint8_t* cand;            // [S]
     int build_valid;          // 0: valid already filled by the caller's mask
     int build_cand;
+    const uint8_t* safe;      // caller's constraint mask (rank 2 or 4), or null: use the constraint kind
+    int safe_rank;
     unsigned long long* counts;  // [0] valid, [1] candidate, [2] candidate-not-valid
 };
 cudaError_t launch_masks(const GridInfo& g, const QueryInfo& q, const MaskArgs& a, cudaStream_t st);

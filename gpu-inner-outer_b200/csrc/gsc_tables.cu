@@ -92,7 +92,12 @@ __global__ void k_masks(GridInfo g, QueryInfo q, MaskArgs a) {
                     }
                 }
             }
-            if (v && q.ckind != 0) v = satisfies(q, x[0], x[1]);
+            // The constraint (abstraction.hpp:96-99): the caller's mask when given
+            // (a kCustom predicate evaluated at the centres), else the built-in kind.
+            if (v && a.safe)
+                v = (a.safe_rank == 4 ? a.safe[s] : a.safe[idx[1] * g.n[0] + idx[0]]) != 0;
+            else if (v && q.ckind != 0)
+                v = satisfies(q, x[0], x[1]);
             a.valid[s] = v ? 1 : 0;
         } else {
             v = a.valid[s] != 0;

@@ -1,0 +1,91 @@
+// gsc/cuda_api.hpp -- the reference's backend entry points, over libgsc_b200's C ABI.
+//
+// Same names and report fields as include/gsc/cuda_api.hpp:11-88 of the
+// reference, so code written against run_case_cuda_u32 keeps working.  The
+// abstraction arrays of the report are filled only when requested (they are
+// P-sized; keeping them on the device is the point of the B200 design).
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "gsc/config.hpp"
+
+namespace gsc {
+
+using InputIndex = std::uint32_t;
+using ReachStep = std::uint32_t;
+constexpr InputIndex kInvalidInput = 0xFFFFFFFFu;
+constexpr ReachStep kUnreachableStep = 0xFFFFFFFFu;
+
+struct SolveResult {
+    std::vector<std::uint8_t> valid_mask;
+    std::vector<std::uint8_t> candidate_mask;
+    std::vector<std::uint8_t> reachable_mask;
+    std::vector<InputIndex> controller;
+    std::vector<ReachStep> reach_step;
+    std::uint32_t iterations = 0;
+    bool converged = false;
+    std::string message;
+    std::uint64_t reachable_states = 0;
+    std::uint64_t certified_candidate_states = 0;
+    double solve_ms = 0.0;
+};
+
+struct IterationStats {
+    std::uint32_t iteration = 0;
+    std::uint64_t newly_reachable = 0;
+    std::uint64_t newly_certified = 0;
+    std::uint64_t total_reachable = 0;
+    std::uint64_t total_certified = 0;
+};
+
+struct KernelTimings {
+    double abstraction_kernel_ms = 0.0;   // resident nominal tables
+    double prepare_ms = 0.0;              // masks and quantised boxes
+    double solve_ms = 0.0;                // the device fixpoint
+    double result_memcpy_d2h_ms = 0.0;
+};
+
+struct GpuMemoryStats {
+    std::uint64_t total_allocated_bytes = 0;
+};
+
+struct GridShape {
+    std::uint32_t shape[kStateDim]{};
+    std::uint64_t total_size = 0;
+};
+
+struct GpuRunReport {
+    bool compiled_with_cuda = false;
+    bool runtime_available = false;
+    bool executed = false;
+    std::string message;
+    double abstraction_ms = 0.0;
+    double solve_ms = 0.0;
+    double total_ms = 0.0;
+    SolveResult result;
+    GridShape state_grid;
+    GridShape input_grid;
+    std::uint64_t pair_count = 0;
+    std::vector<IterationStats> iteration_stats;
+    KernelTimings kernel_timings;
+    GpuMemoryStats memory_stats;
+    std::vector<std::uint32_t> abstraction_min_flat;
+    std::vector<std::uint32_t> abstraction_max_flat;
+    std::vector<std::uint8_t> abstraction_valid;
+};
+
+struct RunOptions {
+    int device = 0;
+    std::uint32_t method = 0;          // GSC_METHOD_*
+    bool graph = true;                 // one CUDA graph for the whole fixpoint
+    bool export_abstraction = false;   // fill abstraction_* (P-sized host copies)
+};
+
+bool cuda_backend_compiled();
+GpuRunReport run_case_cuda_u32(const CaseConfig& cfg);
+GpuRunReport run_case_cuda_u32(const CaseConfig& cfg, const RunOptions& options);
+
+}  // namespace gsc

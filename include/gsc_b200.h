@@ -121,8 +121,9 @@ typedef struct {
     /* Optional host masks replacing the ones built from the description above
      * (NULL = build on the device).  safe_mask is the state constraint
      * evaluated at cell centres: rank 2 = [ny][nx] over (x, y), rank 4 = one
-     * byte per state.  A custom constraint (ConstraintType::kCustom) is passed
-     * this way. */
+     * byte per state.  When given it replaces constraint_kind everywhere: in the
+     * valid mask, at the source state and over every successor box.  A custom
+     * constraint (ConstraintType::kCustom) is passed this way. */
     const uint8_t* safe_mask;
     int32_t safe_mask_rank;
     const uint8_t* valid_mask;      /* one byte per state                         */

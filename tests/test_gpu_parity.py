@@ -122,10 +122,12 @@ def test_safe_mask_overrides(ctx):
                 candidate_lb=[9, 9, 9, 9], candidate_ub=[9, 9, 9, 9])
     safe4, _ = O.masks(free)
     safe2 = safe4[: shape[0] * shape[1]].copy()
+    custom = dict(case, constraint="none")   # the mask alone carries the constraint (kCustom route)
     for rank, mask in ((2, safe2), (4, safe4)):
         for method in METHODS.values():
-            got = solve(ctx, case, method, graph=False, safe_mask=mask, safe_rank=rank)
-            assert_same_result(got, want, f"safe rank {rank}/{method}")
+            for c in (case, custom):
+                got = solve(ctx, c, method, graph=False, safe_mask=mask, safe_rank=rank)
+                assert_same_result(got, want, f"safe rank {rank}/{method}/{c['constraint']}")
     assert S == safe4.size
 
 
