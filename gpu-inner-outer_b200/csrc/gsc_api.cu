@@ -66,10 +66,13 @@ struct gsc_problem {
     int32_t* pd = nullptr;
     uint8_t* reach8 = nullptr;
     // fused
-    uint64_t *validb = nullptr, *unsafeb = nullptr, *srcb = nullptr, *candb = nullptr, *dp = nullptr;
-    uint64_t *reach0 = nullptr, *reach1 = nullptr, *active = nullptr;
-    uint64_t* xcls = nullptr;
+    bword *validb = nullptr, *unsafeb = nullptr, *srcb = nullptr, *candb = nullptr, *dp = nullptr;
+    bword *reach0 = nullptr, *reach1 = nullptr, *active = nullptr, *hit = nullptr;
+    uint32_t* best = nullptr;
+    bword* xcls = nullptr;
+    uint8_t* xrep = nullptr;
     uint32_t ez_rows = 0;
+    uint32_t max_reps = 0;
     int need_valid = 0;
     // common fixpoint state
     uint32_t* controller = nullptr;
@@ -186,9 +189,11 @@ int grid_from_model(const gsc_model_desc* m, GridInfo* g, std::string* err) {
         *err = "padded prefix table exceeds int32 indexing";
         return GSC_ERR_UNSUPPORTED;
     }
-    g->W = (g->n[0] + 63) / 64;
+    g->W = (g->n[0] + kBits - 1) / kBits;
     g->rows = static_cast<uint64_t>(g->n[1]) * g->n[2] * g->n[3];
     g->slices = g->n[2] * g->n[3];
+    g->magic_n1 = fdiv_magic(g->n[1]);
+    g->magic_nw = fdiv_magic(g->n[1] * g->W);
     return GSC_OK;
 }
 
@@ -449,7 +454,7 @@ int build_problem(gsc_problem* p, const gsc_query_desc* qd, uint32_t method) {
 
     // Method selection.
     bool stored_ok = g.n[0] <= 255 && g.n[1] <= 255 && g.n[2] <= 255 && g.n[3] <= 255;
-    bool fused_ok = g.n[0] <= 64 * kMaxWords;
+    bool fused_ok = g.n[0] <= kBits * kMaxWords && g.ma <= 255;
     if (method == GSC_METHOD_STORED && !stored_ok)
         return fail(ctx, GSC_ERR_UNSUPPORTED, "stored method needs at most 255 cells per dimension");
     if (method == GSC_METHOD_FUSED && !fused_ok)
@@ -525,7 +530,7 @@ int build_problem(gsc_problem* p, const gsc_query_desc* qd, uint32_t method) {
         }
         p->ez_rows = rows;
         const int nv = p->safe ? (hc[4] != 0) : (hc[0] != g.S);
-        if (fused_smem_bytes(g, rows, class_words(g), nv) > kFusedSmemMax) fused_ok = false;
+        if (fused_smem_bytes(g, rows, class_words(g), nv, g.ma) > kFusedSmemMax) fused_ok = false;
     }
     if (method == GSC_METHOD_AUTO) method = fused_ok ? GSC_METHOD_FUSED : (stored_ok ? GSC_METHOD_STORED : 0);
     if (method == 0) return fail(ctx, GSC_ERR_UNSUPPORTED, "no method applies to this grid");
@@ -586,13 +591,31 @@ int build_problem(gsc_problem* p, const gsc_query_desc* qd, uint32_t method) {
         GSC_TRY(dalloc(ctx, A, B, &p->reach0, words));
         GSC_TRY(dalloc(ctx, A, B, &p->reach1, words));
         GSC_TRY(dalloc(ctx, A, B, &p->active, words));
+        GSC_TRY(dalloc(ctx, A, B, &p->hit, words));
+        GSC_TRY(dalloc(ctx, A, B, &p->best, g.S));
         GSC_TRY(dalloc(ctx, A, B, &p->xcls, static_cast<uint64_t>(g.slices) * g.M * class_words(g)));
         GSC_CU(ctx, launch_x_classes(g, p->xt, p->xcls, st));
+        GSC_TRY(dalloc(ctx, A, B, &p->xrep, static_cast<uint64_t>(g.slices) * g.M));
+        GSC_CU(ctx, launch_plane_reps(g, p->xt, p->yt, p->wt, p->xrep, st));
+        {
+            // Shared memory of the satisfaction kernel is sized by the largest
+            // number of distinct accelerations in one omega column.
+            std::vector<uint8_t> hrep(static_cast<size_t>(g.slices) * g.M);
+            GSC_CU(ctx, cudaMemcpyAsync(hrep.data(), p->xrep, hrep.size(), cudaMemcpyDeviceToHost, st));
+            GSC_CU(ctx, cudaStreamSynchronize(st));
+            uint32_t mr = 1;
+            for (size_t c = 0; c < hrep.size(); c += g.ma) {
+                uint32_t n = 0;
+                for (uint32_t ja = 0; ja < g.ma; ++ja) n += hrep[c + ja] == ja;
+                mr = std::max(mr, n);
+            }
+            p->max_reps = mr;
+        }
         GSC_CU(ctx, launch_pack_bits(g, 0, p->valid, nullptr, p->validb, st));
         GSC_CU(ctx, launch_pack_bits(g, 0, p->cand, nullptr, p->candb, st));
         if (!p->safe) {
-            GSC_CU(ctx, cudaMemsetAsync(p->unsafeb, 0, words * 8, st));
-            GSC_CU(ctx, cudaMemcpyAsync(p->srcb, p->validb, words * 8, cudaMemcpyDeviceToDevice, st));
+            GSC_CU(ctx, cudaMemsetAsync(p->unsafeb, 0, words * sizeof(bword), st));
+            GSC_CU(ctx, cudaMemcpyAsync(p->srcb, p->validb, words * sizeof(bword), cudaMemcpyDeviceToDevice, st));
         } else if (p->safe_rank == 2) {
             GSC_CU(ctx, launch_pack_bits(g, 2, nullptr, p->safe, p->unsafeb, st));
             GSC_CU(ctx, launch_pack_bits(g, 3, p->valid, p->safe, p->srcb, st));
@@ -638,14 +661,18 @@ FusedFixArgs fused_args(gsc_problem* p, cudaGraphConditionalHandle cond, int use
     a.reach0 = p->reach0;
     a.reach1 = p->reach1;
     a.active = p->active;
+    a.hit = p->hit;
+    a.best = p->best;
     a.controller = p->controller;
     a.reach_step = p->reach_step;
     a.fc = p->fc;
     a.stats = p->stats;
     a.need_valid = p->need_valid;
     a.xcls = p->xcls;
+    a.xrep = p->xrep;
     a.cls_words = class_words(p->g);
     a.ez_rows = p->ez_rows;
+    a.max_reps = p->max_reps;
     a.cond = cond;
     a.use_cond = use_cond;
     return a;
@@ -751,7 +778,7 @@ int gsc_problem_solve(gsc_problem* p, uint32_t flags) {
     uint32_t launches = 0;
     double sat_ms = 0.0, scan_ms = 0.0;
     uint32_t sat_launches = 0;
-    const uint32_t per_iter = (p->method == GSC_METHOD_STORED) ? 6 : 3;
+    const uint32_t per_iter = (p->method == GSC_METHOD_STORED) ? 6 : 2;
     if (flags & GSC_SOLVE_PROFILE) {
         GSC_CU(ctx, enqueue_init(p));
         launches += 2;
@@ -759,7 +786,13 @@ int gsc_problem_solve(gsc_problem* p, uint32_t flags) {
         for (auto& e : ev) GSC_CU(ctx, cudaEventCreate(&e));
         FixControl hfc;
         cudaError_t err = cudaSuccess;
+        uint32_t guard = 0;
         while (err == cudaSuccess) {
+            // The stop rules fire by iteration stats_cap - 1 at the latest.
+            if (++guard > p->stats_cap + 2) {
+                for (auto& e : ev) cudaEventDestroy(e);
+                return fail(ctx, GSC_ERR_TIMEOUT, "fixpoint did not stop within its iteration bound");
+            }
             err = enqueue_iteration(p, 0, 0, &launches, ev);
             if (err == cudaSuccess) err = cudaMemcpyAsync(&hfc, p->fc, sizeof(hfc), cudaMemcpyDeviceToHost, st);
             if (err == cudaSuccess) err = cudaStreamSynchronize(st);
@@ -788,6 +821,8 @@ int gsc_problem_solve(gsc_problem* p, uint32_t flags) {
             GSC_CU(ctx, cudaStreamSynchronize(st));
             host_stop = hfc.stop;
             if (host_stop) break;
+            if (done > p->stats_cap + 64)
+                return fail(ctx, GSC_ERR_TIMEOUT, "fixpoint did not stop within its iteration bound");
             if (chunk < 64) chunk *= 2;
         }
         (void)done;

@@ -21,7 +21,11 @@ namespace gsc_b200 {
 constexpr uint32_t kInvalid32 = 0xFFFFFFFFu;   // kInvalidInput / kUnreachableStep (types.hpp:22-23)
 constexpr uint32_t kReject = 0xFFFFFFFFu;      // axis-table entry of a bounds-rejected pair
 constexpr uint32_t kBoxSentinel = 0xFFFFFFFFu; // stored-box entry of an invalid pair
-constexpr int kMaxWords = 4;                   // bit-sliced rows: n0 <= 256
+// Bit-sliced sets use 32-bit words: every shift of a row is one native
+// funnel shift.  A row of n0 x-cells takes W = ceil(n0 / 32) words.
+using bword = uint32_t;
+constexpr int kBits = 32;
+constexpr int kMaxWords = 8;                   // bit-sliced rows: n0 <= 256
 // Per-iteration counters: [0] newly reachable, [1] newly certified candidates,
 // [2] pair tests performed (stored: boxes streamed; fused: (state, input)
 // tests), [3] stored: box counts evaluated; fused: (slice, input) plane tasks.
@@ -39,10 +43,18 @@ struct GridInfo {
     uint64_t S;          // states
     uint32_t ps[4];      // padded prefix strides (grid.hpp:253-269)
     uint64_t tsize;      // padded prefix entries
-    uint32_t W;          // 64-bit words per x-row of a bit-sliced set
+    uint32_t W;          // 32-bit words per x-row of a bit-sliced set
     uint64_t rows;       // n1 * n2 * n3 x-rows
     uint32_t slices;     // n2 * n3 (theta, v) slices
+    uint32_t magic_n1;   // fdiv(x, n1) / fdiv(x, n1 * W) multipliers (see fdiv)
+    uint32_t magic_nw;
 };
+
+// x / d for x * d < 2^32 with m = floor(2^32 / d) + 1 (m = 0 encodes d = 1).
+__host__ __device__ __forceinline__ uint32_t fdiv_magic(uint32_t d) {
+    return d <= 1 ? 0u : static_cast<uint32_t>((1ull << 32) / d + 1);
+}
+__device__ __forceinline__ uint32_t fdiv(uint32_t x, uint32_t m) { return m ? __umulhi(x, m) : x; }
 
 // Per-query constants.
 struct QueryInfo {
@@ -183,6 +195,8 @@ struct FixControl {
     uint32_t converged;
     uint32_t max_iterations;
     uint32_t stats_cap;       // stats entries (iteration index 1..stats_cap-1)
+    uint32_t ticket;          // blocks of the finalize kernel done this iteration
+    uint32_t pad;
     unsigned long long candidate_count;
     unsigned long long certified;
     unsigned long long reachable;

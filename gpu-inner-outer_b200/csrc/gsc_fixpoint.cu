@@ -227,6 +227,7 @@ __global__ void k_fix_init(FixControl* fc, uint32_t max_iterations, uint32_t sta
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) stats[i] = 0;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         fc->iter = 0;
+        fc->ticket = 0;
         fc->max_iterations = max_iterations;
         fc->stats_cap = stats_cap;
         fc->valid_count = counts[0];
@@ -267,340 +268,6 @@ __global__ void k_set_condition(const FixControl* fc, cudaGraphConditionalHandle
     cudaGraphSetConditional(cond, fc->stop ? 0u : 1u);
 }
 
-// ---- fused method (bit-sliced sets, boxes from per-axis tables) -------------------------
-
-__global__ void k_fused_init(GridInfo g, FusedFixArgs a, const uint8_t* __restrict__ cand) {
-    const uint64_t words = g.rows * g.W;
-    for (uint64_t e = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; e < words;
-         e += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        a.reach0[e] = a.candb[e];
-        a.active[e] = a.srcb[e];
-    }
-    for (uint64_t s = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; s < g.S;
-         s += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        a.controller[s] = kInvalid32;
-        a.reach_step[s] = cand[s] ? 0u : kInvalid32;
-    }
-}
-
-// D' = (valid && !reachable) || unsafe, from the previous iteration's set.
-__global__ void k_fused_dp(GridInfo g, FusedFixArgs a) {
-    const FixControl* fc = a.fc;
-    if (fc->stop) return;
-    const uint64_t* rprev = (fc->iter & 1) ? a.reach1 : a.reach0;
-    const uint64_t words = g.rows * g.W;
-    for (uint64_t e = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; e < words;
-         e += static_cast<uint64_t>(gridDim.x) * blockDim.x)
-        a.dp[e] = (a.validb[e] & ~rprev[e]) | a.unsafeb[e];
-}
-
-template <int W>
-__device__ __forceinline__ uint64_t extract_bits(const uint64_t (&F)[W], uint32_t lx, uint32_t hx) {
-    const uint32_t wi = lx >> 6, sh = lx & 63u, len = hx - lx + 1;
-    uint64_t lo = 0, hi = 0;
-#pragma unroll
-    for (int w = 0; w < W; ++w) {
-        if (static_cast<uint32_t>(w) == wi) lo = F[w];
-        if (static_cast<uint32_t>(w) == wi + 1) hi = F[w];
-    }
-    const uint64_t v = sh ? ((lo >> sh) | (hi << (64 - sh))) : lo;
-    const uint64_t mask = len >= 64 ? ~0ull : ((1ull << len) - 1);
-    return v & mask;
-}
-
-// acc |= F shifted so that bit i of the result is bit i + d of F (|d| < 64).
-template <int W>
-__device__ __forceinline__ void or_shifted(const uint64_t (&F)[W], int d, uint64_t (&acc)[W]) {
-    if (d >= 0) {
-        const uint32_t r = static_cast<uint32_t>(d);
-#pragma unroll
-        for (int w = 0; w < W; ++w) {
-            uint64_t v = F[w] >> r;
-            if (w + 1 < W && r) v |= F[w + 1] << (64 - r);
-            acc[w] |= v;
-        }
-    } else {
-        const uint32_t r = static_cast<uint32_t>(-d);
-#pragma unroll
-        for (int w = 0; w < W; ++w) {
-            uint64_t v = F[w] << r;
-            if (w > 0) v |= F[w - 1] >> (64 - r);
-            acc[w] |= v;
-        }
-    }
-}
-
-// One block per (theta, v) slice, all (x, y) states of the slice.
-//
-// Inputs are visited omega-column by omega-column (j = ja + ma * jw).  For one
-// column every input shares the theta range of its box, so the block first ORs
-// the D' rows over that theta range for every v row the column can reach
-// (Ez, shared memory).  Then each warp takes one acceleration ja: E[y] = OR of
-// Ez over the v range of input j, F[i1] = OR of E over the y range of row i1,
-// and the x test runs 64 states at a time: the x boxes of a plane fall into a
-// few classes (lo - i0, hi - i0) = (a, b), and a state in class c is blocked
-// when F has a bit in [i0 + a, i0 + b], i.e. when bit i0 of
-// OR_{d=a..b} (F >> d) is set.  A plane with more than kClassMax classes uses
-// the per-state test.  The block then resolves the column in input order, so
-// every state records the lowest satisfied input.
-template <int W, bool NV>
-__global__ void __launch_bounds__(kFusedWarps * 32) k_sat_fused(GridInfo g, FusedFixArgs a) {
-    extern __shared__ __align__(16) uint64_t smem[];
-    __shared__ int s_wlo, s_whi;
-    const FixControl* fc = a.fc;
-    if (fc->stop) return;
-    const uint32_t it = fc->iter + 1;
-    const uint64_t* __restrict__ rprev = (fc->iter & 1) ? a.reach1 : a.reach0;
-    uint64_t* __restrict__ rnext = (fc->iter & 1) ? a.reach0 : a.reach1;
-    const uint32_t n0 = g.n[0], n1 = g.n[1], n2 = g.n[2], ma = g.ma;
-    const uint32_t nw = n1 * W;
-    const uint32_t slice = blockIdx.x;
-    const uint32_t i2 = slice % n2, i3 = slice / n2;
-    const uint64_t wbase = static_cast<uint64_t>(slice) * nw;
-    const uint32_t tid = threadIdx.x, bd = blockDim.x;
-    const uint32_t warp = tid >> 5, lane = tid & 31;
-    const uint32_t nv = NV ? 2u : 1u;
-
-    uint64_t* act = smem;
-    uint64_t* fnd = act + nw;
-    uint64_t* Ez = fnd + nw;                       // ez_rows * nw (+ the same for valid)
-    uint64_t* sat = Ez + a.ez_rows * nw * nv;      // ma * nw
-    uint64_t* mine = sat + ma * nw + warp * (nw * nv + a.cls_words);
-    uint64_t* E = mine;                            // nw (+ nw valid)
-    uint64_t* cls = mine + nw * nv;                // class record of the warp's plane
-
-    int any = 0;
-    for (uint32_t e = tid; e < nw; e += bd) {
-        const uint64_t v = a.active[wbase + e];
-        act[e] = v;
-        fnd[e] = 0;
-        any |= (v != 0);
-    }
-    if (tid == 0) {
-        int lo = 1 << 30, hi = -1;
-        for (uint32_t ja = 0; ja < ma; ++ja) {
-            const uint32_t we = a.wt[i3 * ma + ja];
-            if (we == kReject) continue;
-            lo = min(lo, static_cast<int>(lo16(we)));
-            hi = max(hi, static_cast<int>(hi16(we)));
-        }
-        s_wlo = lo;
-        s_whi = hi;
-    }
-    any = __syncthreads_or(any);
-    const int wlo = s_wlo, whi = s_whi;
-    if (!any || whi < wlo) {
-        for (uint32_t e = tid; e < nw; e += bd) rnext[wbase + e] = rprev[wbase + e];
-        return;
-    }
-    const uint32_t nwu = static_cast<uint32_t>(whi - wlo + 1);
-    unsigned long long ntest = 0, nplane = 0;
-    for (uint32_t jw = 0; jw < g.mw; ++jw) {
-        const uint32_t ze = a.zt[i2 * g.mw + jw];
-        const uint32_t lz = lo16(ze), hz = hi16(ze);
-        for (uint32_t e = tid; e < nwu * nw; e += bd) {
-            const uint32_t wr = e / nw, rem = e - wr * nw;
-            const uint32_t y = rem / W, w = rem - y * W;
-            const uint64_t wv = static_cast<uint64_t>(wlo) + wr;
-            uint64_t acc = 0, accv = 0;
-            uint32_t z = lz;
-            for (;;) {
-                const uint64_t r = y + static_cast<uint64_t>(n1) * (z + static_cast<uint64_t>(n2) * wv);
-                acc |= __ldg(a.dp + r * W + w);
-                if (NV) accv |= __ldg(a.validb + r * W + w);
-                if (z == hz) break;
-                z = (z + 1 == n2) ? 0 : z + 1;
-            }
-            Ez[e] = acc;
-            if (NV) Ez[nwu * nw + e] = accv;
-        }
-        __syncthreads();
-        for (uint32_t ja = warp; ja < ma; ja += kFusedWarps) {
-            const uint32_t j = ja + ma * jw;
-            uint64_t* Sj = sat + ja * nw;
-            const uint32_t we = a.wt[i3 * ma + ja];
-            if (we == kReject) {
-                for (uint32_t e = lane; e < nw; e += 32) Sj[e] = 0;
-                continue;
-            }
-            nplane += (lane == 0);
-            const uint32_t lw = lo16(we) - wlo, hw = hi16(we) - wlo;
-            const uint64_t plane = (static_cast<uint64_t>(i2) * g.n[3] + i3) * g.M + j;
-            for (uint32_t e = lane; e < a.cls_words; e += 32) cls[e] = __ldg(a.xcls + plane * a.cls_words + e);
-            for (uint32_t e = lane; e < nw; e += 32) {
-                uint64_t acc = 0, accv = 0;
-                for (uint32_t wr = lw; wr <= hw; ++wr) {
-                    acc |= Ez[wr * nw + e];
-                    if (NV) accv |= Ez[(nwu + wr) * nw + e];
-                }
-                E[e] = acc;
-                if (NV) E[nw + e] = accv;
-            }
-            __syncwarp();
-            const uint64_t h0 = cls[0], h1 = cls[1];
-            const uint32_t ncls = static_cast<uint32_t>(h0 & 0xFFu);
-            uint64_t okm[W];
-#pragma unroll
-            for (int w = 0; w < W; ++w) okm[w] = 0;
-            if (ncls != 0xFFu) {
-                for (uint32_t c = 0; c < ncls; ++c) {
-#pragma unroll
-                    for (int w = 0; w < W; ++w) okm[w] |= cls[2 + c * W + w];
-                }
-            }
-            for (uint32_t i1 = lane; i1 < n1; i1 += 32) {
-                uint64_t cm[W], sw[W];
-                bool anyc = false;
-#pragma unroll
-                for (int w = 0; w < W; ++w) {
-                    cm[w] = act[i1 * W + w] & ~fnd[i1 * W + w];
-                    sw[w] = 0;
-                    anyc |= cm[w] != 0;
-                }
-                const uint32_t ye = anyc ? __ldg(a.yt + plane * n1 + i1) : kReject;
-                if (ye != kReject) {
-#pragma unroll
-                    for (int w = 0; w < W; ++w) ntest += __popcll(cm[w]);
-                    uint64_t F[W], FV[W];
-#pragma unroll
-                    for (int w = 0; w < W; ++w) F[w] = FV[w] = 0;
-                    for (uint32_t y = lo16(ye); y <= hi16(ye); ++y) {
-#pragma unroll
-                        for (int w = 0; w < W; ++w) {
-                            F[w] |= E[y * W + w];
-                            if (NV) FV[w] |= E[nw + y * W + w];
-                        }
-                    }
-                    if (ncls != 0xFFu) {
-                        uint64_t U[W], VA[W];
-#pragma unroll
-                        for (int w = 0; w < W; ++w) U[w] = VA[w] = 0;
-                        for (uint32_t c = 0; c < ncls; ++c) {
-                            const int ca = static_cast<int8_t>((h0 >> (8 * (c + 1))) & 0xFFu);
-                            const int cb = static_cast<int8_t>((h1 >> (8 * c)) & 0xFFu);
-                            uint64_t win[W], winv[W];
-#pragma unroll
-                            for (int w = 0; w < W; ++w) win[w] = winv[w] = 0;
-                            for (int d = ca; d <= cb; ++d) {
-                                or_shifted<W>(F, d, win);
-                                if (NV) or_shifted<W>(FV, d, winv);
-                            }
-#pragma unroll
-                            for (int w = 0; w < W; ++w) {
-                                const uint64_t m = cls[2 + c * W + w];
-                                U[w] |= win[w] & m;
-                                VA[w] |= winv[w] & m;
-                            }
-                        }
-#pragma unroll
-                        for (int w = 0; w < W; ++w) sw[w] = cm[w] & okm[w] & ~U[w] & (NV ? VA[w] : ~0ull);
-                    } else {
-                        const uint32_t* xrow = a.xt + plane * n0;
-#pragma unroll
-                        for (int w = 0; w < W; ++w) {
-                            uint64_t m = cm[w];
-                            while (m) {
-                                const uint32_t b = __ffsll(static_cast<long long>(m)) - 1;
-                                m &= m - 1;
-                                const uint32_t xe = __ldg(xrow + w * 64 + b);
-                                if (xe == kReject) continue;
-                                const uint32_t lx = lo16(xe), hx = hi16(xe);
-                                bool ok = extract_bits<W>(F, lx, hx) == 0;
-                                if (NV) ok = ok && extract_bits<W>(FV, lx, hx) != 0;
-                                if (ok) sw[w] |= 1ull << b;
-                            }
-                        }
-                    }
-                }
-#pragma unroll
-                for (int w = 0; w < W; ++w) Sj[i1 * W + w] = sw[w];
-            }
-        }
-        __syncthreads();
-        // Resolve the column in input order: the lowest satisfied input wins.
-        int left = 0;
-        for (uint32_t e = tid; e < nw; e += bd) {
-            uint64_t f = fnd[e];
-            uint64_t open = act[e] & ~f;
-            const uint64_t srow = (static_cast<uint64_t>(slice) * n1 + e / W) * n0 + (e % W) * 64;
-            for (uint32_t ja = 0; ja < ma && open; ++ja) {
-                const uint64_t nb = sat[ja * nw + e] & open;
-                if (!nb) continue;
-                open &= ~nb;
-                f |= nb;
-                uint64_t m = nb;
-                while (m) {
-                    const uint32_t b = __ffsll(static_cast<long long>(m)) - 1;
-                    m &= m - 1;
-                    a.controller[srow + b] = ja + ma * jw;
-                }
-            }
-            fnd[e] = f;
-            left |= (open != 0);
-        }
-        if (!__syncthreads_or(left)) break;
-    }
-    unsigned long long nr = 0, nc = 0;
-    for (uint32_t e = tid; e < nw; e += bd) {
-        const uint64_t f = fnd[e];
-        const uint64_t gi = wbase + e;
-        const uint64_t rp = rprev[gi];
-        rnext[gi] = rp | f;
-        if (f) {
-            a.active[gi] = act[e] & ~f;
-            const uint64_t c = a.candb[gi];
-            nr += __popcll(f & ~rp);
-            nc += __popcll(f & c);
-            uint64_t m = f & ~c;
-            const uint64_t sbase = (static_cast<uint64_t>(slice) * n1 + e / W) * n0 + (e % W) * 64;
-            while (m) {
-                const uint32_t b = __ffsll(static_cast<long long>(m)) - 1;
-                m &= m - 1;
-                a.reach_step[sbase + b] = it;
-            }
-        }
-    }
-    for (int off = 16; off > 0; off >>= 1) {
-        nr += __shfl_down_sync(0xFFFFFFFFu, nr, off);
-        nc += __shfl_down_sync(0xFFFFFFFFu, nc, off);
-        ntest += __shfl_down_sync(0xFFFFFFFFu, ntest, off);
-        nplane += __shfl_down_sync(0xFFFFFFFFu, nplane, off);
-    }
-    if ((tid & 31) == 0) {
-        unsigned long long* row = a.stats + kStatsCols * it;
-        if (nr) atomicAdd(row, nr);
-        if (nc) atomicAdd(row + 1, nc);
-        if (ntest) atomicAdd(row + 2, ntest);
-        if (nplane) atomicAdd(row + 3, nplane);
-    }
-}
-
-template <int W, bool NV>
-cudaError_t launch_sat_fused_t(const GridInfo& g, const FusedFixArgs& a, size_t sm, cudaStream_t st) {
-    // The opt-in above 48 KB is a per-device function attribute: set it once per device.
-    static bool configured[64] = {};
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= 64 || !configured[dev]) {
-        e = cudaFuncSetAttribute(k_sat_fused<W, NV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(kFusedSmemMax));
-        if (e != cudaSuccess) return e;
-        if (dev >= 0 && dev < 64) configured[dev] = true;
-    }
-    k_sat_fused<W, NV><<<g.slices, kFusedWarps * 32, sm, st>>>(g, a);
-    return cudaGetLastError();
-}
-
-}  // namespace
-
-size_t fused_smem_bytes(const GridInfo& g, uint32_t ez_rows, uint32_t cls_words, int need_valid) {
-    const size_t nw = static_cast<size_t>(g.n[1]) * g.W;
-    const size_t nv = need_valid ? 2 : 1;
-    return 8 * (2 * nw + ez_rows * nw * nv + g.ma * nw + kFusedWarps * (nw * nv + cls_words));
-}
-
-namespace {
 }  // namespace
 
 cudaError_t launch_prefix4(const GridInfo& g, int mode, const uint8_t* a, const uint8_t* b, int32_t* table,
@@ -630,40 +297,6 @@ cudaError_t launch_stored_iteration(const GridInfo& g, const StoredFixArgs& a, c
     if (ev) cudaEventRecord(ev[2], st);
     k_control<<<1, 1, 0, st>>>(a.fc, a.stats, a.cond, a.use_cond);
     if (launches) *launches += 6;
-    return cudaGetLastError();
-}
-
-cudaError_t launch_fused_init(const GridInfo& g, const FusedFixArgs& a, const uint8_t* cand, cudaStream_t st) {
-    k_fused_init<<<blocks_for(g.S, 256), 256, 0, st>>>(g, a, cand);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_fused_iteration(const GridInfo& g, const FusedFixArgs& a, cudaStream_t st, uint32_t* launches,
-                                   cudaEvent_t* ev) {
-    if (ev) cudaEventRecord(ev[0], st);
-    k_fused_dp<<<blocks_for(g.rows * g.W, 256), 256, 0, st>>>(g, a);
-    if (ev) cudaEventRecord(ev[1], st);
-    const size_t sm = fused_smem_bytes(g, a.ez_rows, a.cls_words, a.need_valid);
-    cudaError_t err;
-    if (a.need_valid) {
-        switch (g.W) {
-            case 1: err = launch_sat_fused_t<1, true>(g, a, sm, st); break;
-            case 2: err = launch_sat_fused_t<2, true>(g, a, sm, st); break;
-            case 3: err = launch_sat_fused_t<3, true>(g, a, sm, st); break;
-            default: err = launch_sat_fused_t<4, true>(g, a, sm, st); break;
-        }
-    } else {
-        switch (g.W) {
-            case 1: err = launch_sat_fused_t<1, false>(g, a, sm, st); break;
-            case 2: err = launch_sat_fused_t<2, false>(g, a, sm, st); break;
-            case 3: err = launch_sat_fused_t<3, false>(g, a, sm, st); break;
-            default: err = launch_sat_fused_t<4, false>(g, a, sm, st); break;
-        }
-    }
-    if (err != cudaSuccess) return err;
-    if (ev) cudaEventRecord(ev[2], st);
-    k_control<<<1, 1, 0, st>>>(a.fc, a.stats, a.cond, a.use_cond);
-    if (launches) *launches += 3;
     return cudaGetLastError();
 }
 

@@ -35,12 +35,12 @@ cudaError_t launch_axis_tables(const GridInfo& g, const QueryInfo& q, const doub
                                const double* thf, const double* vf, uint32_t* xt, uint32_t* yt, uint32_t* zt,
                                uint32_t* wt, unsigned int* flags, cudaStream_t st);
 
-// Bit-sliced sets: bit i0 of word w of x-row r is state r*n0 + 64*w + i0.
+// Bit-sliced sets: bit b of word w of x-row r is state r*n0 + 32*w + b.
 // mode 0: bit = src[s] != 0; 1: bit = src[s] == 0; 2: bit = src2d[i1*n0 + i0] == 0;
 // 3: bit = src[s] != 0 && src2d[i1*n0+i0] != 0; 4: bit = src[s] != 0 && src[s] (4-D second) != 0
-cudaError_t launch_pack_bits(const GridInfo& g, int mode, const uint8_t* src, const uint8_t* src2, uint64_t* out,
+cudaError_t launch_pack_bits(const GridInfo& g, int mode, const uint8_t* src, const uint8_t* src2, bword* out,
                              cudaStream_t st);
-cudaError_t launch_unpack_bits(const GridInfo& g, const uint64_t* bits, uint8_t* out, cudaStream_t st);
+cudaError_t launch_unpack_bits(const GridInfo& g, const bword* bits, uint8_t* out, cudaStream_t st);
 
 // Counts cells with valid != safe (safe rank 2 or 4) into *count.
 cudaError_t launch_valid_vs_safe(const GridInfo& g, const uint8_t* valid, const uint8_t* safe, int safe_rank,
@@ -103,22 +103,26 @@ cudaError_t launch_stored_iteration(const GridInfo& g, const StoredFixArgs& a, c
 
 struct FusedFixArgs {
     const uint32_t *xt, *yt, *zt, *wt;
-    const uint64_t* validb;
-    const uint64_t* unsafeb;
-    const uint64_t* srcb;      // valid && source-safe
-    const uint64_t* candb;
-    uint64_t* dp;
-    uint64_t* reach0;
-    uint64_t* reach1;
-    uint64_t* active;
+    const bword* validb;
+    const bword* unsafeb;
+    const bword* srcb;         // valid && source-safe
+    const bword* candb;
+    bword* dp;
+    bword* reach0;
+    bword* reach1;
+    bword* active;
+    bword* hit;                // states satisfied this iteration (cleared by the finalize kernel)
+    uint32_t* best;            // lowest satisfied input per state this iteration (else 0xFFFFFFFF)
     uint32_t* controller;
     uint32_t* reach_step;
     FixControl* fc;
     unsigned long long* stats;
     int need_valid;
-    const uint64_t* xcls;      // per-plane x-box classes (launch_x_classes)
-    uint32_t cls_words;        // 64-bit words per class record
+    const bword* xcls;         // per-plane x-box classes (launch_x_classes)
+    const uint8_t* xrep;       // per plane: the first acceleration of its omega column with identical boxes
+    uint32_t cls_words;        // 32-bit words per class record
     uint32_t ez_rows;          // max number of v rows reachable from one v cell
+    uint32_t max_reps;         // max representative accelerations of one omega column
     cudaGraphConditionalHandle cond;
     int use_cond;
 };
@@ -126,12 +130,19 @@ constexpr int kFusedWarps = 4;
 constexpr int kClassMax = 6;
 constexpr size_t kFusedSmemMax = 200 * 1024;
 // Dynamic shared memory of the fused satisfaction kernel.
-size_t fused_smem_bytes(const GridInfo& g, uint32_t ez_rows, uint32_t cls_words, int need_valid);
-// Class record words per plane: 2 header words + kClassMax * W masks.
-inline uint32_t class_words(const GridInfo& g) { return 2 + kClassMax * g.W; }
-// Per (slice, input) plane: the classes (lo - i0, hi - i0) of its x boxes
-// (header word 0: count (0xFF = irregular) | a[c] << 8(c+1); word 1: b[c] << 8c).
-cudaError_t launch_x_classes(const GridInfo& g, const uint32_t* xt, uint64_t* xcls, cudaStream_t st);
+size_t fused_smem_bytes(const GridInfo& g, uint32_t ez_rows, uint32_t cls_words, int need_valid, uint32_t max_reps);
+// Class record words per plane: a 16-byte header + kClassMax * W masks.
+inline uint32_t class_words(const GridInfo& g) { return 4 + kClassMax * g.W; }
+// Per (slice, input) plane: the classes (lo - i0, hi - i0) = (a, b) of its x
+// boxes.  Header bytes: [0] count (0xFF = irregular), [1 + c] a[c], [7 + c]
+// b[c] (int8); then the state mask of each class.  |a|, |b| < 32.
+cudaError_t launch_x_classes(const GridInfo& g, const uint32_t* xt, bword* xcls, cudaStream_t st);
+// Per plane (slice, j = ja + ma * jw): the lowest ja' of the same omega column
+// whose x row, y row and v box equal those of ja, so the two inputs test every
+// state alike (with one Euler substep the x and y successors do not depend on
+// the acceleration at all).
+cudaError_t launch_plane_reps(const GridInfo& g, const uint32_t* xt, const uint32_t* yt, const uint32_t* wt,
+                              uint8_t* xrep, cudaStream_t st);
 cudaError_t launch_fused_init(const GridInfo& g, const FusedFixArgs& a, const uint8_t* cand, cudaStream_t st);
 cudaError_t launch_fused_iteration(const GridInfo& g, const FusedFixArgs& a, cudaStream_t st, uint32_t* launches,
                                    cudaEvent_t* ev = nullptr);

@@ -168,7 +168,7 @@ __global__ void k_axis_tables(GridInfo g, QueryInfo q, const double* __restrict_
             const bool ok = axis_box(g, d, (is_x ? xn : yn)[ee], r, &lo, &hi);
             (is_x ? xt : yt)[ee] = ok ? pack16(lo, hi) : kReject;
             if (ok && hi < lo) fl |= 1u;
-            if (ok && hi >= lo && hi - lo >= 64) fl |= 2u;
+            if (ok && hi >= lo && hi - lo >= kBits) fl |= 2u;
         } else if (e < nx + ny + nz) {
             const uint32_t ee = static_cast<uint32_t>(e - nx - ny);   // i2 * mw + jw
             const double r = box_radius(g, q, 2, 0.0);
@@ -190,7 +190,7 @@ __global__ void k_axis_tables(GridInfo g, QueryInfo q, const double* __restrict_
 // ---- bit-sliced sets --------------------------------------------------------------------
 
 __global__ void k_pack_bits(GridInfo g, int mode, const uint8_t* __restrict__ src, const uint8_t* __restrict__ src2,
-                            uint64_t* __restrict__ out) {
+                            bword* __restrict__ out) {
     const uint64_t words = g.rows * g.W;
     for (uint64_t e = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; e < words;
          e += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
@@ -198,9 +198,9 @@ __global__ void k_pack_bits(GridInfo g, int mode, const uint8_t* __restrict__ sr
         const uint32_t w = static_cast<uint32_t>(e - r * g.W);
         const uint32_t i1 = static_cast<uint32_t>(r % g.n[1]);
         const uint64_t base = r * g.n[0];
-        uint64_t word = 0;
-        for (uint32_t b = 0; b < 64; ++b) {
-            const uint32_t i0 = w * 64 + b;
+        bword word = 0;
+        for (uint32_t b = 0; b < kBits; ++b) {
+            const uint32_t i0 = w * kBits + b;
             if (i0 >= g.n[0]) break;
             bool bit;
             switch (mode) {
@@ -210,18 +210,18 @@ __global__ void k_pack_bits(GridInfo g, int mode, const uint8_t* __restrict__ sr
                 case 3: bit = src[base + i0] != 0 && src2[i1 * g.n[0] + i0] != 0; break;
                 default: bit = src[base + i0] != 0 && src2[base + i0] != 0; break;
             }
-            word |= static_cast<uint64_t>(bit) << b;
+            word |= static_cast<bword>(bit) << b;
         }
         out[e] = word;
     }
 }
 
-__global__ void k_unpack_bits(GridInfo g, const uint64_t* __restrict__ bits, uint8_t* __restrict__ out) {
+__global__ void k_unpack_bits(GridInfo g, const bword* __restrict__ bits, uint8_t* __restrict__ out) {
     for (uint64_t s = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; s < g.S;
          s += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
         const uint64_t r = s / g.n[0];
         const uint32_t i0 = static_cast<uint32_t>(s - r * g.n[0]);
-        out[s] = static_cast<uint8_t>((bits[r * g.W + (i0 >> 6)] >> (i0 & 63)) & 1u);
+        out[s] = static_cast<uint8_t>((bits[r * g.W + i0 / kBits] >> (i0 % kBits)) & 1u);
     }
 }
 
@@ -370,15 +370,16 @@ __global__ void k_export(GridInfo g, ExportArgs a) {
 }
 
 // Classes of the x boxes of one (slice, input) plane: states whose box is
-// [i0 + a, i0 + b] share the class (a, b).  Up to kClassMax classes, else the
-// plane is marked irregular (0xFF) and tested state by state.
-__global__ void k_x_classes(GridInfo g, const uint32_t* __restrict__ xt, uint64_t* __restrict__ out) {
-    const uint32_t cw = 2 + kClassMax * g.W;
+// [i0 + a, i0 + b] share the class (a, b).  Up to kClassMax classes with
+// |a|, |b| < 32, else the plane is marked irregular (0xFF) and tested state
+// by state.
+__global__ void k_x_classes(GridInfo g, const uint32_t* __restrict__ xt, bword* __restrict__ out) {
+    const uint32_t cw = 4 + kClassMax * g.W;
     const uint64_t planes = static_cast<uint64_t>(g.slices) * g.M;
     for (uint64_t plane = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; plane < planes;
          plane += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
         int cnt = 0, A[kClassMax], B[kClassMax];
-        uint64_t masks[kClassMax][kMaxWords];
+        bword masks[kClassMax][kMaxWords];
         for (int c = 0; c < kClassMax; ++c)
             for (int w = 0; w < kMaxWords; ++w) masks[c][w] = 0;
         bool irregular = false;
@@ -387,7 +388,7 @@ __global__ void k_x_classes(GridInfo g, const uint32_t* __restrict__ xt, uint64_
             if (xe == kReject) continue;
             const int a = static_cast<int>(lo16(xe)) - static_cast<int>(i0);
             const int b = static_cast<int>(hi16(xe)) - static_cast<int>(i0);
-            if (a < -63 || a > 63 || b < -63 || b > 63 || b < a) {
+            if (a < -31 || a > 31 || b < -31 || b > 31 || b < a) {
                 irregular = true;
                 break;
             }
@@ -402,20 +403,49 @@ __global__ void k_x_classes(GridInfo g, const uint32_t* __restrict__ xt, uint64_
                 B[cnt] = b;
                 ++cnt;
             }
-            masks[c][i0 >> 6] |= 1ull << (i0 & 63);
+            masks[c][i0 / kBits] |= bword(1) << (i0 % kBits);
         }
-        uint64_t h0 = irregular ? 0xFFull : static_cast<uint64_t>(cnt), h1 = 0;
+        uint8_t hdr[16] = {};
+        hdr[0] = irregular ? 0xFF : static_cast<uint8_t>(cnt);
         if (!irregular) {
             for (int c = 0; c < cnt; ++c) {
-                h0 |= static_cast<uint64_t>(static_cast<uint8_t>(A[c])) << (8 * (c + 1));
-                h1 |= static_cast<uint64_t>(static_cast<uint8_t>(B[c])) << (8 * c);
+                hdr[1 + c] = static_cast<uint8_t>(static_cast<int8_t>(A[c]));
+                hdr[7 + c] = static_cast<uint8_t>(static_cast<int8_t>(B[c]));
             }
         }
-        uint64_t* o = out + plane * cw;
-        o[0] = h0;
-        o[1] = h1;
+        bword* o = out + plane * cw;
+        for (int k = 0; k < 4; ++k)
+            o[k] = static_cast<bword>(hdr[4 * k]) | (static_cast<bword>(hdr[4 * k + 1]) << 8) |
+                   (static_cast<bword>(hdr[4 * k + 2]) << 16) | (static_cast<bword>(hdr[4 * k + 3]) << 24);
         for (int c = 0; c < kClassMax; ++c)
-            for (uint32_t w = 0; w < g.W; ++w) o[2 + c * g.W + w] = irregular ? 0 : masks[c][w];
+            for (uint32_t w = 0; w < g.W; ++w) o[4 + c * g.W + w] = irregular ? 0 : masks[c][w];
+    }
+}
+
+__global__ void k_plane_reps(GridInfo g, const uint32_t* __restrict__ xt, const uint32_t* __restrict__ yt,
+                             const uint32_t* __restrict__ wt, uint8_t* __restrict__ rep) {
+    const uint64_t columns = static_cast<uint64_t>(g.slices) * g.mw;
+    for (uint64_t col = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; col < columns;
+         col += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        // Planes are ((i2 * n3 + i3) * M + j) with j = ja + ma * jw, so column
+        // col = (i2 * n3 + i3) * mw + jw starts at plane col * ma.
+        const uint32_t i3 = static_cast<uint32_t>((col / g.mw) % g.n[3]);
+        const uint64_t p0 = col * g.ma;
+        for (uint32_t ja = 0; ja < g.ma; ++ja) {
+            uint32_t r = ja;
+            for (uint32_t jb = 0; jb < ja; ++jb) {
+                if (rep[p0 + jb] != jb) continue;
+                if (wt[i3 * g.ma + jb] != wt[i3 * g.ma + ja]) continue;
+                bool same = true;
+                for (uint32_t i = 0; i < g.n[0] && same; ++i) same = xt[(p0 + jb) * g.n[0] + i] == xt[(p0 + ja) * g.n[0] + i];
+                for (uint32_t i = 0; i < g.n[1] && same; ++i) same = yt[(p0 + jb) * g.n[1] + i] == yt[(p0 + ja) * g.n[1] + i];
+                if (same) {
+                    r = jb;
+                    break;
+                }
+            }
+            rep[p0 + ja] = static_cast<uint8_t>(r);
+        }
     }
 }
 
@@ -469,13 +499,13 @@ cudaError_t launch_axis_tables(const GridInfo& g, const QueryInfo& q, const doub
     return cudaGetLastError();
 }
 
-cudaError_t launch_pack_bits(const GridInfo& g, int mode, const uint8_t* src, const uint8_t* src2, uint64_t* out,
+cudaError_t launch_pack_bits(const GridInfo& g, int mode, const uint8_t* src, const uint8_t* src2, bword* out,
                              cudaStream_t st) {
     k_pack_bits<<<blocks_for(g.rows * g.W), kThreads, 0, st>>>(g, mode, src, src2, out);
     return cudaGetLastError();
 }
 
-cudaError_t launch_unpack_bits(const GridInfo& g, const uint64_t* bits, uint8_t* out, cudaStream_t st) {
+cudaError_t launch_unpack_bits(const GridInfo& g, const bword* bits, uint8_t* out, cudaStream_t st) {
     k_unpack_bits<<<blocks_for(g.S), kThreads, 0, st>>>(g, bits, out);
     return cudaGetLastError();
 }
@@ -496,8 +526,14 @@ cudaError_t launch_stored_build(const GridInfo& g, const StoredBuildArgs& a, cud
     return cudaGetLastError();
 }
 
-cudaError_t launch_x_classes(const GridInfo& g, const uint32_t* xt, uint64_t* xcls, cudaStream_t st) {
+cudaError_t launch_x_classes(const GridInfo& g, const uint32_t* xt, bword* xcls, cudaStream_t st) {
     k_x_classes<<<blocks_for(static_cast<uint64_t>(g.slices) * g.M, 128), 128, 0, st>>>(g, xt, xcls);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_plane_reps(const GridInfo& g, const uint32_t* xt, const uint32_t* yt, const uint32_t* wt,
+                              uint8_t* xrep, cudaStream_t st) {
+    k_plane_reps<<<blocks_for(static_cast<uint64_t>(g.slices) * g.mw, 128), 128, 0, st>>>(g, xt, yt, wt, xrep);
     return cudaGetLastError();
 }
 
