@@ -71,8 +71,10 @@ struct gsc_problem {
     uint32_t* best = nullptr;
     bword* xcls = nullptr;
     uint8_t* xrep = nullptr;
-    uint32_t ez_rows = 0;
     uint32_t max_reps = 0;
+    bword *dzw = nullptr, *vzw = nullptr;
+    uint8_t *kidx = nullptr, *lidx = nullptr;
+    DilateArgs dil{};
     int need_valid = 0;
     // common fixpoint state
     uint32_t* controller = nullptr;
@@ -513,29 +515,42 @@ int build_problem(gsc_problem* p, const gsc_query_desc* qd, uint32_t method) {
     p->valid_count = hc[0];
     p->candidate_count = hc[1];
     if (hflags != 0) fused_ok = false;   // an empty or over-wide interval: only the stored count is exact
-    // The fused kernel stages, per v cell, every v row its inputs can reach.
+    // The fused kernel reads (theta, v)-dilated copies of D', one per pair of
+    // theta and v box widths that occurs.
+    std::vector<uint8_t> hk(g.n[2] + 1, 0xFF), hl(g.n[3] + 1, 0xFF);
     {
-        std::vector<uint32_t> hw(static_cast<size_t>(g.n[3]) * g.ma);
+        std::vector<uint32_t> hz(static_cast<size_t>(g.n[2]) * g.mw), hw(static_cast<size_t>(g.n[3]) * g.ma);
+        GSC_CU(ctx, cudaMemcpy(hz.data(), p->zt, hz.size() * 4, cudaMemcpyDeviceToHost));
         GSC_CU(ctx, cudaMemcpy(hw.data(), p->wt, hw.size() * 4, cudaMemcpyDeviceToHost));
-        uint32_t rows = 1;
-        for (uint32_t i3 = 0; i3 < g.n[3]; ++i3) {
-            int lo = 1 << 30, hi = -1;
-            for (uint32_t ja = 0; ja < g.ma; ++ja) {
-                const uint32_t we = hw[static_cast<size_t>(i3) * g.ma + ja];
-                if (we == kReject) continue;
-                lo = std::min(lo, static_cast<int>(lo16(we)));
-                hi = std::max(hi, static_cast<int>(hi16(we)));
-            }
-            if (hi >= lo) rows = std::max<uint32_t>(rows, static_cast<uint32_t>(hi - lo + 1));
+        std::vector<char> kin(g.n[2] + 1, 0), lin(g.n[3] + 1, 0);
+        for (uint32_t ze : hz) {
+            const uint32_t lz = lo16(ze), hz2 = hi16(ze);
+            kin[lz <= hz2 ? hz2 - lz + 1 : g.n[2] - lz + hz2 + 1] = 1;
         }
-        p->ez_rows = rows;
+        for (uint32_t we : hw)
+            if (we != kReject && hi16(we) >= lo16(we)) lin[hi16(we) - lo16(we) + 1] = 1;
+        DilateArgs d{};
+        for (uint32_t k = 1; k <= g.n[2]; ++k)
+            if (kin[k]) {
+                if (d.nk == kMaxDilate) { fused_ok = false; break; }
+                hk[k] = static_cast<uint8_t>(d.nk);
+                d.kval[d.nk++] = k;
+            }
+        for (uint32_t l = 1; l <= g.n[3]; ++l)
+            if (lin[l]) {
+                if (d.nl == kMaxDilate || l > static_cast<uint32_t>(kMaxDilate)) { fused_ok = false; break; }
+                hl[l] = static_cast<uint8_t>(d.nl);
+                d.lval[d.nl++] = l;
+            }
+        if (d.nk == 0 || d.nl == 0) fused_ok = false;
+        p->dil = d;
         const int nv = p->safe ? (hc[4] != 0) : (hc[0] != g.S);
-        if (fused_smem_bytes(g, rows, class_words(g), nv, g.ma) > kFusedSmemMax) fused_ok = false;
+        if (fused_smem_bytes(g, class_words(g), nv, g.ma) > kFusedSmemMax) fused_ok = false;
     }
     if (method == GSC_METHOD_AUTO) method = fused_ok ? GSC_METHOD_FUSED : (stored_ok ? GSC_METHOD_STORED : 0);
     if (method == 0) return fail(ctx, GSC_ERR_UNSUPPORTED, "no method applies to this grid");
     if (method == GSC_METHOD_FUSED && !fused_ok)
-        return fail(ctx, GSC_ERR_UNSUPPORTED, "fused method: an interval is empty or wider than 64 cells");
+        return fail(ctx, GSC_ERR_UNSUPPORTED, "fused method: an interval is empty or wider than 32 cells, or too many box widths");
     p->method = method;
     // need the valid-cell test when some cell's validity is not its safety
     p->need_valid = p->safe ? (hc[4] != 0) : (p->valid_count != g.S);
@@ -593,6 +608,12 @@ int build_problem(gsc_problem* p, const gsc_query_desc* qd, uint32_t method) {
         GSC_TRY(dalloc(ctx, A, B, &p->active, words));
         GSC_TRY(dalloc(ctx, A, B, &p->hit, words));
         GSC_TRY(dalloc(ctx, A, B, &p->best, g.S));
+        const uint64_t combos = static_cast<uint64_t>(p->dil.nk) * p->dil.nl;
+        GSC_TRY(dalloc(ctx, A, B, &p->dzw, combos * words));
+        GSC_TRY(dalloc(ctx, A, B, &p->kidx, hk.size()));
+        GSC_TRY(dalloc(ctx, A, B, &p->lidx, hl.size()));
+        GSC_CU(ctx, cudaMemcpyAsync(p->kidx, hk.data(), hk.size(), cudaMemcpyHostToDevice, st));
+        GSC_CU(ctx, cudaMemcpyAsync(p->lidx, hl.data(), hl.size(), cudaMemcpyHostToDevice, st));
         GSC_TRY(dalloc(ctx, A, B, &p->xcls, static_cast<uint64_t>(g.slices) * g.M * class_words(g)));
         GSC_CU(ctx, launch_x_classes(g, p->xt, p->xcls, st));
         GSC_TRY(dalloc(ctx, A, B, &p->xrep, static_cast<uint64_t>(g.slices) * g.M));
@@ -622,6 +643,10 @@ int build_problem(gsc_problem* p, const gsc_query_desc* qd, uint32_t method) {
         } else {
             GSC_CU(ctx, launch_pack_bits(g, 1, p->safe, nullptr, p->unsafeb, st));
             GSC_CU(ctx, launch_pack_bits(g, 4, p->valid, p->safe, p->srcb, st));
+        }
+        if (p->need_valid) {
+            GSC_TRY(dalloc(ctx, A, B, &p->vzw, combos * words));
+            GSC_CU(ctx, launch_dilate(g, p->validb, p->vzw, p->dil, nullptr, st));
         }
     }
     GSC_CU(ctx, cudaMemcpyAsync(hc, p->counts, sizeof(hc), cudaMemcpyDeviceToHost, st));
@@ -671,8 +696,13 @@ FusedFixArgs fused_args(gsc_problem* p, cudaGraphConditionalHandle cond, int use
     a.xcls = p->xcls;
     a.xrep = p->xrep;
     a.cls_words = class_words(p->g);
-    a.ez_rows = p->ez_rows;
     a.max_reps = p->max_reps;
+    a.dzw = p->dzw;
+    a.vzw = p->vzw;
+    a.kidx = p->kidx;
+    a.lidx = p->lidx;
+    a.nl = p->dil.nl;
+    a.dil = p->dil;
     a.cond = cond;
     a.use_cond = use_cond;
     return a;
@@ -778,7 +808,7 @@ int gsc_problem_solve(gsc_problem* p, uint32_t flags) {
     uint32_t launches = 0;
     double sat_ms = 0.0, scan_ms = 0.0;
     uint32_t sat_launches = 0;
-    const uint32_t per_iter = (p->method == GSC_METHOD_STORED) ? 6 : 2;
+    const uint32_t per_iter = (p->method == GSC_METHOD_STORED) ? 6 : 3;
     if (flags & GSC_SOLVE_PROFILE) {
         GSC_CU(ctx, enqueue_init(p));
         launches += 2;

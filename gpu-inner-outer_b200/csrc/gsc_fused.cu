@@ -5,13 +5,14 @@
 // satisfied input, reach_step = iteration, stop rules in the reference's
 // order), as in the stored method.
 //
-// Data: every set is a bit slice, one 64-bit word per 64 x-cells of a
+// Data: every set is a bit slice, one 32-bit word per 32 x-cells of a
 // (y, theta, v) row.  D' = (valid && !reachable) || unsafe.  A pair is
 // satisfied when its box holds no D' cell (so every cell is safe, and every
 // valid cell already reachable) and, when validity is more than safety, at
 // least one valid cell.
 //
-// One iteration = two launches:
+// One iteration = three launches:
+//   k_dilate         (theta, v)-dilated copies of D' for the box widths in use;
 //   k_sat_col        one block per (theta, v) slice x omega column: tests
 //                    every active state of the slice against every input of
 //                    the column and, per state, records the lowest satisfied
@@ -80,23 +81,65 @@ __global__ void k_fused_init(GridInfo g, FusedFixArgs a, const uint8_t* __restri
     }
 }
 
-// One block per (theta, v) slice x omega column jw.  The column's inputs
-// share the theta range of their boxes, so:
-//  A. Ez[v row][y] = OR of the D' rows over that theta range, for every v row
-//     the column's inputs reach;
-//  B. E[ja][y] = OR of Ez over input ja's v range (with the column's x-box
-//     class records and y tables staged beside it);
-//  C. each (ja, i1) item: F = OR of E[ja] over row i1's y range, then the x
-//     test 32 states per word: the x boxes of a plane fall into a few classes
-//     (lo - i0, hi - i0) = (a, b), and a state of class (a, b) is blocked when
-//     F has a bit in [i0 + a, i0 + b], i.e. bit i0 of OR_{d=a..b} (F >> d); a
-//     plane with more than kClassMax classes is tested state by state;
+// (theta, v)-dilated copies of a bit-sliced set: for every theta width k in
+// d.kval and v width l in d.lval, out[combo][y][z][v] = OR of src over
+// theta cells z .. z+k-1 (wrapped) and v cells v .. v+l-1 (entries whose v
+// window leaves the grid are never read and are left 0).  One thread per
+// word position; the theta ORs are extended incrementally.
+__global__ void k_dilate(GridInfo g, const bword* __restrict__ src, bword* __restrict__ dst, DilateArgs d,
+                         const FixControl* fc) {
+    if (fc && fc->stop) return;
+    const uint32_t n1 = g.n[1], n2 = g.n[2], n3 = g.n[3], W = g.W;
+    const uint32_t pos = static_cast<uint32_t>(g.rows * W);
+    const uint32_t kmax = d.kval[d.nk - 1];
+    uint32_t lmax = d.lval[d.nl - 1];
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < pos; p += gridDim.x * blockDim.x) {
+        const uint32_t r = p / W, wd = p - r * W;
+        const uint32_t y = r % n1, q = r / n1;
+        const uint32_t z = q % n2, v = q / n2;
+        const uint32_t lfit = min(lmax, n3 - v);   // v windows that stay inside the grid
+        bword zor[kMaxDilate];
+#pragma unroll
+        for (uint32_t j = 0; j < kMaxDilate; ++j) zor[j] = 0;
+        uint32_t ki = 0, zz = z;
+        for (uint32_t i = 0; i < kmax; ++i) {
+#pragma unroll
+            for (uint32_t j = 0; j < kMaxDilate; ++j)
+                if (j < lfit) zor[j] |= __ldg(src + (y + n1 * (zz + n2 * (v + j))) * W + wd);
+            zz = (zz + 1 == n2) ? 0 : zz + 1;
+            if (i + 1 == d.kval[ki]) {
+                bword acc = 0;
+                uint32_t li = 0;
+#pragma unroll
+                for (uint32_t j = 0; j < kMaxDilate; ++j) {
+                    acc |= zor[j];
+                    if (li < d.nl && j + 1 == d.lval[li]) {
+                        dst[static_cast<uint64_t>(ki * d.nl + li) * pos + p] = (j < lfit) ? acc : 0u;
+                        ++li;
+                    }
+                }
+                ++ki;
+            }
+        }
+    }
+}
+
+// One block per (theta, v) slice x omega column jw.
+//  B. per representative acceleration (the lowest of each group of inputs
+//     whose boxes coincide), E[y] = the (theta, v)-dilated D' row at the
+//     input's box corner: one load per word;
+//  C. each (representative, i1) item: F = OR of E over row i1's y range, then
+//     the x test 32 states per word: the x boxes of a plane fall into a few
+//     classes (lo - i0, hi - i0) = (a, b), and a state of class (a, b) is
+//     blocked when F has a bit in [i0 + a, i0 + b], i.e. bit i0 of
+//     OR_{d=a..b} (F >> d); a plane with more than kClassMax classes is tested
+//     state by state;
 //  D. per state, the lowest satisfied input of the column goes to best[]
 //     (atomicMin, so the lowest over all columns wins) and the hit bit is set.
 template <int W, bool NV>
 __global__ void __launch_bounds__(kFusedWarps * 32) k_sat_col(GridInfo g, FusedFixArgs a) {
     extern __shared__ __align__(16) bword smem[];
-    __shared__ int s_wlo, s_whi;
+    __shared__ uint32_t s_nrep;
     const FixControl* fc = a.fc;
     if (fc->stop) return;
     const uint32_t n0 = g.n[0], n1 = g.n[1], n2 = g.n[2], ma = g.ma, mw = g.mw;
@@ -105,106 +148,61 @@ __global__ void __launch_bounds__(kFusedWarps * 32) k_sat_col(GridInfo g, FusedF
     const uint32_t i2 = slice % n2, i3 = slice / n2;
     const uint64_t wbase = static_cast<uint64_t>(slice) * nw;
     const uint32_t tid = threadIdx.x, bd = blockDim.x;
+    const uint32_t lane = tid & 31;
     const uint32_t nv = NV ? 2u : 1u;
     const uint32_t cw = a.cls_words;
-
     const uint32_t mr = a.max_reps;
+    const uint32_t pos = static_cast<uint32_t>(g.rows * W);
+
     bword* act = smem;
-    bword* Ez = act + nw;                                 // ez_rows * nw * nv
-    bword* Eall = Ez + a.ez_rows * nw * nv;               // max_reps * nw * nv
+    bword* Eall = act + nw;                               // max_reps * nw * nv
     bword* sat = Eall + mr * nw * nv;                     // max_reps * nw
     bword* cls = sat + mr * nw;                           // max_reps * cw
     uint32_t* yts = cls + mr * cw;                        // max_reps * n1
-    uint32_t* wts = yts + mr * n1;                        // ma
-    uint32_t* slot = wts + ma;                            // ma: representative slot of each acceleration
-    uint32_t* reps = slot + ma;                           // ma: acceleration of each slot
-    __shared__ uint32_t s_nrep;
+    uint32_t* reps = yts + mr * n1;                       // ma: acceleration of each representative slot
 
+    const uint64_t pcol = (static_cast<uint64_t>(i2) * g.n[3] + i3) * g.M + static_cast<uint64_t>(ma) * jw;
     int any = 0;
     for (uint32_t e = tid; e < nw; e += bd) {
         const bword v = a.active[wbase + e];
         act[e] = v;
         any |= (v != 0);
     }
-    for (uint32_t ja = tid; ja < ma; ja += bd) wts[ja] = a.wt[i3 * ma + ja];
-    const uint64_t pcol = (static_cast<uint64_t>(i2) * g.n[3] + i3) * g.M + static_cast<uint64_t>(ma) * jw;
-    if (tid == 0) {
-        int lo = 1 << 30, hi = -1;
-        uint32_t nrep = 0;
-        for (uint32_t ja = 0; ja < ma; ++ja) {
-            const uint32_t we = a.wt[i3 * ma + ja];
-            if (we != kReject) {
-                lo = min(lo, static_cast<int>(lo16(we)));
-                hi = max(hi, static_cast<int>(hi16(we)));
-            }
-            const uint32_t r = a.xrep[pcol + ja];
-            if (r == ja) {
-                reps[nrep] = ja;
-                slot[ja] = nrep++;
-            } else {
-                slot[ja] = slot[r];
-            }
+    if (tid < 32) {
+        // Representatives in increasing acceleration order (warp ballot).
+        uint32_t n = 0;
+        for (uint32_t base = 0; base < ma; base += 32) {
+            const uint32_t ja = base + lane;
+            const bool is_rep = ja < ma && a.xrep[pcol + ja] == ja && a.wt[i3 * ma + ja] != kReject;
+            const uint32_t m = __ballot_sync(0xFFFFFFFFu, is_rep);
+            if (is_rep) reps[n + __popc(m & ((1u << lane) - 1))] = ja;
+            n += __popc(m);
         }
-        s_wlo = lo;
-        s_whi = hi;
-        s_nrep = nrep;
+        if (lane == 0) s_nrep = n;
     }
     any = __syncthreads_or(any);
-    const int wlo = s_wlo, whi = s_whi;
-    if (!any || whi < wlo) return;
-    const uint32_t nwu = static_cast<uint32_t>(whi - wlo + 1);
     const uint32_t nrep = s_nrep;
+    if (!any || nrep == 0) return;
 
-    // A. theta-range ORs; an item's loads are issued together.
+    // B. dilated D' rows at each representative's (theta, v) box corner.
     const uint32_t ze = a.zt[i2 * mw + jw];
     const uint32_t lz = lo16(ze), hz = hi16(ze);
     const uint32_t nz = (lz <= hz) ? hz - lz + 1 : n2 - lz + hz + 1;
-    const uint32_t zstride = n1 * W;                      // words between theta planes
-    for (uint32_t e = tid; e < nwu * nw; e += bd) {
-        const uint32_t wr = fdiv(e, g.magic_nw), rem = e - wr * nw;
-        const uint32_t rowbase = n1 * n2 * W * (static_cast<uint32_t>(wlo) + wr) + rem;
-        bword acc = 0, accv = 0;
-        uint32_t z = lz;
-        for (uint32_t k = 0; k < nz; k += 4) {
-            bword v[4], vv[4];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const bool in = k + u < nz;
-                // lanes past the range read a valid row and discard it
-                const uint32_t zz = !in ? lz : (z + u >= n2) ? z + u - n2 : z + u;
-                const uint32_t r = rowbase + zstride * zz;
-                v[u] = in ? __ldg(a.dp + r) : 0u;
-                vv[u] = (NV && in) ? __ldg(a.validb + r) : 0u;
-            }
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                acc |= v[u];
-                accv |= vv[u];
-            }
-            z = (z + 4 >= n2) ? z + 4 - n2 : z + 4;
-        }
-        Ez[e] = acc;
-        if (NV) Ez[nwu * nw + e] = accv;
+    const uint32_t kslot = a.kidx[nz];
+    for (uint32_t e = tid; e < nrep * nw; e += bd) {
+        const uint32_t r = fdiv(e, g.magic_nw), rem = e - r * nw;
+        const uint32_t y = rem / W, wd = rem - y * W;
+        const uint32_t we = a.wt[i3 * ma + reps[r]];
+        const uint32_t lw = lo16(we), nwb = hi16(we) - lw + 1;
+        const uint64_t off = static_cast<uint64_t>(kslot * a.nl + a.lidx[nwb]) * pos +
+                             (y + n1 * (lz + n2 * lw)) * W + wd;
+        Eall[r * nw * nv + rem] = __ldg(a.dzw + off);
+        if (NV) Eall[r * nw * nv + nw + rem] = __ldg(a.vzw + off);
     }
     for (uint32_t r = tid >> 5; r < nrep; r += bd >> 5) {
         const uint64_t pl = pcol + reps[r];
-        for (uint32_t e = tid & 31; e < cw; e += 32) cls[r * cw + e] = __ldg(a.xcls + pl * cw + e);
-        for (uint32_t e = tid & 31; e < n1; e += 32) yts[r * n1 + e] = __ldg(a.yt + pl * n1 + e);
-    }
-    __syncthreads();
-    // B. v-range ORs per representative acceleration.
-    for (uint32_t e = tid; e < nrep * nw; e += bd) {
-        const uint32_t r = fdiv(e, g.magic_nw), rem = e - r * nw;
-        const uint32_t we = wts[reps[r]];
-        bword acc = 0, accv = 0;
-        if (we != kReject) {
-            for (uint32_t wr = lo16(we) - wlo; wr <= hi16(we) - wlo; ++wr) {
-                acc |= Ez[wr * nw + rem];
-                if (NV) accv |= Ez[(nwu + wr) * nw + rem];
-            }
-        }
-        Eall[r * nw * nv + rem] = acc;
-        if (NV) Eall[r * nw * nv + nw + rem] = accv;
+        for (uint32_t e = lane; e < cw; e += 32) cls[r * cw + e] = __ldg(a.xcls + pl * cw + e);
+        for (uint32_t e = lane; e < n1; e += 32) yts[r * n1 + e] = __ldg(a.yt + pl * n1 + e);
     }
     __syncthreads();
     // C. the (representative, row) items.
@@ -221,7 +219,7 @@ __global__ void __launch_bounds__(kFusedWarps * 32) k_sat_col(GridInfo g, FusedF
             anyc |= cm[w];
         }
         const uint32_t ye = yts[r * n1 + i1];
-        if (anyc && ye != kReject && wts[ja] != kReject) {
+        if (anyc && ye != kReject) {
             nplane += (i1 == 0);
 #pragma unroll
             for (int w = 0; w < W; ++w) ntest += __popc(cm[w]);
@@ -284,21 +282,25 @@ __global__ void __launch_bounds__(kFusedWarps * 32) k_sat_col(GridInfo g, FusedF
         for (int w = 0; w < W; ++w) sat[r * nw + i1 * W + w] = sw[w];
     }
     __syncthreads();
-    // D. lowest satisfied input of the column per state -> best[] and hit bits.
+    // D. lowest satisfied input of the column per state -> best[] and hit
+    // bits.  Representatives are in increasing order and each is the lowest
+    // input of its group, so the first representative that satisfies a state
+    // gives its lowest satisfied input of the column.
     for (uint32_t e = tid; e < nw; e += bd) {
         bword open = act[e], got = 0;
         const uint32_t y = e / W;
         const uint64_t srow = (static_cast<uint64_t>(slice) * n1 + y) * n0 + (e - y * W) * kBits;
-        for (uint32_t ja = 0; ja < ma && open; ++ja) {
-            const bword nb = sat[slot[ja] * nw + e] & open;
+        for (uint32_t r = 0; r < nrep && open; ++r) {
+            const bword nb = sat[r * nw + e] & open;
             if (!nb) continue;
             open &= ~nb;
             got |= nb;
+            const uint32_t j = reps[r] + ma * jw;
             bword m = nb;
             while (m) {
                 const uint32_t b = __ffs(m) - 1;
                 m &= m - 1;
-                atomicMin(a.best + srow + b, ja + ma * jw);
+                atomicMin(a.best + srow + b, j);
             }
         }
         if (got) atomicOr(a.hit + wbase + e, got);
@@ -414,13 +416,21 @@ cudaError_t launch_sat_col_t(const GridInfo& g, const FusedFixArgs& a, size_t sm
 
 }  // namespace
 
-size_t fused_smem_bytes(const GridInfo& g, uint32_t ez_rows, uint32_t cls_words, int need_valid, uint32_t max_reps) {
+size_t fused_smem_bytes(const GridInfo& g, uint32_t cls_words, int need_valid, uint32_t max_reps) {
     const size_t nw = static_cast<size_t>(g.n[1]) * g.W;
     const size_t nv = need_valid ? 2 : 1;
     const size_t mr = max_reps;
-    const size_t words = nw + ez_rows * nw * nv + mr * nw * nv + mr * nw + mr * cls_words +
-                         mr * g.n[1] + 3 * static_cast<size_t>(g.ma);
+    const size_t words = nw + mr * nw * nv + mr * nw + mr * cls_words + mr * g.n[1] + static_cast<size_t>(g.ma);
     return sizeof(bword) * words;
+}
+
+cudaError_t launch_dilate(const GridInfo& g, const bword* src, bword* dst, const DilateArgs& d, const FixControl* fc,
+                          cudaStream_t st) {
+    const uint64_t pos = g.rows * g.W;
+    uint64_t b = (pos + 255) / 256;
+    if (b > 8192) b = 8192;
+    k_dilate<<<static_cast<unsigned int>(b ? b : 1), 256, 0, st>>>(g, src, dst, d, fc);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_fused_init(const GridInfo& g, const FusedFixArgs& a, const uint8_t* cand, cudaStream_t st) {
@@ -431,8 +441,10 @@ cudaError_t launch_fused_init(const GridInfo& g, const FusedFixArgs& a, const ui
 cudaError_t launch_fused_iteration(const GridInfo& g, const FusedFixArgs& a, cudaStream_t st, uint32_t* launches,
                                    cudaEvent_t* ev) {
     if (ev) cudaEventRecord(ev[0], st);
+    cudaError_t derr = launch_dilate(g, a.dp, a.dzw, a.dil, a.fc, st);
+    if (derr != cudaSuccess) return derr;
     if (ev) cudaEventRecord(ev[1], st);
-    const size_t sm = fused_smem_bytes(g, a.ez_rows, a.cls_words, a.need_valid, a.max_reps);
+    const size_t sm = fused_smem_bytes(g, a.cls_words, a.need_valid, a.max_reps);
     cudaError_t err;
 #define GSC_SAT_CASE(Wn)                                                                         \
     case Wn:                                                                                     \
@@ -457,7 +469,7 @@ cudaError_t launch_fused_iteration(const GridInfo& g, const FusedFixArgs& a, cud
     uint64_t fb = (words + 255) / 256;
     if (fb > 4096) fb = 4096;
     k_fused_finalize<<<static_cast<unsigned int>(fb ? fb : 1), 256, 0, st>>>(g, a);
-    if (launches) *launches += 2;
+    if (launches) *launches += 3;
     return cudaGetLastError();
 }
 

@@ -101,6 +101,15 @@ cudaError_t launch_stored_init(const GridInfo& g, const StoredFixArgs& a, cudaSt
 cudaError_t launch_stored_iteration(const GridInfo& g, const StoredFixArgs& a, cudaStream_t st, uint32_t* launches,
                                     cudaEvent_t* ev = nullptr);
 
+// Box widths present in a problem: theta widths kval[0..nk) and v widths
+// lval[0..nl), ascending; combo (ki, li) indexes the dilated copies.
+constexpr int kMaxDilate = 8;
+struct DilateArgs {
+    uint32_t nk, nl;
+    uint32_t kval[kMaxDilate];
+    uint32_t lval[kMaxDilate];
+};
+
 struct FusedFixArgs {
     const uint32_t *xt, *yt, *zt, *wt;
     const bword* validb;
@@ -121,8 +130,13 @@ struct FusedFixArgs {
     const bword* xcls;         // per-plane x-box classes (launch_x_classes)
     const uint8_t* xrep;       // per plane: the first acceleration of its omega column with identical boxes
     uint32_t cls_words;        // 32-bit words per class record
-    uint32_t ez_rows;          // max number of v rows reachable from one v cell
     uint32_t max_reps;         // max representative accelerations of one omega column
+    bword* dzw;                // (theta, v)-dilated D' [combo][rows * W], rebuilt each iteration
+    const bword* vzw;          // (theta, v)-dilated valid set (when validity is more than safety)
+    const uint8_t* kidx;       // [n2 + 1]: theta width -> its slot in dil.kval
+    const uint8_t* lidx;       // [n3 + 1]: v width -> its slot in dil.lval
+    uint32_t nl;
+    DilateArgs dil;
     cudaGraphConditionalHandle cond;
     int use_cond;
 };
@@ -130,7 +144,9 @@ constexpr int kFusedWarps = 4;
 constexpr int kClassMax = 6;
 constexpr size_t kFusedSmemMax = 200 * 1024;
 // Dynamic shared memory of the fused satisfaction kernel.
-size_t fused_smem_bytes(const GridInfo& g, uint32_t ez_rows, uint32_t cls_words, int need_valid, uint32_t max_reps);
+size_t fused_smem_bytes(const GridInfo& g, uint32_t cls_words, int need_valid, uint32_t max_reps);
+cudaError_t launch_dilate(const GridInfo& g, const bword* src, bword* dst, const DilateArgs& d, const FixControl* fc,
+                          cudaStream_t st);
 // Class record words per plane: a 16-byte header + kClassMax * W masks.
 inline uint32_t class_words(const GridInfo& g) { return 4 + kClassMax * g.W; }
 // Per (slice, input) plane: the classes (lo - i0, hi - i0) = (a, b) of its x
