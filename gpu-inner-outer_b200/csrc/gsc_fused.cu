@@ -183,6 +183,7 @@ __global__ void __launch_bounds__(kFusedWarps * 32) k_sat_col(GridInfo g, FusedF
     any = __syncthreads_or(any);
     const uint32_t nrep = s_nrep;
     if (!any || nrep == 0) return;
+    if (tid == 0) atomicAdd(a.stats + kStatsCols * (fc->iter + 1) + 3, static_cast<unsigned long long>(nrep));
 
     // B. dilated D' rows at each representative's (theta, v) box corner.
     const uint32_t ze = a.zt[i2 * mw + jw];
@@ -206,7 +207,7 @@ __global__ void __launch_bounds__(kFusedWarps * 32) k_sat_col(GridInfo g, FusedF
     }
     __syncthreads();
     // C. the (representative, row) items.
-    unsigned long long ntest = 0, nplane = 0;
+    unsigned long long ntest = 0;
     for (uint32_t e = tid; e < nrep * n1; e += bd) {
         const uint32_t r = fdiv(e, g.magic_n1), i1 = e - r * n1;
         const uint32_t ja = reps[r];
@@ -220,7 +221,6 @@ __global__ void __launch_bounds__(kFusedWarps * 32) k_sat_col(GridInfo g, FusedF
         }
         const uint32_t ye = yts[r * n1 + i1];
         if (anyc && ye != kReject) {
-            nplane += (i1 == 0);
 #pragma unroll
             for (int w = 0; w < W; ++w) ntest += __popc(cm[w]);
             const bword* E = Eall + r * nw * nv;
@@ -305,16 +305,8 @@ __global__ void __launch_bounds__(kFusedWarps * 32) k_sat_col(GridInfo g, FusedF
         }
         if (got) atomicOr(a.hit + wbase + e, got);
     }
-    for (int off = 16; off > 0; off >>= 1) {
-        ntest += __shfl_down_sync(0xFFFFFFFFu, ntest, off);
-        nplane += __shfl_down_sync(0xFFFFFFFFu, nplane, off);
-    }
-    if ((tid & 31) == 0) {
-        const uint32_t it = fc->iter + 1;
-        unsigned long long* row = a.stats + kStatsCols * it;
-        if (ntest) atomicAdd(row + 2, ntest);
-        if (nplane) atomicAdd(row + 3, nplane);
-    }
+    for (int off = 16; off > 0; off >>= 1) ntest += __shfl_down_sync(0xFFFFFFFFu, ntest, off);
+    if ((tid & 31) == 0 && ntest) atomicAdd(a.stats + kStatsCols * (fc->iter + 1) + 2, ntest);
 }
 
 // Apply the iteration's hits, build next iteration's D', count, and let the

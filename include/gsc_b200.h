@@ -167,11 +167,13 @@ typedef struct {
     uint32_t iterations;            /* fixpoint iterations of the last solve      */
     uint32_t sat_launches;          /* satisfaction-kernel launches timed         */
     double sat_kernel_ms;           /* GSC_SOLVE_PROFILE: satisfaction kernels    */
-    double scan_kernel_ms;          /* GSC_SOLVE_PROFILE: set / prefix rebuilds   */
+    double scan_kernel_ms;          /* GSC_SOLVE_PROFILE: set / prefix rebuilds
+                                       (fused: the (theta, v) dilation)           */
     uint64_t pair_tests;            /* stored: boxes streamed; fused: (state,
                                        input) tests, summed over iterations       */
     uint64_t aux_count;             /* stored: box counts evaluated; fused:
-                                       (slice, input) plane tasks                 */
+                                       (slice, representative input) planes
+                                       staged, summed over iterations             */
 } gsc_timings;
 
 typedef struct gsc_context gsc_context;
