@@ -13,104 +13,15 @@
 #include <string>
 #include <vector>
 
-#include "../../include/gsc_b200.h"
-#include "gsc_kernels.cuh"
+#include "gsc_internal.hpp"
 
 using namespace gsc_b200;
 
-struct gsc_context {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    bool own_stream = false;
-    std::string last_error;
-    uint64_t budget = 0;
-    uint64_t in_use = 0;
-    cudaEvent_t ev[2] = {nullptr, nullptr};
-};
-
-struct gsc_abstraction {
-    gsc_context* ctx = nullptr;
-    GridInfo g{};
-    gsc_model_desc model{};
-    double* xn = nullptr;
-    double* yn = nullptr;
-    double* thf = nullptr;
-    double* vf = nullptr;
-    uint64_t bytes = 0;
-    double build_ms = 0.0;
-};
-
-struct gsc_problem {
-    gsc_context* ctx = nullptr;
-    const gsc_abstraction* abs = nullptr;
-    GridInfo g{};
-    QueryInfo q{};
-    uint32_t method = 0;
-    std::vector<void*> allocs;
-    uint64_t bytes = 0;
-    // masks and tables
-    uint8_t* valid = nullptr;
-    uint8_t* cand = nullptr;
-    uint8_t* safe = nullptr;
-    int safe_rank = 0;
-    double* obstacles = nullptr;
-    unsigned long long* counts = nullptr;   // [0] valid [1] cand [2] cand-not-valid [3] valid pairs [4] valid!=safe
-    unsigned int* flags = nullptr;
-    uint32_t *xt = nullptr, *yt = nullptr, *zt = nullptr, *wt = nullptr;
-    int32_t* unsafe2 = nullptr;
-    int32_t* unsafe4 = nullptr;
-    int32_t* pvalid = nullptr;
-    // stored
-    uint2* boxes = nullptr;
-    uint64_t S_pad = 0;
-    int32_t* pd = nullptr;
-    uint8_t* reach8 = nullptr;
-    // fused
-    bword *validb = nullptr, *unsafeb = nullptr, *srcb = nullptr, *candb = nullptr, *dp = nullptr;
-    bword *reach0 = nullptr, *reach1 = nullptr, *active = nullptr, *hit = nullptr;
-    uint32_t* best = nullptr;
-    bword* xcls = nullptr;
-    uint8_t* xrep = nullptr;
-    uint32_t max_reps = 0;
-    bword *dzw = nullptr, *vzw = nullptr;
-    uint8_t *kidx = nullptr, *lidx = nullptr;
-    DilateArgs dil{};
-    int need_valid = 0;
-    // common fixpoint state
-    uint32_t* controller = nullptr;
-    uint32_t* reach_step = nullptr;
-    FixControl* fc = nullptr;
-    unsigned long long* stats = nullptr;
-    uint32_t stats_cap = 0;
-    uint64_t valid_count = 0, candidate_count = 0, valid_pairs = 0;
-    // graph
-    cudaGraphExec_t exec = nullptr;
-    cudaGraph_t graph = nullptr;
-    gsc_timings timings{};
-    ~gsc_problem();
-};
+using namespace gsc_api;
 
 namespace {
 
 constexpr uint32_t kStatsCapMax = 1u << 20;
-
-struct Fail {
-    int status;
-};
-
-int fail(gsc_context* ctx, int status, const std::string& msg) {
-    if (ctx) ctx->last_error = msg;
-    return status;
-}
-
-#define GSC_CU(ctx, expr)                                                                              \
-    do {                                                                                               \
-        cudaError_t e__ = (expr);                                                                      \
-        if (e__ != cudaSuccess) {                                                                      \
-            return fail((ctx), e__ == cudaErrorMemoryAllocation ? GSC_ERR_OUT_OF_MEMORY : GSC_ERR_CUDA, \
-                        std::string(#expr) + ": " + cudaGetErrorString(e__));                          \
-        }                                                                                              \
-    } while (0)
 
 // Reference wrap_angle (model.hpp:14-24).
 double wrap_angle(double x) {
@@ -120,6 +31,10 @@ double wrap_angle(double x) {
     while (x >= kPi) x -= kTwoPi;
     return x;
 }
+
+}  // namespace
+
+namespace gsc_api {
 
 int grid_from_model(const gsc_model_desc* m, GridInfo* g, std::string* err) {
     std::memset(g, 0, sizeof(*g));
@@ -199,37 +114,183 @@ int grid_from_model(const gsc_model_desc* m, GridInfo* g, std::string* err) {
     return GSC_OK;
 }
 
-template <typename T>
-int dalloc(gsc_context* ctx, std::vector<void*>& allocs, uint64_t& bytes, T** p, uint64_t count) {
-    const uint64_t nbytes = count * sizeof(T);
-    if (ctx->budget && ctx->in_use + nbytes > ctx->budget)
-        return fail(ctx, GSC_ERR_OUT_OF_MEMORY, "device memory budget exceeded");
+int device_alloc(gsc_context* ctx, DevicePool* pool, std::vector<std::pair<void*, uint64_t>>& allocs,
+                 uint64_t& bytes, void** p, uint64_t nbytes) {
+    *p = nullptr;
     void* q = nullptr;
-    cudaError_t e = cudaMalloc(&q, nbytes ? nbytes : 1);
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        return fail(ctx, GSC_ERR_OUT_OF_MEMORY, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    if (pool) {
+        q = pool->alloc(nbytes);
+        if (!q) return fail(ctx, GSC_ERR_OUT_OF_MEMORY, "device memory pool exhausted");
+    } else {
+        std::lock_guard<std::mutex> lk(ctx->mem_mu);
+        if (ctx->budget && ctx->in_use + nbytes > ctx->budget)
+            return fail(ctx, GSC_ERR_OUT_OF_MEMORY, "device memory budget exceeded");
+        const cudaError_t e = cudaMalloc(&q, nbytes ? nbytes : 1);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return fail(ctx, GSC_ERR_OUT_OF_MEMORY, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        }
+        ctx->in_use += nbytes;
     }
-    allocs.push_back(q);
+    allocs.emplace_back(q, nbytes);
     bytes += nbytes;
-    ctx->in_use += nbytes;
-    *p = static_cast<T*>(q);
+    *p = q;
     return GSC_OK;
 }
 
-#define GSC_TRY(expr)              \
-    do {                           \
-        int s__ = (expr);          \
-        if (s__ != GSC_OK) return s__; \
-    } while (0)
+void device_release_all(gsc_context* ctx, DevicePool* pool, std::vector<std::pair<void*, uint64_t>>& allocs,
+                        uint64_t& bytes) {
+    for (auto& pr : allocs) {
+        if (pool) {
+            pool->release(pr.first, pr.second);
+        } else {
+            cudaFree(pr.first);
+            if (ctx) ctx->in_use -= pr.second;
+        }
+    }
+    allocs.clear();
+    bytes = 0;
+}
 
-}  // namespace
+int abstraction_enqueue(gsc_abstraction* a, cudaStream_t st, std::vector<std::pair<void*, uint64_t>>& tmp) {
+    gsc_context* ctx = a->ctx;
+    const GridInfo& g = a->g;
+    const uint32_t K = g.K;
+    // Host tabulation of the theta and v trajectories (model.hpp:34-45).
+    std::vector<double> host;   // cos | sin | vseq | thf | vf
+    const size_t ncs = static_cast<size_t>(g.n[2]) * g.mw * K, nvs = static_cast<size_t>(g.n[3]) * g.ma * K;
+    const size_t nth = static_cast<size_t>(g.n[2]) * g.mw, nvf = static_cast<size_t>(g.n[3]) * g.ma;
+    host.resize(2 * ncs + nvs + nth + nvf);
+    double* cosT = host.data();
+    double* sinT = cosT + ncs;
+    double* vseq = sinT + ncs;
+    double* thf = vseq + nvs;
+    double* vf = thf + nth;
+    for (uint32_t i2 = 0; i2 < g.n[2]; ++i2) {
+        for (uint32_t jw = 0; jw < g.mw; ++jw) {
+            double th = g.lb[2] + (static_cast<double>(i2) + 0.5) * g.eta[2];
+            const double omega = g.ilb[1] + (static_cast<double>(jw) + 0.5) * g.ieta[1];
+            const size_t base = (static_cast<size_t>(i2) * g.mw + jw) * K;
+            for (uint32_t k = 0; k < K; ++k) {
+                cosT[base + k] = std::cos(th);
+                sinT[base + k] = std::sin(th);
+                th = wrap_angle(th + g.dt * omega);
+            }
+            thf[static_cast<size_t>(i2) * g.mw + jw] = th;
+        }
+    }
+    for (uint32_t i3 = 0; i3 < g.n[3]; ++i3) {
+        for (uint32_t ja = 0; ja < g.ma; ++ja) {
+            double v = g.lb[3] + (static_cast<double>(i3) + 0.5) * g.eta[3];
+            const double acc = g.ilb[0] + (static_cast<double>(ja) + 0.5) * g.ieta[0];
+            const size_t base = (static_cast<size_t>(i3) * g.ma + ja) * K;
+            for (uint32_t k = 0; k < K; ++k) {
+                vseq[base + k] = v;
+                v += g.dt * acc;
+            }
+            vf[static_cast<size_t>(i3) * g.ma + ja] = v;
+        }
+    }
+    const uint64_t planes = static_cast<uint64_t>(g.slices) * g.M;
+    void* q = nullptr;
+    GSC_TRY(device_alloc(ctx, a->pool, a->allocs, a->bytes, &q, planes * g.n[0] * 8));
+    a->xn = static_cast<double*>(q);
+    GSC_TRY(device_alloc(ctx, a->pool, a->allocs, a->bytes, &q, planes * g.n[1] * 8));
+    a->yn = static_cast<double*>(q);
+    GSC_TRY(device_alloc(ctx, a->pool, a->allocs, a->bytes, &q, nth * 8));
+    a->thf = static_cast<double*>(q);
+    GSC_TRY(device_alloc(ctx, a->pool, a->allocs, a->bytes, &q, nvf * 8));
+    a->vf = static_cast<double*>(q);
+    uint64_t tmp_bytes = 0;
+    GSC_TRY(device_alloc(ctx, a->pool, tmp, tmp_bytes, &q, (2 * ncs + nvs) * 8));
+    double* d_tab = static_cast<double*>(q);
+    // One upload of the trajectory tables; cudaMemcpyAsync from pageable
+    // memory has returned once the source may be reused.
+    GSC_CU(ctx, cudaMemcpyAsync(d_tab, cosT, (2 * ncs + nvs) * 8, cudaMemcpyHostToDevice, st));
+    GSC_CU(ctx, cudaMemcpyAsync(a->thf, thf, nth * 8, cudaMemcpyHostToDevice, st));
+    GSC_CU(ctx, cudaMemcpyAsync(a->vf, vf, nvf * 8, cudaMemcpyHostToDevice, st));
+    GSC_CU(ctx, launch_nominal_xy(g, d_tab, d_tab + ncs, d_tab + 2 * ncs, a->xn, a->yn, st));
+    return GSC_OK;
+}
+
+int sm_count(gsc_context* ctx) { return ctx->sm_count > 0 ? ctx->sm_count : 148; }
+
+}  // namespace gsc_api
+
+DevicePool::~DevicePool() {
+    for (auto& s : slabs) {
+        cudaFree(s.base);
+        if (ctx) ctx->in_use -= s.bytes;
+    }
+}
+
+bool DevicePool::reserve(uint64_t bytes) {
+    std::lock_guard<std::mutex> lk(mu);
+    const uint64_t n = gsc_b200::RangePool::rounded(bytes);
+    {
+        std::lock_guard<std::mutex> lk2(ctx->mem_mu);
+        if (ctx->budget && ctx->in_use + n > ctx->budget) return false;
+        void* q = nullptr;
+        if (cudaMalloc(&q, n) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        ctx->in_use += n;
+        Slab s;
+        s.base = static_cast<char*>(q);
+        s.bytes = n;
+        s.ranges.reset(n);
+        slabs.push_back(std::move(s));
+    }
+    total += n;
+    return true;
+}
+
+void* DevicePool::alloc(uint64_t bytes) {
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        for (auto& s : slabs) {
+            const uint64_t off = s.ranges.alloc(bytes);
+            if (off != gsc_b200::RangePool::kNone) return s.base + off;
+        }
+        if (slab_bytes == 0) return nullptr;
+    }
+    uint64_t n = gsc_b200::RangePool::rounded(bytes);
+    if (n < slab_bytes) n = slab_bytes;
+    if (cap && total + n > cap) {
+        if (total + gsc_b200::RangePool::rounded(bytes) > cap) return nullptr;
+        n = cap - total;
+    }
+    if (!reserve(n)) return nullptr;
+    std::lock_guard<std::mutex> lk(mu);
+    const uint64_t off = slabs.back().ranges.alloc(bytes);
+    return off == gsc_b200::RangePool::kNone ? nullptr : slabs.back().base + off;
+}
+
+void DevicePool::release(void* p, uint64_t bytes) {
+    std::lock_guard<std::mutex> lk(mu);
+    char* c = static_cast<char*>(p);
+    for (auto& s : slabs) {
+        if (c >= s.base && c < s.base + s.bytes) {
+            s.ranges.release(static_cast<uint64_t>(c - s.base), bytes);
+            return;
+        }
+    }
+}
+
+uint64_t DevicePool::used() {
+    std::lock_guard<std::mutex> lk(mu);
+    uint64_t u = 0;
+    for (auto& s : slabs) u += s.ranges.used();
+    return u;
+}
+
+gsc_abstraction::~gsc_abstraction() { device_release_all(ctx, pool, allocs, bytes); }
 
 gsc_problem::~gsc_problem() {
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
-    for (void* p : allocs) cudaFree(p);
-    if (ctx) ctx->in_use -= bytes;
+    device_release_all(ctx, pool, allocs, bytes);
 }
 
 extern "C" {
@@ -295,6 +356,7 @@ int gsc_context_create(int device, void* cuda_stream, gsc_context** out) {
         }
         ctx->own_stream = true;
     }
+    cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device);
     if (cudaEventCreate(&ctx->ev[0]) != cudaSuccess || cudaEventCreate(&ctx->ev[1]) != cudaSuccess) {
         if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
         delete ctx;
@@ -321,7 +383,7 @@ int gsc_context_set_memory_budget(gsc_context* ctx, uint64_t bytes) {
     return GSC_OK;
 }
 
-uint64_t gsc_context_memory_in_use(const gsc_context* ctx) { return ctx ? ctx->in_use : 0; }
+uint64_t gsc_context_memory_in_use(const gsc_context* ctx) { return ctx ? ctx->in_use.load() : 0; }
 
 int gsc_abstraction_create(gsc_context* ctx, const gsc_model_desc* model, gsc_abstraction** out) {
     if (!ctx || !model || !out) return GSC_ERR_INVALID_ARGUMENT;
@@ -335,78 +397,21 @@ int gsc_abstraction_create(gsc_context* ctx, const gsc_model_desc* model, gsc_ab
     std::string err;
     const int s = grid_from_model(model, &a->g, &err);
     if (s != GSC_OK) return fail(ctx, s, err);
-    const GridInfo& g = a->g;
-    const uint32_t K = g.K;
-
-    // Host tabulation of the theta and v trajectories (model.hpp:34-45).
-    std::vector<double> cosT(static_cast<size_t>(g.n[2]) * g.mw * K), sinT(cosT.size());
-    std::vector<double> thf(static_cast<size_t>(g.n[2]) * g.mw), vf(static_cast<size_t>(g.n[3]) * g.ma);
-    std::vector<double> vseq(static_cast<size_t>(g.n[3]) * g.ma * K);
-    for (uint32_t i2 = 0; i2 < g.n[2]; ++i2) {
-        for (uint32_t jw = 0; jw < g.mw; ++jw) {
-            double th = g.lb[2] + (static_cast<double>(i2) + 0.5) * g.eta[2];
-            const double omega = g.ilb[1] + (static_cast<double>(jw) + 0.5) * g.ieta[1];
-            const size_t base = (static_cast<size_t>(i2) * g.mw + jw) * K;
-            for (uint32_t k = 0; k < K; ++k) {
-                cosT[base + k] = std::cos(th);
-                sinT[base + k] = std::sin(th);
-                th = wrap_angle(th + g.dt * omega);
-            }
-            thf[static_cast<size_t>(i2) * g.mw + jw] = th;
-        }
-    }
-    for (uint32_t i3 = 0; i3 < g.n[3]; ++i3) {
-        for (uint32_t ja = 0; ja < g.ma; ++ja) {
-            double v = g.lb[3] + (static_cast<double>(i3) + 0.5) * g.eta[3];
-            const double acc = g.ilb[0] + (static_cast<double>(ja) + 0.5) * g.ieta[0];
-            const size_t base = (static_cast<size_t>(i3) * g.ma + ja) * K;
-            for (uint32_t k = 0; k < K; ++k) {
-                vseq[base + k] = v;
-                v += g.dt * acc;
-            }
-            vf[static_cast<size_t>(i3) * g.ma + ja] = v;
-        }
-    }
-    std::vector<void*> allocs;
-    uint64_t bytes = 0;
-    const uint64_t planes = static_cast<uint64_t>(g.slices) * g.M;
-    double *d_cos = nullptr, *d_sin = nullptr, *d_vseq = nullptr;
-    auto cleanup_tmp = [&]() {
-        cudaFree(d_cos);
-        cudaFree(d_sin);
-        cudaFree(d_vseq);
-    };
-    int st = dalloc(ctx, allocs, bytes, &a->xn, planes * g.n[0]);
-    if (st == GSC_OK) st = dalloc(ctx, allocs, bytes, &a->yn, planes * g.n[1]);
-    if (st == GSC_OK) st = dalloc(ctx, allocs, bytes, &a->thf, thf.size());
-    if (st == GSC_OK) st = dalloc(ctx, allocs, bytes, &a->vf, vf.size());
-    if (st != GSC_OK) {
-        for (void* p : allocs) cudaFree(p);
-        ctx->in_use -= bytes;
-        return st;
-    }
-    a->bytes = bytes;
-    cudaError_t e = cudaMalloc(&d_cos, cosT.size() * sizeof(double));
-    if (e == cudaSuccess) e = cudaMalloc(&d_sin, sinT.size() * sizeof(double));
-    if (e == cudaSuccess) e = cudaMalloc(&d_vseq, vseq.size() * sizeof(double));
-    if (e == cudaSuccess) e = cudaMemcpyAsync(d_cos, cosT.data(), cosT.size() * 8, cudaMemcpyHostToDevice, ctx->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(d_sin, sinT.data(), sinT.size() * 8, cudaMemcpyHostToDevice, ctx->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(d_vseq, vseq.data(), vseq.size() * 8, cudaMemcpyHostToDevice, ctx->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(a->thf, thf.data(), thf.size() * 8, cudaMemcpyHostToDevice, ctx->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(a->vf, vf.data(), vf.size() * 8, cudaMemcpyHostToDevice, ctx->stream);
-    if (e == cudaSuccess) e = cudaEventRecord(ctx->ev[0], ctx->stream);
-    if (e == cudaSuccess) e = launch_nominal_xy(g, d_cos, d_sin, d_vseq, a->xn, a->yn, ctx->stream);
-    if (e == cudaSuccess) e = cudaEventRecord(ctx->ev[1], ctx->stream);
+    std::vector<std::pair<void*, uint64_t>> tmp;
+    uint64_t tmp_bytes = 0;
+    GSC_CU(ctx, cudaEventRecord(ctx->ev[0], ctx->stream));
+    int st = abstraction_enqueue(a.get(), ctx->stream, tmp);
+    cudaError_t e = cudaSuccess;
+    if (st == GSC_OK) e = cudaEventRecord(ctx->ev[1], ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    for (auto& t : tmp) tmp_bytes += t.second;
+    device_release_all(ctx, nullptr, tmp, tmp_bytes);
+    if (st != GSC_OK) return st;
     float ms = 0.f;
     if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);
-    cleanup_tmp();
-    if (e != cudaSuccess) {
-        for (void* p : allocs) cudaFree(p);
-        ctx->in_use -= bytes;
+    if (e != cudaSuccess)
         return fail(ctx, e == cudaErrorMemoryAllocation ? GSC_ERR_OUT_OF_MEMORY : GSC_ERR_CUDA,
                     std::string("abstraction: ") + cudaGetErrorString(e));
-    }
     a->build_ms = ms;
     *out = a.release();
     return GSC_OK;
@@ -415,11 +420,6 @@ int gsc_abstraction_create(gsc_context* ctx, const gsc_model_desc* model, gsc_ab
 void gsc_abstraction_destroy(gsc_abstraction* a) {
     if (!a) return;
     cudaSetDevice(a->ctx->device);
-    cudaFree(a->xn);
-    cudaFree(a->yn);
-    cudaFree(a->thf);
-    cudaFree(a->vf);
-    a->ctx->in_use -= a->bytes;
     delete a;
 }
 
@@ -427,12 +427,15 @@ void gsc_abstraction_destroy(gsc_abstraction* a) {
 
 namespace {
 
-int build_problem(gsc_problem* p, const gsc_query_desc* qd, uint32_t method) {
+}  // namespace
+
+namespace gsc_api {
+
+int problem_stage1(gsc_problem* p, const gsc_query_desc* qd) {
     gsc_context* ctx = p->ctx;
     const GridInfo& g = p->g;
-    cudaStream_t st = ctx->stream;
-    auto& A = p->allocs;
-    auto& B = p->bytes;
+    cudaStream_t st = p->stream;
+    const uint32_t method = p->method;
     QueryInfo& q = p->q;
     std::memset(&q, 0, sizeof(q));
     for (int d = 0; d < 4; ++d) {
@@ -454,24 +457,25 @@ int build_problem(gsc_problem* p, const gsc_query_desc* qd, uint32_t method) {
     for (int i = 0; i < 8; ++i) q.cand[i] = qd->candidate[i];
     q.max_iterations = qd->max_iterations;
 
-    // Method selection.
-    bool stored_ok = g.n[0] <= 255 && g.n[1] <= 255 && g.n[2] <= 255 && g.n[3] <= 255;
-    bool fused_ok = g.n[0] <= kBits * kMaxWords && g.ma <= 255;
+    // Method pre-check by shape.
+    const bool stored_ok = g.n[0] <= 255 && g.n[1] <= 255 && g.n[2] <= 255 && g.n[3] <= 255;
+    const bool fused_shape = g.n[0] <= kBits * kMaxWords && g.ma <= 255 && g.n[2] <= 65535 && g.n[3] <= 65535;
     if (method == GSC_METHOD_STORED && !stored_ok)
         return fail(ctx, GSC_ERR_UNSUPPORTED, "stored method needs at most 255 cells per dimension");
-    if (method == GSC_METHOD_FUSED && !fused_ok)
+    if (method == GSC_METHOD_FUSED && !fused_shape)
         return fail(ctx, GSC_ERR_UNSUPPORTED, "fused method needs at most 256 cells along x");
     if (method > GSC_METHOD_FUSED) return fail(ctx, GSC_ERR_INVALID_ARGUMENT, "unknown method");
+    p->fused_candidate = method != GSC_METHOD_STORED && fused_shape;
 
     // Masks.
-    GSC_TRY(dalloc(ctx, A, B, &p->valid, g.S));
-    GSC_TRY(dalloc(ctx, A, B, &p->cand, g.S));
-    GSC_TRY(dalloc(ctx, A, B, &p->counts, 8));
-    GSC_TRY(dalloc(ctx, A, B, &p->flags, 1));
+    GSC_TRY(palloc(p, &p->valid, g.S));
+    GSC_TRY(palloc(p, &p->cand, g.S));
+    GSC_TRY(palloc(p, &p->counts, 8));
+    GSC_TRY(palloc(p, &p->flags, 1));
     GSC_CU(ctx, cudaMemsetAsync(p->counts, 0, 8 * sizeof(unsigned long long), st));
     GSC_CU(ctx, cudaMemsetAsync(p->flags, 0, sizeof(unsigned int), st));
     if (qd->obstacle_count) {
-        GSC_TRY(dalloc(ctx, A, B, &p->obstacles, 8ull * qd->obstacle_count));
+        GSC_TRY(palloc(p, &p->obstacles, 8ull * qd->obstacle_count));
         GSC_CU(ctx, cudaMemcpyAsync(p->obstacles, qd->obstacles, 64ull * qd->obstacle_count, cudaMemcpyHostToDevice, st));
     }
     if (qd->valid_mask) GSC_CU(ctx, cudaMemcpyAsync(p->valid, qd->valid_mask, g.S, cudaMemcpyHostToDevice, st));
@@ -479,11 +483,11 @@ int build_problem(gsc_problem* p, const gsc_query_desc* qd, uint32_t method) {
     if (qd->safe_mask) {
         p->safe_rank = qd->safe_mask_rank;
         const uint64_t n = (p->safe_rank == 4) ? g.S : static_cast<uint64_t>(g.n[0]) * g.n[1];
-        GSC_TRY(dalloc(ctx, A, B, &p->safe, n));
+        GSC_TRY(palloc(p, &p->safe, n));
         GSC_CU(ctx, cudaMemcpyAsync(p->safe, qd->safe_mask, n, cudaMemcpyHostToDevice, st));
     } else if (q.ckind != GSC_CONSTRAINT_NONE) {
         p->safe_rank = 2;
-        GSC_TRY(dalloc(ctx, A, B, &p->safe, static_cast<uint64_t>(g.n[0]) * g.n[1]));
+        GSC_TRY(palloc(p, &p->safe, static_cast<uint64_t>(g.n[0]) * g.n[1]));
         GSC_CU(ctx, launch_safe2(g, q, p->safe, st));
     }
     MaskArgs ma{};
@@ -499,87 +503,87 @@ int build_problem(gsc_problem* p, const gsc_query_desc* qd, uint32_t method) {
 
     // Per-axis boxes.
     const uint64_t planes = static_cast<uint64_t>(g.slices) * g.M;
-    GSC_TRY(dalloc(ctx, A, B, &p->xt, planes * g.n[0]));
-    GSC_TRY(dalloc(ctx, A, B, &p->yt, planes * g.n[1]));
-    GSC_TRY(dalloc(ctx, A, B, &p->zt, static_cast<uint64_t>(g.n[2]) * g.mw));
-    GSC_TRY(dalloc(ctx, A, B, &p->wt, static_cast<uint64_t>(g.n[3]) * g.ma));
+    GSC_TRY(palloc(p, &p->xt, planes * g.n[0]));
+    GSC_TRY(palloc(p, &p->yt, planes * g.n[1]));
+    GSC_TRY(palloc(p, &p->zt, static_cast<uint64_t>(g.n[2]) * g.mw));
+    GSC_TRY(palloc(p, &p->wt, static_cast<uint64_t>(g.n[3]) * g.ma));
     GSC_CU(ctx, launch_axis_tables(g, q, p->abs->xn, p->abs->yn, p->abs->thf, p->abs->vf, p->xt, p->yt, p->zt, p->wt,
                                    p->flags, st));
     if (p->safe) GSC_CU(ctx, launch_valid_vs_safe(g, p->valid, p->safe, p->safe_rank, p->counts + 4, st));
-    unsigned long long hc[8];
-    unsigned int hflags = 0;
-    GSC_CU(ctx, cudaMemcpyAsync(hc, p->counts, sizeof(hc), cudaMemcpyDeviceToHost, st));
-    GSC_CU(ctx, cudaMemcpyAsync(&hflags, p->flags, sizeof(hflags), cudaMemcpyDeviceToHost, st));
-    GSC_CU(ctx, cudaStreamSynchronize(st));
-    if (hc[2] != 0) return fail(ctx, GSC_ERR_CANDIDATE_INVALID, "candidate set contains invalid states");
-    p->valid_count = hc[0];
-    p->candidate_count = hc[1];
-    if (hflags != 0) fused_ok = false;   // an empty or over-wide interval: only the stored count is exact
-    // The fused kernel reads (theta, v)-dilated copies of D', one per pair of
-    // theta and v box widths that occurs.
-    std::vector<uint8_t> hk(g.n[2] + 1, 0xFF), hl(g.n[3] + 1, 0xFF);
-    {
-        std::vector<uint32_t> hz(static_cast<size_t>(g.n[2]) * g.mw), hw(static_cast<size_t>(g.n[3]) * g.ma);
-        GSC_CU(ctx, cudaMemcpy(hz.data(), p->zt, hz.size() * 4, cudaMemcpyDeviceToHost));
-        GSC_CU(ctx, cudaMemcpy(hw.data(), p->wt, hw.size() * 4, cudaMemcpyDeviceToHost));
-        std::vector<char> kin(g.n[2] + 1, 0), lin(g.n[3] + 1, 0);
-        for (uint32_t ze : hz) {
-            const uint32_t lz = lo16(ze), hz2 = hi16(ze);
-            kin[lz <= hz2 ? hz2 - lz + 1 : g.n[2] - lz + hz2 + 1] = 1;
-        }
-        for (uint32_t we : hw)
-            if (we != kReject && hi16(we) >= lo16(we)) lin[hi16(we) - lo16(we) + 1] = 1;
-        DilateArgs d{};
-        for (uint32_t k = 1; k <= g.n[2]; ++k)
-            if (kin[k]) {
-                if (d.nk == kMaxDilate) { fused_ok = false; break; }
-                hk[k] = static_cast<uint8_t>(d.nk);
-                d.kval[d.nk++] = k;
-            }
-        for (uint32_t l = 1; l <= g.n[3]; ++l)
-            if (lin[l]) {
-                if (d.nl == kMaxDilate || l > static_cast<uint32_t>(kMaxDilate)) { fused_ok = false; break; }
-                hl[l] = static_cast<uint8_t>(d.nl);
-                d.lval[d.nl++] = l;
-            }
-        if (d.nk == 0 || d.nl == 0) fused_ok = false;
-        p->dil = d;
-        const int nv = p->safe ? (hc[4] != 0) : (hc[0] != g.S);
-        if (fused_smem_bytes(g, class_words(g), nv, g.ma) > kFusedSmemMax) fused_ok = false;
+
+    // Fused tables that do not depend on the sets, and the plan.
+    if (p->fused_candidate) {
+        GSC_TRY(palloc(p, &p->xcls, planes * class_words(g)));
+        GSC_CU(ctx, launch_x_classes(g, p->xt, p->xcls, st));
+        GSC_TRY(palloc(p, &p->xrep, planes));
+        GSC_CU(ctx, launch_plane_reps(g, p->xt, p->yt, p->wt, p->xrep, st));
+        GSC_TRY(palloc(p, &p->kidx, static_cast<uint64_t>(g.n[2]) + 1));
+        GSC_TRY(palloc(p, &p->lidx, static_cast<uint64_t>(g.n[3]) + 1));
     }
+    GSC_TRY(palloc(p, &p->dplan, 1));
+    GSC_CU(ctx, launch_plan(g, p->zt, p->wt, p->fused_candidate ? p->xrep : nullptr, p->counts, p->flags, p->kidx,
+                            p->lidx, p->dplan, st));
+    if (!p->hplan) p->hplan = &p->hplan_own;
+    GSC_CU(ctx, cudaMemcpyAsync(p->hplan, p->dplan, sizeof(PlanRecord), cudaMemcpyDeviceToHost, st));
+    return GSC_OK;
+}
+
+int problem_plan(gsc_problem* p) {
+    gsc_context* ctx = p->ctx;
+    const GridInfo& g = p->g;
+    const PlanRecord& pl = *p->hplan;
+    if (pl.counts[2] != 0) return fail(ctx, GSC_ERR_CANDIDATE_INVALID, "candidate set contains invalid states");
+    p->valid_count = pl.counts[0];
+    p->candidate_count = pl.counts[1];
+    // need the valid-cell test when some cell's validity is not its safety
+    p->need_valid = p->safe ? (pl.counts[4] != 0) : (p->valid_count != g.S);
+    const bool stored_ok = g.n[0] <= 255 && g.n[1] <= 255 && g.n[2] <= 255 && g.n[3] <= 255;
+    // An empty or over-wide interval, or too many box widths: only the
+    // stored count is exact.
+    bool fused_ok = p->fused_candidate && pl.fused && pl.flags == 0 && !pl.width_overflow;
+    if (fused_ok) {
+        p->max_reps = pl.max_reps;
+        p->dil = pl.dil;
+        if (fused_smem_bytes(g, class_words(g), p->need_valid, p->max_reps) > kFusedSmemMax) fused_ok = false;
+    }
+    uint32_t method = p->method;
     if (method == GSC_METHOD_AUTO) method = fused_ok ? GSC_METHOD_FUSED : (stored_ok ? GSC_METHOD_STORED : 0);
     if (method == 0) return fail(ctx, GSC_ERR_UNSUPPORTED, "no method applies to this grid");
     if (method == GSC_METHOD_FUSED && !fused_ok)
-        return fail(ctx, GSC_ERR_UNSUPPORTED, "fused method: an interval is empty or wider than 32 cells, or too many box widths");
+        return fail(ctx, GSC_ERR_UNSUPPORTED,
+                    "fused method: an interval is empty or wider than 32 cells, or too many box widths");
     p->method = method;
-    // need the valid-cell test when some cell's validity is not its safety
-    p->need_valid = p->safe ? (hc[4] != 0) : (p->valid_count != g.S);
-
-    // Fixpoint state.
-    const uint64_t iter_bound = std::min<uint64_t>(q.max_iterations, g.S + 1);
+    const uint64_t iter_bound = std::min<uint64_t>(p->q.max_iterations, g.S + 1);
     if (iter_bound + 2 > kStatsCapMax)
         return fail(ctx, GSC_ERR_UNSUPPORTED, "more than 2^20 fixpoint iterations requested");
     p->stats_cap = static_cast<uint32_t>(iter_bound + 2);
-    GSC_TRY(dalloc(ctx, A, B, &p->controller, g.S));
-    GSC_TRY(dalloc(ctx, A, B, &p->reach_step, g.S));
-    GSC_TRY(dalloc(ctx, A, B, &p->fc, 1));
-    GSC_TRY(dalloc(ctx, A, B, &p->stats, static_cast<uint64_t>(kStatsCols) * p->stats_cap));
-    GSC_TRY(dalloc(ctx, A, B, &p->reach8, g.S));
+    return GSC_OK;
+}
 
-    if (method == GSC_METHOD_STORED) {
-        GSC_TRY(dalloc(ctx, A, B, &p->pvalid, g.tsize));
+int problem_stage2(gsc_problem* p) {
+    gsc_context* ctx = p->ctx;
+    const GridInfo& g = p->g;
+    cudaStream_t st = p->stream;
+    GSC_TRY(palloc(p, &p->controller, g.S));
+    GSC_TRY(palloc(p, &p->reach_step, g.S));
+    GSC_TRY(palloc(p, &p->fc, 1));
+    GSC_TRY(palloc(p, &p->stats, static_cast<uint64_t>(kStatsCols) * p->stats_cap));
+    GSC_TRY(palloc(p, &p->reach8, g.S));
+
+    if (p->method == GSC_METHOD_STORED) {
+        GSC_TRY(palloc(p, &p->pvalid, g.tsize));
         GSC_CU(ctx, cudaMemsetAsync(p->pvalid, 0, g.tsize * 4, st));
         GSC_CU(ctx, launch_prefix4(g, 0, p->valid, nullptr, p->pvalid, nullptr, st));
         if (p->safe && p->safe_rank == 2) {
-            GSC_TRY(dalloc(ctx, A, B, &p->unsafe2, static_cast<uint64_t>(g.n[0] + 1) * (g.n[1] + 1)));
+            GSC_TRY(palloc(p, &p->unsafe2, static_cast<uint64_t>(g.n[0] + 1) * (g.n[1] + 1)));
             GSC_CU(ctx, launch_prefix2_unsafe(g, p->safe, p->unsafe2, st));
         } else if (p->safe) {
-            GSC_TRY(dalloc(ctx, A, B, &p->unsafe4, g.tsize));
+            GSC_TRY(palloc(p, &p->unsafe4, g.tsize));
             GSC_CU(ctx, cudaMemsetAsync(p->unsafe4, 0, g.tsize * 4, st));
             GSC_CU(ctx, launch_prefix4(g, 2, p->safe, nullptr, p->unsafe4, nullptr, st));
         }
         p->S_pad = (g.S + 1) & ~1ull;
-        GSC_TRY(dalloc(ctx, A, B, &p->boxes, p->S_pad * g.M));
+        GSC_TRY(palloc(p, &p->boxes, p->S_pad * g.M));
         StoredBuildArgs sb{};
         sb.xt = p->xt;
         sb.yt = p->yt;
@@ -594,68 +598,47 @@ int build_problem(gsc_problem* p, const gsc_query_desc* qd, uint32_t method) {
         sb.S_pad = p->S_pad;
         sb.valid_pairs = p->counts + 3;
         GSC_CU(ctx, launch_stored_build(g, sb, st));
-        GSC_TRY(dalloc(ctx, A, B, &p->pd, g.tsize));
+        GSC_TRY(palloc(p, &p->pd, g.tsize));
         GSC_CU(ctx, cudaMemsetAsync(p->pd, 0, g.tsize * 4, st));
-    } else {
-        const uint64_t words = g.rows * g.W;
-        GSC_TRY(dalloc(ctx, A, B, &p->validb, words));
-        GSC_TRY(dalloc(ctx, A, B, &p->unsafeb, words));
-        GSC_TRY(dalloc(ctx, A, B, &p->srcb, words));
-        GSC_TRY(dalloc(ctx, A, B, &p->candb, words));
-        GSC_TRY(dalloc(ctx, A, B, &p->dp, words));
-        GSC_TRY(dalloc(ctx, A, B, &p->reach0, words));
-        GSC_TRY(dalloc(ctx, A, B, &p->reach1, words));
-        GSC_TRY(dalloc(ctx, A, B, &p->active, words));
-        GSC_TRY(dalloc(ctx, A, B, &p->hit, words));
-        GSC_TRY(dalloc(ctx, A, B, &p->best, g.S));
-        const uint64_t combos = static_cast<uint64_t>(p->dil.nk) * p->dil.nl;
-        GSC_TRY(dalloc(ctx, A, B, &p->dzw, combos * words));
-        GSC_TRY(dalloc(ctx, A, B, &p->kidx, hk.size()));
-        GSC_TRY(dalloc(ctx, A, B, &p->lidx, hl.size()));
-        GSC_CU(ctx, cudaMemcpyAsync(p->kidx, hk.data(), hk.size(), cudaMemcpyHostToDevice, st));
-        GSC_CU(ctx, cudaMemcpyAsync(p->lidx, hl.data(), hl.size(), cudaMemcpyHostToDevice, st));
-        GSC_TRY(dalloc(ctx, A, B, &p->xcls, static_cast<uint64_t>(g.slices) * g.M * class_words(g)));
-        GSC_CU(ctx, launch_x_classes(g, p->xt, p->xcls, st));
-        GSC_TRY(dalloc(ctx, A, B, &p->xrep, static_cast<uint64_t>(g.slices) * g.M));
-        GSC_CU(ctx, launch_plane_reps(g, p->xt, p->yt, p->wt, p->xrep, st));
-        {
-            // Shared memory of the satisfaction kernel is sized by the largest
-            // number of distinct accelerations in one omega column.
-            std::vector<uint8_t> hrep(static_cast<size_t>(g.slices) * g.M);
-            GSC_CU(ctx, cudaMemcpyAsync(hrep.data(), p->xrep, hrep.size(), cudaMemcpyDeviceToHost, st));
-            GSC_CU(ctx, cudaStreamSynchronize(st));
-            uint32_t mr = 1;
-            for (size_t c = 0; c < hrep.size(); c += g.ma) {
-                uint32_t n = 0;
-                for (uint32_t ja = 0; ja < g.ma; ++ja) n += hrep[c + ja] == ja;
-                mr = std::max(mr, n);
-            }
-            p->max_reps = mr;
-        }
-        GSC_CU(ctx, launch_pack_bits(g, 0, p->valid, nullptr, p->validb, st));
-        GSC_CU(ctx, launch_pack_bits(g, 0, p->cand, nullptr, p->candb, st));
-        if (!p->safe) {
-            GSC_CU(ctx, cudaMemsetAsync(p->unsafeb, 0, words * sizeof(bword), st));
-            GSC_CU(ctx, cudaMemcpyAsync(p->srcb, p->validb, words * sizeof(bword), cudaMemcpyDeviceToDevice, st));
-        } else if (p->safe_rank == 2) {
-            GSC_CU(ctx, launch_pack_bits(g, 2, nullptr, p->safe, p->unsafeb, st));
-            GSC_CU(ctx, launch_pack_bits(g, 3, p->valid, p->safe, p->srcb, st));
-        } else {
-            GSC_CU(ctx, launch_pack_bits(g, 1, p->safe, nullptr, p->unsafeb, st));
-            GSC_CU(ctx, launch_pack_bits(g, 4, p->valid, p->safe, p->srcb, st));
-        }
-        if (p->need_valid) {
-            GSC_TRY(dalloc(ctx, A, B, &p->vzw, combos * words));
-            GSC_CU(ctx, launch_dilate(g, p->validb, p->vzw, p->dil, nullptr, st));
-        }
+        return GSC_OK;
     }
-    GSC_CU(ctx, cudaMemcpyAsync(hc, p->counts, sizeof(hc), cudaMemcpyDeviceToHost, st));
-    GSC_CU(ctx, cudaStreamSynchronize(st));
-    p->valid_pairs = hc[3];
+    const uint64_t words = g.rows * g.W;
+    GSC_TRY(palloc(p, &p->validb, words));
+    GSC_TRY(palloc(p, &p->unsafeb, words));
+    GSC_TRY(palloc(p, &p->srcb, words));
+    GSC_TRY(palloc(p, &p->candb, words));
+    GSC_TRY(palloc(p, &p->dp, words));
+    GSC_TRY(palloc(p, &p->reach0, words));
+    GSC_TRY(palloc(p, &p->reach1, words));
+    GSC_TRY(palloc(p, &p->active, words));
+    GSC_TRY(palloc(p, &p->hit, words));
+    GSC_TRY(palloc(p, &p->best, g.S));
+    const uint64_t combos = static_cast<uint64_t>(p->dil.nk) * p->dil.nl;
+    GSC_TRY(palloc(p, &p->dzw, combos * words));
+    GSC_CU(ctx, launch_pack_bits(g, 0, p->valid, nullptr, p->validb, st));
+    GSC_CU(ctx, launch_pack_bits(g, 0, p->cand, nullptr, p->candb, st));
+    if (!p->safe) {
+        GSC_CU(ctx, cudaMemsetAsync(p->unsafeb, 0, words * sizeof(bword), st));
+        GSC_CU(ctx, cudaMemcpyAsync(p->srcb, p->validb, words * sizeof(bword), cudaMemcpyDeviceToDevice, st));
+    } else if (p->safe_rank == 2) {
+        GSC_CU(ctx, launch_pack_bits(g, 2, nullptr, p->safe, p->unsafeb, st));
+        GSC_CU(ctx, launch_pack_bits(g, 3, p->valid, p->safe, p->srcb, st));
+    } else {
+        GSC_CU(ctx, launch_pack_bits(g, 1, p->safe, nullptr, p->unsafeb, st));
+        GSC_CU(ctx, launch_pack_bits(g, 4, p->valid, p->safe, p->srcb, st));
+    }
+    if (p->need_valid) {
+        GSC_TRY(palloc(p, &p->vzw, combos * words));
+        GSC_CU(ctx, launch_dilate(g, p->validb, p->vzw, p->dil, nullptr, st));
+    }
     return GSC_OK;
 }
 
-StoredFixArgs stored_args(gsc_problem* p, cudaGraphConditionalHandle cond, int use_cond) {
+}  // namespace gsc_api
+
+namespace {
+
+StoredFixArgs stored_args(const gsc_problem* p, cudaGraphConditionalHandle cond, int use_cond) {
     StoredFixArgs a{};
     a.boxes = p->boxes;
     a.S_pad = p->S_pad;
@@ -672,7 +655,11 @@ StoredFixArgs stored_args(gsc_problem* p, cudaGraphConditionalHandle cond, int u
     return a;
 }
 
-FusedFixArgs fused_args(gsc_problem* p, cudaGraphConditionalHandle cond, int use_cond) {
+}  // namespace
+
+namespace gsc_api {
+
+FusedFixArgs fused_args(const gsc_problem* p, cudaGraphConditionalHandle cond, int use_cond) {
     FusedFixArgs a{};
     a.xt = p->xt;
     a.yt = p->yt;
@@ -707,6 +694,10 @@ FusedFixArgs fused_args(gsc_problem* p, cudaGraphConditionalHandle cond, int use
     a.use_cond = use_cond;
     return a;
 }
+
+}  // namespace gsc_api
+
+namespace {
 
 cudaError_t enqueue_init(gsc_problem* p) {
     cudaStream_t st = p->ctx->stream;
@@ -777,11 +768,18 @@ int gsc_problem_create(gsc_context* ctx, const gsc_abstraction* abs, const gsc_q
     p->ctx = ctx;
     p->abs = abs;
     p->g = abs->g;
+    p->stream = ctx->stream;
+    p->method = method;
     GSC_CU(ctx, cudaEventRecord(ctx->ev[0], ctx->stream));
-    const int s = build_problem(p.get(), query, method);
-    if (s != GSC_OK) return s;
+    GSC_TRY(problem_stage1(p.get(), query));
+    GSC_CU(ctx, cudaStreamSynchronize(ctx->stream));
+    GSC_TRY(problem_plan(p.get()));
+    GSC_TRY(problem_stage2(p.get()));
+    unsigned long long hc[8];
+    GSC_CU(ctx, cudaMemcpyAsync(hc, p->counts, sizeof(hc), cudaMemcpyDeviceToHost, ctx->stream));
     GSC_CU(ctx, cudaEventRecord(ctx->ev[1], ctx->stream));
     GSC_CU(ctx, cudaEventSynchronize(ctx->ev[1]));
+    p->valid_pairs = hc[3];
     float ms = 0.f;
     GSC_CU(ctx, cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));
     p->timings.prepare_ms = ms;
@@ -951,10 +949,10 @@ int gsc_problem_export_abstraction(gsc_problem* p, uint32_t* min_flat, uint32_t*
     // The export needs the unsafe prefix of the stored build; make it if the
     // fused method skipped it.
     if (p->safe && p->safe_rank == 2 && !p->unsafe2) {
-        GSC_TRY(dalloc(ctx, p->allocs, p->bytes, &p->unsafe2, static_cast<uint64_t>(g.n[0] + 1) * (g.n[1] + 1)));
+        GSC_TRY(palloc(p, &p->unsafe2, static_cast<uint64_t>(g.n[0] + 1) * (g.n[1] + 1)));
         GSC_CU(ctx, launch_prefix2_unsafe(g, p->safe, p->unsafe2, st));
     } else if (p->safe && p->safe_rank == 4 && !p->unsafe4) {
-        GSC_TRY(dalloc(ctx, p->allocs, p->bytes, &p->unsafe4, g.tsize));
+        GSC_TRY(palloc(p, &p->unsafe4, g.tsize));
         GSC_CU(ctx, cudaMemsetAsync(p->unsafe4, 0, g.tsize * 4, st));
         GSC_CU(ctx, launch_prefix4(g, 2, p->safe, nullptr, p->unsafe4, nullptr, st));
     }

@@ -124,6 +124,97 @@ __global__ void k_dilate(GridInfo g, const bword* __restrict__ src, bword* __res
     }
 }
 
+// The set-up plan (one block): which theta widths (wrapped lengths of the
+// omega columns' theta boxes) and v widths (of the accelerations' v boxes)
+// occur, numbered in increasing order, and the most representative
+// accelerations of one omega column.
+__global__ void __launch_bounds__(256) k_plan(GridInfo g, const uint32_t* __restrict__ zt,
+                                              const uint32_t* __restrict__ wt, const uint8_t* __restrict__ xrep,
+                                              const unsigned long long* __restrict__ counts,
+                                              const unsigned int* __restrict__ flags, uint8_t* __restrict__ kidx,
+                                              uint8_t* __restrict__ lidx, PlanRecord* __restrict__ out) {
+    __shared__ uint32_t kbits[2048], lbits[2048];   // widths 1 .. 65535
+    __shared__ uint32_t s_maxrep;
+    __shared__ DilateArgs s_dil;
+    const uint32_t tid = threadIdx.x;
+    if (tid < 8) out->counts[tid] = counts[tid];
+    if (tid == 0) {
+        out->flags = *flags;
+        out->fused = xrep ? 1u : 0u;
+    }
+    if (!xrep) {
+        if (tid == 0) {
+            out->max_reps = 0;
+            out->width_overflow = 0;
+            out->dil = DilateArgs{};
+        }
+        return;
+    }
+    const uint32_t n2 = g.n[2], n3 = g.n[3];
+    for (uint32_t i = tid; i < 2048; i += blockDim.x) kbits[i] = lbits[i] = 0;
+    if (tid == 0) s_maxrep = 1;
+    __syncthreads();
+    for (uint32_t e = tid; e < n2 * g.mw; e += blockDim.x) {
+        const uint32_t ze = zt[e];
+        const uint32_t lz = lo16(ze), hz = hi16(ze);
+        const uint32_t k = (lz <= hz) ? hz - lz + 1 : n2 - lz + hz + 1;
+        atomicOr(&kbits[k >> 5], 1u << (k & 31));
+    }
+    for (uint32_t e = tid; e < n3 * g.ma; e += blockDim.x) {
+        const uint32_t we = wt[e];
+        if (we == kReject || hi16(we) < lo16(we)) continue;
+        const uint32_t l = hi16(we) - lo16(we) + 1;
+        atomicOr(&lbits[l >> 5], 1u << (l & 31));
+    }
+    const uint64_t columns = static_cast<uint64_t>(g.slices) * g.mw;
+    uint32_t mr = 1;
+    for (uint64_t c = tid; c < columns; c += blockDim.x) {
+        uint32_t n = 0;
+        for (uint32_t ja = 0; ja < g.ma; ++ja) n += xrep[c * g.ma + ja] == ja;
+        mr = max(mr, n);
+    }
+    atomicMax(&s_maxrep, mr);
+    __syncthreads();
+    if (tid == 0) {
+        DilateArgs d{};
+        uint32_t over = 0;
+        for (uint32_t k = 1; k <= n2; ++k) {
+            if (!((kbits[k >> 5] >> (k & 31)) & 1u)) continue;
+            if (d.nk == kMaxDilate) {
+                over = 1;
+                break;
+            }
+            d.kval[d.nk++] = k;
+        }
+        for (uint32_t l = 1; l <= n3; ++l) {
+            if (!((lbits[l >> 5] >> (l & 31)) & 1u)) continue;
+            if (d.nl == kMaxDilate || l > static_cast<uint32_t>(kMaxDilate)) {
+                over = 1;
+                break;
+            }
+            d.lval[d.nl++] = l;
+        }
+        if (d.nk == 0 || d.nl == 0) over = 1;
+        s_dil = d;
+        out->dil = d;
+        out->width_overflow = over;
+        out->max_reps = s_maxrep;
+    }
+    __syncthreads();
+    for (uint32_t k = tid; k <= n2; k += blockDim.x) {
+        uint32_t slot = 0xFF;
+        for (uint32_t i = 0; i < s_dil.nk; ++i)
+            if (s_dil.kval[i] == k) slot = i;
+        kidx[k] = static_cast<uint8_t>(slot);
+    }
+    for (uint32_t l = tid; l <= n3; l += blockDim.x) {
+        uint32_t slot = 0xFF;
+        for (uint32_t i = 0; i < s_dil.nl; ++i)
+            if (s_dil.lval[i] == l) slot = i;
+        lidx[l] = static_cast<uint8_t>(slot);
+    }
+}
+
 // One block per (theta, v) slice x omega column jw.
 //  B. per representative acceleration (the lowest of each group of inputs
 //     whose boxes coincide), E[y] = the (theta, v)-dilated D' row at the
@@ -414,6 +505,14 @@ size_t fused_smem_bytes(const GridInfo& g, uint32_t cls_words, int need_valid, u
     const size_t mr = max_reps;
     const size_t words = nw + mr * nw * nv + mr * nw + mr * cls_words + mr * g.n[1] + static_cast<size_t>(g.ma);
     return sizeof(bword) * words;
+}
+
+cudaError_t launch_plan(const GridInfo& g, const uint32_t* zt, const uint32_t* wt, const uint8_t* xrep,
+                        const unsigned long long* counts, const unsigned int* flags, uint8_t* kidx, uint8_t* lidx,
+                        PlanRecord* out, cudaStream_t st) {
+    if (xrep && (g.n[2] > 65535 || g.n[3] > 65535)) return cudaErrorInvalidValue;
+    k_plan<<<1, 256, 0, st>>>(g, zt, wt, xrep, counts, flags, kidx, lidx, out);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_dilate(const GridInfo& g, const bword* src, bword* dst, const DilateArgs& d, const FixControl* fc,

@@ -1,0 +1,187 @@
+// gsc_internal.hpp -- host-side objects behind the C ABI handles, shared by
+// the plain API (gsc_api.cu), the batched instances (gsc_batch.cu) and the
+// serving loop (gsc_server.cu).
+#pragma once
+
+#include <atomic>
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../../include/gsc_b200.h"
+#include "gsc_kernels.cuh"
+#include "gsc_pool.hpp"
+
+// Device memory regions carved up by a RangePool.  `slab_bytes` > 0 lets the
+// pool add regions of at least that size on demand; `cap` bounds the total
+// (0 = no bound besides the context's budget).
+struct DevicePool {
+    struct Slab {
+        char* base = nullptr;
+        uint64_t bytes = 0;
+        gsc_b200::RangePool ranges;
+    };
+    gsc_context* ctx = nullptr;
+    std::vector<Slab> slabs;
+    uint64_t slab_bytes = 0;
+    uint64_t cap = 0;
+    uint64_t total = 0;
+    std::mutex mu;
+
+    DevicePool(gsc_context* c, uint64_t slab, uint64_t capacity) : ctx(c), slab_bytes(slab), cap(capacity) {}
+    ~DevicePool();
+    // One region of exactly `bytes` now (a fixed pool); false when the device
+    // or the context budget refuses it.
+    bool reserve(uint64_t bytes);
+    void* alloc(uint64_t bytes);   // nullptr when no region fits and none may be added
+    void release(void* p, uint64_t bytes);
+    uint64_t used();
+};
+
+struct gsc_context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::string last_error;
+    uint64_t budget = 0;
+    std::atomic<uint64_t> in_use{0};
+    std::mutex mem_mu;   // budget check + in_use update
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    int sm_count = 0;
+};
+
+struct gsc_abstraction {
+    gsc_context* ctx = nullptr;
+    gsc_b200::GridInfo g{};
+    gsc_model_desc model{};
+    double* xn = nullptr;
+    double* yn = nullptr;
+    double* thf = nullptr;
+    double* vf = nullptr;
+    DevicePool* pool = nullptr;                        // nullptr: cudaMalloc'd
+    std::vector<std::pair<void*, uint64_t>> allocs;
+    uint64_t bytes = 0;
+    double build_ms = 0.0;
+    ~gsc_abstraction();
+};
+
+struct gsc_problem {
+    gsc_context* ctx = nullptr;
+    const gsc_abstraction* abs = nullptr;
+    gsc_b200::GridInfo g{};
+    gsc_b200::QueryInfo q{};
+    uint32_t method = 0;          // requested, then the one chosen
+    DevicePool* pool = nullptr;   // nullptr: every buffer cudaMalloc'd
+    cudaStream_t stream = nullptr;
+    std::vector<std::pair<void*, uint64_t>> allocs;
+    uint64_t bytes = 0;
+    // masks and tables
+    uint8_t* valid = nullptr;
+    uint8_t* cand = nullptr;
+    uint8_t* safe = nullptr;
+    int safe_rank = 0;
+    double* obstacles = nullptr;
+    unsigned long long* counts = nullptr;   // [0] valid [1] cand [2] cand-not-valid [3] valid pairs [4] valid!=safe
+    unsigned int* flags = nullptr;
+    uint32_t *xt = nullptr, *yt = nullptr, *zt = nullptr, *wt = nullptr;
+    int32_t* unsafe2 = nullptr;
+    int32_t* unsafe4 = nullptr;
+    int32_t* pvalid = nullptr;
+    // the set-up plan (counts, flags, dilation widths), written by the device
+    gsc_b200::PlanRecord* dplan = nullptr;
+    gsc_b200::PlanRecord* hplan = nullptr;   // host copy (caller-provided pinned memory, or hplan_own)
+    gsc_b200::PlanRecord hplan_own{};
+    bool fused_candidate = false;
+    // stored
+    uint2* boxes = nullptr;
+    uint64_t S_pad = 0;
+    int32_t* pd = nullptr;
+    uint8_t* reach8 = nullptr;
+    // fused
+    gsc_b200::bword *validb = nullptr, *unsafeb = nullptr, *srcb = nullptr, *candb = nullptr, *dp = nullptr;
+    gsc_b200::bword *reach0 = nullptr, *reach1 = nullptr, *active = nullptr, *hit = nullptr;
+    uint32_t* best = nullptr;
+    gsc_b200::bword* xcls = nullptr;
+    uint8_t* xrep = nullptr;
+    uint32_t max_reps = 0;
+    gsc_b200::bword *dzw = nullptr, *vzw = nullptr;
+    uint8_t *kidx = nullptr, *lidx = nullptr;
+    gsc_b200::DilateArgs dil{};
+    int need_valid = 0;
+    // common fixpoint state
+    uint32_t* controller = nullptr;
+    uint32_t* reach_step = nullptr;
+    gsc_b200::FixControl* fc = nullptr;
+    unsigned long long* stats = nullptr;
+    uint32_t stats_cap = 0;
+    uint64_t valid_count = 0, candidate_count = 0, valid_pairs = 0;
+    // graph
+    cudaGraphExec_t exec = nullptr;
+    cudaGraph_t graph = nullptr;
+    gsc_timings timings{};
+    ~gsc_problem();
+};
+
+namespace gsc_api {
+
+inline int fail(gsc_context* ctx, int status, const std::string& msg) {
+    if (ctx) ctx->last_error = msg;
+    return status;
+}
+
+#define GSC_CU(ctx, expr)                                                                              \
+    do {                                                                                               \
+        cudaError_t e__ = (expr);                                                                      \
+        if (e__ != cudaSuccess) {                                                                      \
+            return ::gsc_api::fail((ctx),                                                              \
+                                   e__ == cudaErrorMemoryAllocation ? GSC_ERR_OUT_OF_MEMORY : GSC_ERR_CUDA, \
+                                   std::string(#expr) + ": " + cudaGetErrorString(e__));               \
+        }                                                                                              \
+    } while (0)
+
+#define GSC_TRY(expr)                  \
+    do {                               \
+        int s__ = (expr);              \
+        if (s__ != GSC_OK) return s__; \
+    } while (0)
+
+int grid_from_model(const gsc_model_desc* m, gsc_b200::GridInfo* g, std::string* err);
+
+// Device memory for a handle: from `pool` when set, else cudaMalloc under
+// the context's budget.  Recorded in `allocs` and released by the owner.
+int device_alloc(gsc_context* ctx, DevicePool* pool, std::vector<std::pair<void*, uint64_t>>& allocs,
+                 uint64_t& bytes, void** p, uint64_t nbytes);
+void device_release_all(gsc_context* ctx, DevicePool* pool, std::vector<std::pair<void*, uint64_t>>& allocs,
+                        uint64_t& bytes);
+
+template <typename T>
+int palloc(gsc_problem* p, T** out, uint64_t count) {
+    void* q = nullptr;
+    const int s = device_alloc(p->ctx, p->pool, p->allocs, p->bytes, &q, count * sizeof(T));
+    *out = static_cast<T*>(q);
+    return s;
+}
+
+// Abstraction set-up without a host wait: tabulates the theta / v
+// trajectories, uploads them and launches the nominal-successor kernel on
+// `st`.  The three temporary tables are returned in `tmp` (owned by the
+// caller until the stream has passed the kernel).
+int abstraction_enqueue(gsc_abstraction* a, cudaStream_t st, std::vector<std::pair<void*, uint64_t>>& tmp);
+
+// Problem set-up in three steps:
+//   stage1  masks, per-axis boxes and (for the fused method) the x classes,
+//           plane representatives and the set-up plan, ending with the copy
+//           of the plan record to p->hplan -- no host wait;
+//   plan    (after the stream has passed stage1) chooses the method from the
+//           plan record and checks the candidate set;
+//   stage2  fixpoint buffers and the method's tables -- no host wait.
+int problem_stage1(gsc_problem* p, const gsc_query_desc* qd);
+int problem_plan(gsc_problem* p);
+int problem_stage2(gsc_problem* p);
+
+gsc_b200::FusedFixArgs fused_args(const gsc_problem* p, cudaGraphConditionalHandle cond, int use_cond);
+int sm_count(gsc_context* ctx);
+
+}  // namespace gsc_api

@@ -110,6 +110,18 @@ struct DilateArgs {
     uint32_t lval[kMaxDilate];
 };
 
+// Set-up plan of a problem, written by k_plan and copied to the host once:
+// the mask counts and axis-table flags, the largest number of representative
+// accelerations in one omega column, and the theta / v box widths in use.
+struct PlanRecord {
+    unsigned long long counts[8];
+    uint32_t flags;
+    uint32_t max_reps;
+    uint32_t width_overflow;   // more widths than kMaxDilate, or a v width above kMaxDilate
+    uint32_t fused;            // 1 when the fused tables were planned
+    DilateArgs dil;
+};
+
 struct FusedFixArgs {
     const uint32_t *xt, *yt, *zt, *wt;
     const bword* validb;
@@ -147,6 +159,11 @@ constexpr size_t kFusedSmemMax = 200 * 1024;
 size_t fused_smem_bytes(const GridInfo& g, uint32_t cls_words, int need_valid, uint32_t max_reps);
 cudaError_t launch_dilate(const GridInfo& g, const bword* src, bword* dst, const DilateArgs& d, const FixControl* fc,
                           cudaStream_t st);
+// Fills a PlanRecord from the counts, flags and (when xrep is set) the
+// theta / v tables and plane representatives; writes kidx / lidx.
+cudaError_t launch_plan(const GridInfo& g, const uint32_t* zt, const uint32_t* wt, const uint8_t* xrep,
+                        const unsigned long long* counts, const unsigned int* flags, uint8_t* kidx, uint8_t* lidx,
+                        PlanRecord* out, cudaStream_t st);
 // Class record words per plane: a 16-byte header + kClassMax * W masks.
 inline uint32_t class_words(const GridInfo& g) { return 4 + kClassMax * g.W; }
 // Per (slice, input) plane: the classes (lo - i0, hi - i0) = (a, b) of its x

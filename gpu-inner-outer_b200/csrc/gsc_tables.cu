@@ -422,29 +422,46 @@ __global__ void k_x_classes(GridInfo g, const uint32_t* __restrict__ xt, bword* 
     }
 }
 
+constexpr int kThreadsReps = 128;
+
 __global__ void k_plane_reps(GridInfo g, const uint32_t* __restrict__ xt, const uint32_t* __restrict__ yt,
                              const uint32_t* __restrict__ wt, uint8_t* __restrict__ rep) {
+    // One warp per column; the lanes compare a pair of planes' x and y rows
+    // together.  Representatives are kept in increasing order, so an input
+    // maps to the lowest earlier input with the same rows and v box.
+    __shared__ uint8_t s_reps[kThreadsReps / 32][256];
+    const uint32_t lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    uint8_t* reps = s_reps[wib];
     const uint64_t columns = static_cast<uint64_t>(g.slices) * g.mw;
-    for (uint64_t col = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; col < columns;
-         col += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    const uint64_t wstride = static_cast<uint64_t>(gridDim.x) * (blockDim.x >> 5);
+    for (uint64_t col = blockIdx.x * static_cast<uint64_t>(blockDim.x >> 5) + wib; col < columns; col += wstride) {
         // Planes are ((i2 * n3 + i3) * M + j) with j = ja + ma * jw, so column
         // col = (i2 * n3 + i3) * mw + jw starts at plane col * ma.
         const uint32_t i3 = static_cast<uint32_t>((col / g.mw) % g.n[3]);
         const uint64_t p0 = col * g.ma;
+        uint32_t nrep = 0;
         for (uint32_t ja = 0; ja < g.ma; ++ja) {
+            const uint32_t we = wt[i3 * g.ma + ja];
             uint32_t r = ja;
-            for (uint32_t jb = 0; jb < ja; ++jb) {
-                if (rep[p0 + jb] != jb) continue;
-                if (wt[i3 * g.ma + jb] != wt[i3 * g.ma + ja]) continue;
+            for (uint32_t k = 0; k < nrep; ++k) {
+                const uint32_t jb = reps[k];
+                if (wt[i3 * g.ma + jb] != we) continue;
                 bool same = true;
-                for (uint32_t i = 0; i < g.n[0] && same; ++i) same = xt[(p0 + jb) * g.n[0] + i] == xt[(p0 + ja) * g.n[0] + i];
-                for (uint32_t i = 0; i < g.n[1] && same; ++i) same = yt[(p0 + jb) * g.n[1] + i] == yt[(p0 + ja) * g.n[1] + i];
-                if (same) {
+                for (uint32_t i = lane; i < g.n[0]; i += 32)
+                    same = same && xt[(p0 + jb) * g.n[0] + i] == xt[(p0 + ja) * g.n[0] + i];
+                for (uint32_t i = lane; i < g.n[1]; i += 32)
+                    same = same && yt[(p0 + jb) * g.n[1] + i] == yt[(p0 + ja) * g.n[1] + i];
+                if (__all_sync(0xFFFFFFFFu, same)) {
                     r = jb;
                     break;
                 }
             }
-            rep[p0 + ja] = static_cast<uint8_t>(r);
+            if (r == ja) {
+                if (lane == 0) reps[nrep] = static_cast<uint8_t>(ja);
+                ++nrep;
+            }
+            if (lane == 0) rep[p0 + ja] = static_cast<uint8_t>(r);
+            __syncwarp();
         }
     }
 }
@@ -533,7 +550,10 @@ cudaError_t launch_x_classes(const GridInfo& g, const uint32_t* xt, bword* xcls,
 
 cudaError_t launch_plane_reps(const GridInfo& g, const uint32_t* xt, const uint32_t* yt, const uint32_t* wt,
                               uint8_t* xrep, cudaStream_t st) {
-    k_plane_reps<<<blocks_for(static_cast<uint64_t>(g.slices) * g.mw, 128), 128, 0, st>>>(g, xt, yt, wt, xrep);
+    const uint64_t warps = static_cast<uint64_t>(g.slices) * g.mw;
+    uint64_t b = (warps + kThreadsReps / 32 - 1) / (kThreadsReps / 32);
+    if (b > 8192) b = 8192;
+    k_plane_reps<<<static_cast<unsigned int>(b), kThreadsReps, 0, st>>>(g, xt, yt, wt, xrep);
     return cudaGetLastError();
 }
 
