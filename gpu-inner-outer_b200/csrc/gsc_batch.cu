@@ -1,0 +1,475 @@
+// gsc_batch.cu -- batched instances (gsc_batch_* of include/gsc_b200.h).
+//
+// No counterpart in the reference, which runs one case per call
+// (cuda/kernels.cu:492-875).  Set-up of N instances is the one-problem
+// set-up run N times on one stream with a single host wait (for the N plan
+// records) in the middle; all device memory comes from one growable pool.
+// The fixpoint is the batched kernels of gsc_batch_kernels.cu over every
+// instance, optionally as one CUDA graph: [init] -> while (any running)
+// { dilate, satisfaction, finalize, status }.  Launch shapes come from the
+// options, or from a small autotuner that times candidate shapes on the
+// batch itself and caches the winner per shape class.
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "gsc_internal.hpp"
+
+using namespace gsc_b200;
+using namespace gsc_api;
+
+namespace gsc_api {
+
+InstanceDesc make_instance(const gsc_problem* p) {
+    InstanceDesc d;
+    std::memset(&d, 0, sizeof(d));
+    d.g = p->g;
+    d.a = fused_args(p, 0, 0);
+    d.cand = p->cand;
+    d.counts = p->counts;
+    d.max_iterations = p->q.max_iterations;
+    d.stats_cap = p->stats_cap;
+    d.sat_tasks = p->g.slices * p->g.mw;
+    d.words = static_cast<uint32_t>(p->g.rows * p->g.W);
+    return d;
+}
+
+size_t instance_smem(const gsc_problem* p) {
+    return fused_smem_bytes(p->g, class_words(p->g), p->need_valid, p->max_reps);
+}
+
+void build_work_list(const std::vector<const gsc_problem*>& probs, const std::vector<uint32_t>& slots,
+                     uint32_t chunk, std::vector<uint32_t>& buf, WorkTotals& tot) {
+    const size_t n = slots.size();
+    buf.assign(n + 4 * (n + 1), 0);
+    uint32_t* slot = buf.data();
+    uint32_t* sat = slot + n;
+    uint32_t* dil = sat + n + 1;
+    uint32_t* fin = dil + n + 1;
+    uint32_t* ini = fin + n + 1;
+    for (size_t k = 0; k < n; ++k) {
+        const gsc_problem* p = probs[k];
+        const uint64_t words = p->g.rows * p->g.W;
+        const uint64_t span = std::max<uint64_t>({words, p->g.S, static_cast<uint64_t>(kStatsCols) * p->stats_cap});
+        slot[k] = slots[k];
+        sat[k + 1] = sat[k] + p->g.slices * p->g.mw;
+        dil[k + 1] = dil[k] + static_cast<uint32_t>((words + chunk - 1) / chunk);
+        fin[k + 1] = fin[k] + static_cast<uint32_t>((words + chunk - 1) / chunk);
+        ini[k + 1] = ini[k] + static_cast<uint32_t>((span + chunk - 1) / chunk);
+    }
+    tot.sat = sat[n];
+    tot.dil = dil[n];
+    tot.fin = fin[n];
+    tot.ini = ini[n];
+}
+
+WorkList device_work_list(const uint32_t* dbuf, uint32_t n, uint32_t chunk, uint32_t* status, uint32_t* running) {
+    WorkList wl{};
+    wl.slot = dbuf;
+    wl.sat_off = dbuf + n;
+    wl.dil_off = wl.sat_off + n + 1;
+    wl.fin_off = wl.dil_off + n + 1;
+    wl.ini_off = wl.fin_off + n + 1;
+    wl.n = n;
+    wl.chunk = chunk;
+    wl.status = status;
+    wl.running = running;
+    return wl;
+}
+
+uint32_t wmax_of(uint32_t w) { return w <= 1 ? 1 : w == 2 ? 2 : w <= 4 ? 4 : 8; }
+
+}  // namespace gsc_api
+
+struct gsc_batch {
+    gsc_context* ctx = nullptr;
+    // Declaration order is destruction order reversed: problems, then
+    // abstractions, release into the pool before the pool frees its regions.
+    std::unique_ptr<DevicePool> pool;
+    std::vector<std::unique_ptr<gsc_abstraction>> abs;
+    std::vector<std::unique_ptr<gsc_problem>> probs;
+    PlanRecord* hplans = nullptr;   // pinned
+    uint32_t* hrunning = nullptr;   // pinned
+    InstanceDesc* ddesc = nullptr;
+    uint32_t* dlist = nullptr;
+    uint32_t* drunning = nullptr;
+    std::vector<uint32_t> hlist;
+    WorkTotals tot{};
+    WorkList wl{};
+    BatchShape shape{};
+    uint32_t wmax = 1;
+    size_t smem = 0;
+    cudaGraphExec_t exec = nullptr;
+    cudaGraph_t graph = nullptr;
+    BatchShape graph_shape{};
+    gsc_batch_report t{};
+    uint32_t last_launches = 0;
+    ~gsc_batch() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        probs.clear();
+        abs.clear();
+        if (hplans) cudaFreeHost(hplans);
+        if (hrunning) cudaFreeHost(hrunning);
+    }
+};
+
+namespace {
+
+struct ShapeKey {
+    uint32_t wmax, n, sat_log, words_log, nv;
+    bool operator<(const ShapeKey& o) const {
+        return std::tie(wmax, n, sat_log, words_log, nv) < std::tie(o.wmax, o.n, o.sat_log, o.words_log, o.nv);
+    }
+};
+std::mutex g_tune_mu;
+std::map<ShapeKey, BatchShape> g_tuned;
+
+uint32_t log2_ceil(uint64_t v) {
+    uint32_t l = 0;
+    while ((1ull << l) < v && l < 63) ++l;
+    return l;
+}
+
+int upload_list(gsc_batch* b, uint32_t chunk) {
+    std::vector<const gsc_problem*> probs;
+    std::vector<uint32_t> slots;
+    for (uint32_t i = 0; i < b->probs.size(); ++i) {
+        probs.push_back(b->probs[i].get());
+        slots.push_back(i);
+    }
+    build_work_list(probs, slots, chunk, b->hlist, b->tot);
+    GSC_CU(b->ctx, cudaMemcpyAsync(b->dlist, b->hlist.data(), b->hlist.size() * 4, cudaMemcpyHostToDevice,
+                                   b->ctx->stream));
+    GSC_CU(b->ctx, cudaStreamSynchronize(b->ctx->stream));   // the host list is reused
+    b->wl = device_work_list(b->dlist, static_cast<uint32_t>(slots.size()), chunk, nullptr, b->drunning);
+    return GSC_OK;
+}
+
+int enqueue_iterations(gsc_batch* b, uint32_t count, uint32_t* launches) {
+    const int sms = sm_count(b->ctx);
+    for (uint32_t i = 0; i < count; ++i)
+        GSC_CU(b->ctx, launch_batch_iteration(b->ddesc, b->wl, b->tot, b->shape, b->wmax, b->smem, sms, 0, 0,
+                                              b->ctx->stream, launches));
+    return GSC_OK;
+}
+
+// Time `reps` iterations from a fresh start under each candidate shape;
+// keep the fastest.
+int autotune(gsc_batch* b) {
+    gsc_context* ctx = b->ctx;
+    const int sms = sm_count(ctx);
+    const uint32_t threads[] = {64, 128, 256};
+    const uint32_t per_sm[] = {0, 4, 8, 16};
+    const uint32_t chunks[] = {1024, 4096};
+    const uint32_t reps = 4;
+    cudaEvent_t e0, e1;
+    GSC_CU(ctx, cudaEventCreate(&e0));
+    GSC_CU(ctx, cudaEventCreate(&e1));
+    float best = 1e30f;
+    BatchShape best_shape = b->shape;
+    int status = GSC_OK;
+    for (uint32_t ch : chunks) {
+        status = upload_list(b, ch);
+        if (status != GSC_OK) break;
+        for (uint32_t th : threads) {
+            for (uint32_t ps : per_sm) {
+                b->shape = BatchShape{th, ps * static_cast<uint32_t>(sms), ch};
+                cudaError_t e = launch_batch_init(b->ddesc, b->wl, b->tot, sms, ctx->stream);
+                if (e == cudaSuccess) e = cudaEventRecord(e0, ctx->stream);
+                for (uint32_t r = 0; e == cudaSuccess && r < reps; ++r)
+                    e = launch_batch_iteration(b->ddesc, b->wl, b->tot, b->shape, b->wmax, b->smem, sms, 0, 0,
+                                               ctx->stream, nullptr);
+                if (e == cudaSuccess) e = cudaEventRecord(e1, ctx->stream);
+                if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+                float ms = 0.f;
+                if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+                if (e != cudaSuccess) {
+                    status = fail(ctx, GSC_ERR_CUDA, std::string("autotune: ") + cudaGetErrorString(e));
+                    break;
+                }
+                if (ms < best) {
+                    best = ms;
+                    best_shape = b->shape;
+                }
+            }
+            if (status != GSC_OK) break;
+        }
+        if (status != GSC_OK) break;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (status != GSC_OK) return status;
+    b->shape = best_shape;
+    return upload_list(b, best_shape.chunk);
+}
+
+int build_batch_graph(gsc_batch* b) {
+    gsc_context* ctx = b->ctx;
+    cudaStream_t st = ctx->stream;
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+    const int sms = sm_count(ctx);
+    cudaGraph_t g = nullptr, ginit = nullptr;
+    GSC_CU(ctx, cudaGraphCreate(&g, 0));
+    b->graph = g;
+    GSC_CU(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = launch_batch_init(b->ddesc, b->wl, b->tot, sms, st);
+    cudaError_t e2 = cudaStreamEndCapture(st, &ginit);
+    GSC_CU(ctx, e);
+    GSC_CU(ctx, e2);
+    cudaGraphNode_t init_node;
+    e = cudaGraphAddChildGraphNode(&init_node, g, nullptr, 0, ginit);
+    cudaGraphDestroy(ginit);
+    GSC_CU(ctx, e);
+    cudaGraphConditionalHandle handle;
+    GSC_CU(ctx, cudaGraphConditionalHandleCreate(&handle, g, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+    cp.conditional.handle = handle;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t cnode;
+    GSC_CU(ctx, cudaGraphAddNode(&cnode, g, &init_node, 1, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    GSC_CU(ctx, cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    e = launch_batch_iteration(b->ddesc, b->wl, b->tot, b->shape, b->wmax, b->smem, sms, handle, 1, st, nullptr);
+    cudaGraph_t body_out = nullptr;
+    e2 = cudaStreamEndCapture(st, &body_out);
+    GSC_CU(ctx, e);
+    GSC_CU(ctx, e2);
+    GSC_CU(ctx, cudaGraphInstantiate(&b->exec, g, 0));
+    b->graph_shape = b->shape;
+    return GSC_OK;
+}
+
+int batch_create(gsc_batch* b, uint32_t count, const gsc_model_desc* models, const gsc_query_desc* queries,
+                 const gsc_batch_options* opt) {
+    gsc_context* ctx = b->ctx;
+    cudaStream_t st = ctx->stream;
+    b->pool.reset(new DevicePool(ctx, 256ull << 20, 0));
+    GSC_CU(ctx, cudaMallocHost(&b->hplans, sizeof(PlanRecord) * count));
+    GSC_CU(ctx, cudaMallocHost(&b->hrunning, sizeof(uint32_t)));
+    std::vector<std::vector<std::pair<void*, uint64_t>>> tmp(count);
+    // Stage 1 of every instance, then one wait for all plan records.
+    for (uint32_t i = 0; i < count; ++i) {
+        std::unique_ptr<gsc_abstraction> a(new (std::nothrow) gsc_abstraction());
+        if (!a) return GSC_ERR_OUT_OF_MEMORY;
+        a->ctx = ctx;
+        a->model = models[i];
+        a->pool = b->pool.get();
+        std::string err;
+        const int s = grid_from_model(&models[i], &a->g, &err);
+        if (s != GSC_OK) return fail(ctx, s, "instance " + std::to_string(i) + ": " + err);
+        if (a->g.rows * a->g.W >= 0xFFFFFFFFull)
+            return fail(ctx, GSC_ERR_UNSUPPORTED, "instance " + std::to_string(i) + ": grid too large for a batch");
+        GSC_TRY(abstraction_enqueue(a.get(), st, tmp[i]));
+        b->abs.push_back(std::move(a));
+    }
+    for (uint32_t i = 0; i < count; ++i) {
+        std::unique_ptr<gsc_problem> p(new (std::nothrow) gsc_problem());
+        if (!p) return GSC_ERR_OUT_OF_MEMORY;
+        p->ctx = ctx;
+        p->abs = b->abs[i].get();
+        p->g = b->abs[i]->g;
+        p->pool = b->pool.get();
+        p->stream = st;
+        p->method = GSC_METHOD_FUSED;
+        p->hplan = b->hplans + i;
+        const int s = problem_stage1(p.get(), &queries[i]);
+        if (s != GSC_OK) return fail(ctx, s, "instance " + std::to_string(i) + ": " + ctx->last_error);
+        b->probs.push_back(std::move(p));
+    }
+    GSC_CU(ctx, cudaStreamSynchronize(st));
+    for (uint32_t i = 0; i < count; ++i) {
+        uint64_t tb = 0;
+        device_release_all(ctx, b->pool.get(), tmp[i], tb);
+    }
+    for (uint32_t i = 0; i < count; ++i) {
+        gsc_problem* p = b->probs[i].get();
+        int s = problem_plan(p);
+        if (s == GSC_OK) s = problem_stage2(p);
+        if (s != GSC_OK) return fail(ctx, s, "instance " + std::to_string(i) + ": " + ctx->last_error);
+    }
+    // Instance table, work list and launch shapes.
+    std::vector<InstanceDesc> hd(count);
+    uint32_t wmax = 1, nv_any = 0;
+    size_t smem = 0;
+    for (uint32_t i = 0; i < count; ++i) {
+        const gsc_problem* p = b->probs[i].get();
+        hd[i] = make_instance(p);
+        wmax = std::max(wmax, p->g.W);
+        smem = std::max(smem, instance_smem(p));
+        nv_any |= p->need_valid ? 1u : 0u;
+    }
+    b->wmax = wmax_of(wmax);
+    b->smem = smem;
+    if (smem > kFusedSmemMax) return fail(ctx, GSC_ERR_UNSUPPORTED, "batch: an instance needs too much shared memory");
+    void* q = nullptr;
+    uint64_t own = 0;
+    std::vector<std::pair<void*, uint64_t>> bufs;
+    GSC_TRY(device_alloc(ctx, b->pool.get(), bufs, own, &q, sizeof(InstanceDesc) * count));
+    b->ddesc = static_cast<InstanceDesc*>(q);
+    GSC_TRY(device_alloc(ctx, b->pool.get(), bufs, own, &q, 4ull * (count + 4ull * (count + 1))));
+    b->dlist = static_cast<uint32_t*>(q);
+    GSC_TRY(device_alloc(ctx, b->pool.get(), bufs, own, &q, 4));
+    b->drunning = static_cast<uint32_t*>(q);
+    GSC_CU(ctx, cudaMemcpyAsync(b->ddesc, hd.data(), sizeof(InstanceDesc) * count, cudaMemcpyHostToDevice, st));
+
+    const int sms = sm_count(ctx);
+    b->shape.sat_threads = (opt && opt->sat_threads) ? opt->sat_threads : 128;
+    b->shape.sat_blocks = (opt ? opt->sat_blocks_per_sm : 0) * static_cast<uint32_t>(sms);
+    b->shape.chunk = (opt && opt->chunk_words) ? opt->chunk_words : 2048;
+    if (b->shape.sat_threads != 64 && b->shape.sat_threads != 128 && b->shape.sat_threads != 256)
+        return fail(ctx, GSC_ERR_INVALID_ARGUMENT, "sat_threads must be 64, 128 or 256");
+    if (b->shape.chunk < 256 || b->shape.chunk % 256)
+        return fail(ctx, GSC_ERR_INVALID_ARGUMENT, "chunk_words must be a positive multiple of 256");
+    GSC_TRY(upload_list(b, b->shape.chunk));
+    b->t.tuned = 0;
+    if (opt && opt->autotune) {
+        uint64_t words = 0;
+        for (const auto& d : hd) words += d.words;
+        const ShapeKey key{b->wmax, count, log2_ceil(b->tot.sat), log2_ceil(words), nv_any};
+        bool hit = false;
+        {
+            std::lock_guard<std::mutex> lk(g_tune_mu);
+            auto it = g_tuned.find(key);
+            if (it != g_tuned.end()) {
+                b->shape = it->second;
+                hit = true;
+            }
+        }
+        if (hit) {
+            GSC_TRY(upload_list(b, b->shape.chunk));
+            b->t.tuned = 2;
+        } else {
+            const auto t0 = std::chrono::steady_clock::now();
+            GSC_TRY(autotune(b));
+            b->t.tune_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+            b->t.tuned = 1;
+            std::lock_guard<std::mutex> lk(g_tune_mu);
+            g_tuned[key] = b->shape;
+        }
+    }
+    b->t.instances = count;
+    return GSC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gsc_batch_create(gsc_context* ctx, uint32_t count, const gsc_model_desc* models, const gsc_query_desc* queries,
+                     const gsc_batch_options* options, gsc_batch** out) {
+    if (!ctx || !models || !queries || !out || count == 0) return GSC_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    cudaGetLastError();
+    GSC_CU(ctx, cudaSetDevice(ctx->device));
+    const auto t0 = std::chrono::steady_clock::now();
+    std::unique_ptr<gsc_batch> b(new (std::nothrow) gsc_batch());
+    if (!b) return GSC_ERR_OUT_OF_MEMORY;
+    b->ctx = ctx;
+    const int s = batch_create(b.get(), count, models, queries, options);
+    if (s != GSC_OK) {
+        cudaStreamSynchronize(ctx->stream);   // nothing of the failed batch may still be in flight
+        return s;
+    }
+    b->t.create_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    *out = b.release();
+    return GSC_OK;
+}
+
+int gsc_batch_solve(gsc_batch* b, uint32_t flags) {
+    if (!b) return GSC_ERR_INVALID_ARGUMENT;
+    gsc_context* ctx = b->ctx;
+    cudaGetLastError();
+    GSC_CU(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    const int sms = sm_count(ctx);
+    GSC_CU(ctx, cudaEventRecord(ctx->ev[0], st));
+    uint32_t launches = 0;
+    if (flags & GSC_SOLVE_GRAPH) {
+        if (!b->exec || std::memcmp(&b->graph_shape, &b->shape, sizeof(BatchShape)) != 0)
+            GSC_TRY(build_batch_graph(b));
+        GSC_CU(ctx, cudaGraphLaunch(b->exec, st));
+        launches = 0;   // counted below from the iterations run
+    } else {
+        GSC_CU(ctx, launch_batch_init(b->ddesc, b->wl, b->tot, sms, st));
+        launches = 1;
+        uint32_t cap = 0;
+        for (const auto& p : b->probs) cap = std::max(cap, p->stats_cap);
+        uint32_t done = 0, chunk = 4;
+        while (true) {
+            GSC_TRY(enqueue_iterations(b, chunk, &launches));
+            done += chunk;
+            GSC_CU(ctx, cudaMemcpyAsync(b->hrunning, b->drunning, 4, cudaMemcpyDeviceToHost, st));
+            GSC_CU(ctx, cudaStreamSynchronize(st));
+            if (*b->hrunning == 0) break;
+            if (done > cap + 64) return fail(ctx, GSC_ERR_TIMEOUT, "batch fixpoint did not stop within its bound");
+            if (chunk < 32) chunk *= 2;
+        }
+    }
+    GSC_CU(ctx, cudaEventRecord(ctx->ev[1], st));
+    GSC_CU(ctx, cudaEventSynchronize(ctx->ev[1]));
+    float ms = 0.f;
+    GSC_CU(ctx, cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));
+    b->t.solve_ms = ms;
+    b->last_launches = (flags & GSC_SOLVE_GRAPH) ? 0xFFFFFFFFu : launches;
+    b->t.max_iterations_run = 0;
+    b->t.pair_tests = 0;
+    return GSC_OK;
+}
+
+int gsc_batch_read(gsc_batch* b, uint32_t index, gsc_result* out) {
+    if (!b || !out || index >= b->probs.size()) return GSC_ERR_INVALID_ARGUMENT;
+    return gsc_problem_read(b->probs[index].get(), out);
+}
+
+int gsc_batch_timings(gsc_batch* b, gsc_batch_report* out) {
+    if (!b || !out) return GSC_ERR_INVALID_ARGUMENT;
+    gsc_context* ctx = b->ctx;
+    GSC_CU(ctx, cudaSetDevice(ctx->device));
+    // Per-instance iteration counts and pair tests of the last solve.
+    uint32_t maxit = 0;
+    uint64_t tests = 0;
+    for (const auto& p : b->probs) {
+        FixControl fc;
+        GSC_CU(ctx, cudaMemcpyAsync(&fc, p->fc, sizeof(fc), cudaMemcpyDeviceToHost, ctx->stream));
+        GSC_CU(ctx, cudaStreamSynchronize(ctx->stream));
+        maxit = std::max(maxit, fc.iter);
+        if (fc.iter) {
+            std::vector<unsigned long long> hs(static_cast<size_t>(kStatsCols) * (fc.iter + 1));
+            GSC_CU(ctx, cudaMemcpyAsync(hs.data(), p->stats, hs.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
+            GSC_CU(ctx, cudaStreamSynchronize(ctx->stream));
+            for (uint32_t i = 1; i <= fc.iter; ++i) tests += hs[kStatsCols * i + 2];
+        }
+    }
+    b->t.max_iterations_run = maxit;
+    b->t.pair_tests = tests;
+    // Graph solves run the body once per iteration of the longest instance.
+    b->t.kernel_launches = b->last_launches == 0xFFFFFFFFu ? 1 + 4 * std::max<uint32_t>(maxit, 1) : b->last_launches;
+    b->t.sat_threads = b->shape.sat_threads;
+    const int sms = sm_count(ctx);
+    b->t.sat_blocks_per_sm = b->shape.sat_blocks / static_cast<uint32_t>(sms);
+    b->t.chunk_words = b->shape.chunk;
+    b->t.device_bytes = b->pool ? b->pool->total : 0;
+    *out = b->t;
+    return GSC_OK;
+}
+
+void gsc_batch_destroy(gsc_batch* b) {
+    if (!b) return;
+    cudaSetDevice(b->ctx->device);
+    cudaStreamSynchronize(b->ctx->stream);
+    delete b;
+}
+
+}  // extern "C"

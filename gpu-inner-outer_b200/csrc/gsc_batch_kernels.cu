@@ -1,0 +1,210 @@
+// gsc_batch_kernels.cu -- the fused fixpoint over many instances at once.
+//
+// Each kernel is one launch over every listed instance: persistent blocks
+// walk a task list (instance k owns tasks off[k] .. off[k+1]-1, found by a
+// binary search) and run the same device bodies as the one-problem kernels
+// (gsc_fused_body.cuh), so an instance computes the same bits alone and in a
+// batch.  Instances that have stopped skip their tasks.  One iteration:
+//   k_batch_dilate    (theta, v)-dilated D' of every running instance;
+//   k_batch_sat       slice x omega-column tasks of every running instance;
+//   k_batch_finalize  word chunks; the last chunk of an instance (ticket)
+//                     applies its stop rules;
+//   k_batch_status    one block: per-instance stop flags, the number still
+//                     running, and the CUDA-graph loop condition.
+#include "gsc_fused_body.cuh"
+
+namespace gsc_b200 {
+
+using namespace fused;
+
+namespace {
+
+// Largest k in [0, n) with off[k] <= t, given off[0] <= t < off[n].
+__device__ __forceinline__ uint32_t find_task(const uint32_t* __restrict__ off, uint32_t n, uint32_t t) {
+    uint32_t lo = 0, hi = n;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (off[mid] <= t)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(256) k_batch_init(const InstanceDesc* __restrict__ descs, WorkList wl) {
+    const uint32_t total = wl.ini_off[wl.n];
+    for (uint32_t t = blockIdx.x; t < total; t += gridDim.x) {
+        const uint32_t k = find_task(wl.ini_off, wl.n, t);
+        const InstanceDesc& d = descs[wl.slot[k]];
+        const uint64_t b = static_cast<uint64_t>(t - wl.ini_off[k]) * wl.chunk;
+        const uint64_t e_end = b + wl.chunk;
+        const uint64_t wend = min(e_end, static_cast<uint64_t>(d.words));
+        for (uint64_t e = b + threadIdx.x; e < wend; e += blockDim.x) init_word(d.a, e);
+        const uint64_t send = min(e_end, d.g.S);
+        for (uint64_t s = b + threadIdx.x; s < send; s += blockDim.x) init_state(d.a, d.cand, s);
+        const uint64_t tend = min(e_end, static_cast<uint64_t>(kStatsCols) * d.stats_cap);
+        for (uint64_t i = b + threadIdx.x; i < tend; i += blockDim.x) d.a.stats[i] = 0;
+        if (t == wl.ini_off[k] && threadIdx.x == 0) init_control(d.a.fc, d.max_iterations, d.stats_cap, d.counts);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_batch_dilate(const InstanceDesc* __restrict__ descs, WorkList wl) {
+    const uint32_t total = wl.dil_off[wl.n];
+    for (uint32_t t = blockIdx.x; t < total; t += gridDim.x) {
+        const uint32_t k = find_task(wl.dil_off, wl.n, t);
+        const InstanceDesc& d = descs[wl.slot[k]];
+        if (d.a.fc->stop) continue;
+        const uint32_t b = (t - wl.dil_off[k]) * wl.chunk;
+        const uint32_t end = min(b + wl.chunk, d.words);
+        for (uint32_t p = b + threadIdx.x; p < end; p += blockDim.x) dilate_position(d.g, d.a.dp, d.a.dzw, d.a.dil, p);
+    }
+}
+
+// The instance of the current task is copied to shared memory when it
+// changes; the dynamic shared memory holds the largest instance's staging.
+template <int WMAX>
+__global__ void __launch_bounds__(256) k_batch_sat(const InstanceDesc* __restrict__ descs, WorkList wl) {
+    extern __shared__ __align__(16) bword smem[];
+    __shared__ __align__(16) InstanceDesc sd;
+    __shared__ uint32_t s_nrep;
+    const uint32_t total = wl.sat_off[wl.n];
+    uint32_t cur = 0xFFFFFFFFu;
+    for (uint32_t t = blockIdx.x; t < total; t += gridDim.x) {
+        const uint32_t k = find_task(wl.sat_off, wl.n, t);
+        const uint32_t slot = wl.slot[k];
+        if (slot != cur) {
+            const uint32_t* src = reinterpret_cast<const uint32_t*>(descs + slot);
+            uint32_t* dst = reinterpret_cast<uint32_t*>(&sd);
+            for (uint32_t i = threadIdx.x; i < sizeof(InstanceDesc) / 4; i += blockDim.x) dst[i] = src[i];
+            __syncthreads();
+            cur = slot;
+        }
+        sat_col_task<WMAX, false, 2>(sd.g, sd.a, t - wl.sat_off[k], smem, &s_nrep);
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(256) k_batch_finalize(const InstanceDesc* __restrict__ descs, WorkList wl) {
+    __shared__ bool last;
+    const uint32_t total = wl.fin_off[wl.n];
+    for (uint32_t t = blockIdx.x; t < total; t += gridDim.x) {
+        const uint32_t k = find_task(wl.fin_off, wl.n, t);
+        const InstanceDesc& d = descs[wl.slot[k]];
+        FixControl* fc = d.a.fc;
+        // No chunk of this instance has taken its ticket yet, so its stop
+        // flag and iteration cannot change before this task's ticket.
+        if (fc->stop) continue;
+        const uint32_t it = fc->iter + 1;
+        const bword* rprev = (fc->iter & 1) ? d.a.reach1 : d.a.reach0;
+        bword* rnext = (fc->iter & 1) ? d.a.reach0 : d.a.reach1;
+        const uint64_t b = static_cast<uint64_t>(t - wl.fin_off[k]) * wl.chunk;
+        const uint64_t end = min(b + wl.chunk, static_cast<uint64_t>(d.words));
+        unsigned long long nr = 0, nc = 0;
+        for (uint64_t e = b + threadIdx.x; e < end; e += blockDim.x) finalize_word(d.g, d.a, rprev, rnext, e, it, nr, nc);
+        unsigned long long* row = d.a.stats + kStatsCols * it;
+        add_counters(row, nr, nc);
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) last = atomicAdd(&fc->ticket, 1u) == wl.fin_off[k + 1] - wl.fin_off[k] - 1;
+        __syncthreads();
+        if (last && threadIdx.x == 0) {
+            __threadfence();
+            fc->ticket = 0;
+            control_step(fc, row, it);
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(256) k_batch_status(const InstanceDesc* __restrict__ descs, WorkList wl,
+                                                      cudaGraphConditionalHandle cond, int use_cond) {
+    __shared__ uint32_t running;
+    if (threadIdx.x == 0) running = 0;
+    __syncthreads();
+    uint32_t mine = 0;
+    for (uint32_t k = threadIdx.x; k < wl.n; k += blockDim.x) {
+        const uint32_t stop = descs[wl.slot[k]].a.fc->stop;
+        if (wl.status) wl.status[k] = stop ? 1u : 0u;
+        mine += stop ? 0u : 1u;
+    }
+    if (mine) atomicAdd(&running, mine);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (wl.running) *wl.running = running;
+        if (use_cond) cudaGraphSetConditional(cond, running ? 1u : 0u);
+    }
+}
+
+inline unsigned int grid_of(uint32_t tasks, uint32_t cap) {
+    const uint32_t b = tasks < cap ? tasks : cap;
+    return b ? b : 1u;
+}
+
+template <int WMAX>
+cudaError_t launch_sat_t(const InstanceDesc* descs, const WorkList& wl, const WorkTotals& tot, const BatchShape& sh,
+                         size_t smem, cudaStream_t st) {
+    static bool configured[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64 || !configured[dev]) {
+        e = cudaFuncSetAttribute(k_batch_sat<WMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(kFusedSmemMax));
+        if (e != cudaSuccess) return e;
+        if (dev >= 0 && dev < 64) configured[dev] = true;
+    }
+    const uint32_t blocks = sh.sat_blocks ? grid_of(tot.sat, sh.sat_blocks) : grid_of(tot.sat, 0xFFFFFFFFu);
+    k_batch_sat<WMAX><<<blocks, sh.sat_threads, smem, st>>>(descs, wl);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+size_t batch_sat_static_smem() { return sizeof(InstanceDesc) + 16; }
+
+cudaError_t launch_batch_init(const InstanceDesc* descs, const WorkList& wl, const WorkTotals& tot, int sms,
+                              cudaStream_t st) {
+    if (tot.ini == 0) return cudaSuccess;
+    k_batch_init<<<grid_of(tot.ini, 8u * sms), 256, 0, st>>>(descs, wl);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_iteration(const InstanceDesc* descs, const WorkList& wl, const WorkTotals& tot,
+                                   const BatchShape& sh, uint32_t wmax, size_t smem, int sms,
+                                   cudaGraphConditionalHandle cond, int use_cond, cudaStream_t st,
+                                   uint32_t* launches) {
+    if (sh.sat_threads < 32 || sh.sat_threads > 256 || sh.sat_threads % 32 || smem > kFusedSmemMax)
+        return cudaErrorInvalidValue;
+    uint32_t n = 0;
+    cudaError_t e = cudaSuccess;
+    if (tot.dil) {
+        k_batch_dilate<<<grid_of(tot.dil, 16u * sms), 256, 0, st>>>(descs, wl);
+        e = cudaGetLastError();
+        ++n;
+    }
+    if (e == cudaSuccess && tot.sat) {
+        switch (wmax) {
+            case 1: e = launch_sat_t<1>(descs, wl, tot, sh, smem, st); break;
+            case 2: e = launch_sat_t<2>(descs, wl, tot, sh, smem, st); break;
+            case 3:
+            case 4: e = launch_sat_t<4>(descs, wl, tot, sh, smem, st); break;
+            default: e = launch_sat_t<8>(descs, wl, tot, sh, smem, st); break;
+        }
+        ++n;
+    }
+    if (e == cudaSuccess && tot.fin) {
+        k_batch_finalize<<<grid_of(tot.fin, 16u * sms), 256, 0, st>>>(descs, wl);
+        e = cudaGetLastError();
+        ++n;
+    }
+    if (e == cudaSuccess) {
+        k_batch_status<<<1, 256, 0, st>>>(descs, wl, cond, use_cond);
+        e = cudaGetLastError();
+        ++n;
+    }
+    if (launches) *launches += n;
+    return e;
+}
+
+}  // namespace gsc_b200

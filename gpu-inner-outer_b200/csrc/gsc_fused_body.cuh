@@ -1,0 +1,375 @@
+// gsc_fused_body.cuh -- device bodies of the fused fixpoint, shared by the
+// one-problem kernels (gsc_fused.cu) and the batched kernels (gsc_batch.cu),
+// so that a problem computes the same bits alone and inside a batch.
+//
+// Semantics are those of reachability.hpp:53-153 (Jacobi update, lowest
+// satisfied input, reach_step = iteration, stop rules in the reference's
+// order).
+#pragma once
+
+#include "gsc_kernels.cuh"
+
+namespace gsc_b200 {
+namespace fused {
+
+// Bits [lx, hx] of the row F (hx - lx < 32), in the low bits.
+template <int W>
+__device__ __forceinline__ bword extract_bits(const bword (&F)[W], uint32_t lx, uint32_t hx) {
+    const uint32_t wi = lx / kBits, sh = lx % kBits, len = hx - lx + 1;
+    bword lo = 0, hi = 0;
+#pragma unroll
+    for (int w = 0; w < W; ++w) {
+        if (static_cast<uint32_t>(w) == wi) lo = F[w];
+        if (static_cast<uint32_t>(w) == wi + 1) hi = F[w];
+    }
+    const bword v = __funnelshift_r(lo, hi, sh);
+    return len >= kBits ? v : (v & ((bword(1) << len) - 1));
+}
+
+// acc |= F shifted so that bit i of the result is bit i + d of F (|d| < 32):
+// one funnel shift per word.
+template <int W>
+__device__ __forceinline__ void or_shifted(const bword (&F)[W], int d, bword (&acc)[W]) {
+    if (d >= 0) {
+#pragma unroll
+        for (int w = 0; w < W; ++w) acc[w] |= __funnelshift_r(F[w], (w + 1 < W) ? F[w + 1] : 0u, d);
+    } else {
+#pragma unroll
+        for (int w = 0; w < W; ++w) acc[w] |= __funnelshift_l((w > 0) ? F[w - 1] : 0u, F[w], -d);
+    }
+}
+
+__device__ __forceinline__ int hdr_byte(const bword* rec, int k) {
+    return static_cast<int8_t>((rec[k >> 2] >> (8 * (k & 3))) & 0xFFu);
+}
+
+// Initial sets of word e: reachable = candidate, active = valid && safe
+// source, D' = (valid && !candidate) || unsafe.
+__device__ __forceinline__ void init_word(const FusedFixArgs& a, uint64_t e) {
+    const bword c = a.candb[e];
+    a.reach0[e] = c;
+    a.active[e] = a.srcb[e];
+    a.hit[e] = 0;
+    a.dp[e] = (a.validb[e] & ~c) | a.unsafeb[e];
+}
+
+__device__ __forceinline__ void init_state(const FusedFixArgs& a, const uint8_t* cand, uint64_t s) {
+    a.controller[s] = kInvalid32;
+    a.reach_step[s] = cand[s] ? 0u : kInvalid32;
+    a.best[s] = kInvalid32;
+}
+
+// FixControl at the start of a solve (counts: [0] valid, [1] candidates).
+__device__ __forceinline__ void init_control(FixControl* fc, uint32_t max_iterations, uint32_t stats_cap,
+                                             const unsigned long long* counts) {
+    fc->iter = 0;
+    fc->ticket = 0;
+    fc->max_iterations = max_iterations;
+    fc->stats_cap = stats_cap;
+    fc->valid_count = counts[0];
+    fc->candidate_count = counts[1];
+    fc->certified = 0;
+    fc->reachable = counts[1];
+    fc->converged = 0;
+    fc->stop = (max_iterations == 0) ? 1u : 0u;
+    fc->message = (max_iterations == 0) ? 3u : 0u;
+}
+
+// (theta, v)-dilated copies of a bit-sliced set at word position p: for
+// every theta width k in d.kval and v width l in d.lval, out[combo][y][z][v]
+// = OR of src over theta cells z .. z+k-1 (wrapped) and v cells v .. v+l-1
+// (entries whose v window leaves the grid are never read and are left 0).
+// The theta ORs are extended incrementally.
+__device__ __forceinline__ void dilate_position(const GridInfo& g, const bword* __restrict__ src,
+                                                bword* __restrict__ dst, const DilateArgs& d, uint32_t p) {
+    const uint32_t n1 = g.n[1], n2 = g.n[2], n3 = g.n[3], W = g.W;
+    const uint32_t pos = static_cast<uint32_t>(g.rows * W);
+    const uint32_t kmax = d.kval[d.nk - 1];
+    const uint32_t lmax = d.lval[d.nl - 1];
+    const uint32_t r = p / W, wd = p - r * W;
+    const uint32_t y = r % n1, q = r / n1;
+    const uint32_t z = q % n2, v = q / n2;
+    const uint32_t lfit = min(lmax, n3 - v);   // v windows that stay inside the grid
+    bword zor[kMaxDilate];
+#pragma unroll
+    for (uint32_t j = 0; j < kMaxDilate; ++j) zor[j] = 0;
+    uint32_t ki = 0, zz = z;
+    for (uint32_t i = 0; i < kmax; ++i) {
+#pragma unroll
+        for (uint32_t j = 0; j < kMaxDilate; ++j)
+            if (j < lfit) zor[j] |= __ldg(src + (y + n1 * (zz + n2 * (v + j))) * W + wd);
+        zz = (zz + 1 == n2) ? 0 : zz + 1;
+        if (i + 1 == d.kval[ki]) {
+            bword acc = 0;
+            uint32_t li = 0;
+#pragma unroll
+            for (uint32_t j = 0; j < kMaxDilate; ++j) {
+                acc |= zor[j];
+                if (li < d.nl && j + 1 == d.lval[li]) {
+                    dst[static_cast<uint64_t>(ki * d.nl + li) * pos + p] = (j < lfit) ? acc : 0u;
+                    ++li;
+                }
+            }
+            ++ki;
+        }
+    }
+}
+
+// One (theta, v) slice x omega column jw (task = slice * mw + jw) of the
+// satisfaction test, by the whole block:
+//  B. per representative acceleration (the lowest of each group of inputs
+//     whose boxes coincide), E[y] = the (theta, v)-dilated D' row at the
+//     input's box corner: one load per word;
+//  C. each (representative, i1) item: F = OR of E over row i1's y range, then
+//     the x test 32 states per word: the x boxes of a plane fall into a few
+//     classes (lo - i0, hi - i0) = (a, b), and a state of class (a, b) is
+//     blocked when F has a bit in [i0 + a, i0 + b], i.e. bit i0 of
+//     OR_{d=a..b} (F >> d); a plane with more than kClassMax classes is tested
+//     state by state;
+//  D. per state, the lowest satisfied input of the column goes to best[]
+//     (atomicMin, so the lowest over all columns wins) and the hit bit is set.
+// WMAX: register words per row; EXACTW: g.W == WMAX (else g.W <= WMAX at run
+// time).  NVMODE: 0 / 1 = validity test off / on, 2 = a.need_valid decides.
+// Every early return is taken by the whole block.
+template <int WMAX, bool EXACTW, int NVMODE>
+__device__ __forceinline__ void sat_col_task(const GridInfo& g, const FusedFixArgs& a, uint32_t task,
+                                             bword* smem, uint32_t* s_nrep) {
+    const FixControl* fc = a.fc;
+    if (fc->stop) return;
+    const uint32_t W = EXACTW ? static_cast<uint32_t>(WMAX) : g.W;
+    const bool NV = NVMODE == 2 ? (a.need_valid != 0) : (NVMODE == 1);
+    const uint32_t n0 = g.n[0], n1 = g.n[1], n2 = g.n[2], ma = g.ma, mw = g.mw;
+    const uint32_t nw = n1 * W;
+    const uint32_t slice = task / mw, jw = task - slice * mw;
+    const uint32_t i2 = slice % n2, i3 = slice / n2;
+    const uint64_t wbase = static_cast<uint64_t>(slice) * nw;
+    const uint32_t tid = threadIdx.x, bd = blockDim.x;
+    const uint32_t lane = tid & 31;
+    const uint32_t nv = NV ? 2u : 1u;
+    const uint32_t cw = a.cls_words;
+    const uint32_t mr = a.max_reps;
+    const uint32_t pos = static_cast<uint32_t>(g.rows * W);
+
+    bword* act = smem;
+    bword* Eall = act + nw;                               // max_reps * nw * nv
+    bword* sat = Eall + mr * nw * nv;                     // max_reps * nw
+    bword* cls = sat + mr * nw;                           // max_reps * cw
+    uint32_t* yts = cls + mr * cw;                        // max_reps * n1
+    uint32_t* reps = yts + mr * n1;                       // ma: acceleration of each representative slot
+
+    const uint64_t pcol = (static_cast<uint64_t>(i2) * g.n[3] + i3) * g.M + static_cast<uint64_t>(ma) * jw;
+    int any = 0;
+    for (uint32_t e = tid; e < nw; e += bd) {
+        const bword v = a.active[wbase + e];
+        act[e] = v;
+        any |= (v != 0);
+    }
+    if (tid < 32) {
+        // Representatives in increasing acceleration order (warp ballot).
+        uint32_t n = 0;
+        for (uint32_t base = 0; base < ma; base += 32) {
+            const uint32_t ja = base + lane;
+            const bool is_rep = ja < ma && a.xrep[pcol + ja] == ja && a.wt[i3 * ma + ja] != kReject;
+            const uint32_t m = __ballot_sync(0xFFFFFFFFu, is_rep);
+            if (is_rep) reps[n + __popc(m & ((1u << lane) - 1))] = ja;
+            n += __popc(m);
+        }
+        if (lane == 0) *s_nrep = n;
+    }
+    any = __syncthreads_or(any);
+    const uint32_t nrep = *s_nrep;
+    if (!any || nrep == 0) return;
+    if (tid == 0) atomicAdd(a.stats + kStatsCols * (fc->iter + 1) + 3, static_cast<unsigned long long>(nrep));
+
+    // B. dilated D' rows at each representative's (theta, v) box corner.
+    const uint32_t ze = a.zt[i2 * mw + jw];
+    const uint32_t lz = lo16(ze), hz = hi16(ze);
+    const uint32_t nz = (lz <= hz) ? hz - lz + 1 : n2 - lz + hz + 1;
+    const uint32_t kslot = a.kidx[nz];
+    for (uint32_t e = tid; e < nrep * nw; e += bd) {
+        const uint32_t r = fdiv(e, g.magic_nw), rem = e - r * nw;
+        const uint32_t y = rem / W, wd = rem - y * W;
+        const uint32_t we = a.wt[i3 * ma + reps[r]];
+        const uint32_t lw = lo16(we), nwb = hi16(we) - lw + 1;
+        const uint64_t off = static_cast<uint64_t>(kslot * a.nl + a.lidx[nwb]) * pos +
+                             (y + n1 * (lz + n2 * lw)) * W + wd;
+        Eall[r * nw * nv + rem] = __ldg(a.dzw + off);
+        if (NV) Eall[r * nw * nv + nw + rem] = __ldg(a.vzw + off);
+    }
+    for (uint32_t r = tid >> 5; r < nrep; r += bd >> 5) {
+        const uint64_t pl = pcol + reps[r];
+        for (uint32_t e = lane; e < cw; e += 32) cls[r * cw + e] = __ldg(a.xcls + pl * cw + e);
+        for (uint32_t e = lane; e < n1; e += 32) yts[r * n1 + e] = __ldg(a.yt + pl * n1 + e);
+    }
+    __syncthreads();
+    // C. the (representative, row) items.
+    unsigned long long ntest = 0;
+    for (uint32_t e = tid; e < nrep * n1; e += bd) {
+        const uint32_t r = fdiv(e, g.magic_n1), i1 = e - r * n1;
+        const uint32_t ja = reps[r];
+        bword cm[WMAX], sw[WMAX];
+        bword anyc = 0;
+#pragma unroll
+        for (int w = 0; w < WMAX; ++w) {
+            cm[w] = (EXACTW || static_cast<uint32_t>(w) < W) ? act[i1 * W + w] : 0u;
+            sw[w] = 0;
+            anyc |= cm[w];
+        }
+        const uint32_t ye = yts[r * n1 + i1];
+        if (anyc && ye != kReject) {
+#pragma unroll
+            for (int w = 0; w < WMAX; ++w) ntest += __popc(cm[w]);
+            const bword* E = Eall + r * nw * nv;
+            bword F[WMAX], FV[WMAX];
+#pragma unroll
+            for (int w = 0; w < WMAX; ++w) F[w] = FV[w] = 0;
+            for (uint32_t y = lo16(ye); y <= hi16(ye); ++y) {
+#pragma unroll
+                for (int w = 0; w < WMAX; ++w) {
+                    if (!EXACTW && static_cast<uint32_t>(w) >= W) continue;
+                    F[w] |= E[y * W + w];
+                    if (NV) FV[w] |= E[nw + y * W + w];
+                }
+            }
+            const bword* rec = cls + r * cw;
+            const uint32_t ncls = rec[0] & 0xFFu;
+            if (ncls != 0xFFu) {
+                bword U[WMAX], VA[WMAX], OK[WMAX];
+#pragma unroll
+                for (int w = 0; w < WMAX; ++w) U[w] = VA[w] = OK[w] = 0;
+                for (uint32_t c = 0; c < ncls; ++c) {
+                    const int ca = hdr_byte(rec, 1 + c);
+                    const int cb = hdr_byte(rec, 7 + c);
+                    bword win[WMAX], winv[WMAX];
+#pragma unroll
+                    for (int w = 0; w < WMAX; ++w) win[w] = winv[w] = 0;
+                    for (int d = ca; d <= cb; ++d) {
+                        or_shifted<WMAX>(F, d, win);
+                        if (NV) or_shifted<WMAX>(FV, d, winv);
+                    }
+#pragma unroll
+                    for (int w = 0; w < WMAX; ++w) {
+                        if (!EXACTW && static_cast<uint32_t>(w) >= W) continue;
+                        const bword m = rec[4 + c * W + w];
+                        OK[w] |= m;
+                        U[w] |= win[w] & m;
+                        if (NV) VA[w] |= winv[w] & m;
+                    }
+                }
+#pragma unroll
+                for (int w = 0; w < WMAX; ++w) sw[w] = cm[w] & OK[w] & ~U[w] & (NV ? VA[w] : ~0u);
+            } else {
+                const uint32_t* xrow = a.xt + (pcol + ja) * n0;
+#pragma unroll
+                for (int w = 0; w < WMAX; ++w) {
+                    bword m = cm[w];
+                    while (m) {
+                        const uint32_t b = __ffs(m) - 1;
+                        m &= m - 1;
+                        const uint32_t xe = __ldg(xrow + w * kBits + b);
+                        if (xe == kReject) continue;
+                        const uint32_t lx = lo16(xe), hx = hi16(xe);
+                        bool ok = extract_bits<WMAX>(F, lx, hx) == 0;
+                        if (NV) ok = ok && extract_bits<WMAX>(FV, lx, hx) != 0;
+                        if (ok) sw[w] |= bword(1) << b;
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int w = 0; w < WMAX; ++w)
+            if (EXACTW || static_cast<uint32_t>(w) < W) sat[r * nw + i1 * W + w] = sw[w];
+    }
+    __syncthreads();
+    // D. lowest satisfied input of the column per state -> best[] and hit
+    // bits.  Representatives are in increasing order and each is the lowest
+    // input of its group, so the first representative that satisfies a state
+    // gives its lowest satisfied input of the column.
+    for (uint32_t e = tid; e < nw; e += bd) {
+        bword open = act[e], got = 0;
+        const uint32_t y = e / W;
+        const uint64_t srow = (static_cast<uint64_t>(slice) * n1 + y) * n0 + (e - y * W) * kBits;
+        for (uint32_t r = 0; r < nrep && open; ++r) {
+            const bword nb = sat[r * nw + e] & open;
+            if (!nb) continue;
+            open &= ~nb;
+            got |= nb;
+            const uint32_t j = reps[r] + ma * jw;
+            bword m = nb;
+            while (m) {
+                const uint32_t b = __ffs(m) - 1;
+                m &= m - 1;
+                atomicMin(a.best + srow + b, j);
+            }
+        }
+        if (got) atomicOr(a.hit + wbase + e, got);
+    }
+    for (int off = 16; off > 0; off >>= 1) ntest += __shfl_down_sync(0xFFFFFFFFu, ntest, off);
+    if ((tid & 31) == 0 && ntest) atomicAdd(a.stats + kStatsCols * (fc->iter + 1) + 2, ntest);
+}
+
+// Apply the iteration's hits to word e and build next iteration's D';
+// nr / nc collect newly reachable states and newly certified candidates.
+__device__ __forceinline__ void finalize_word(const GridInfo& g, const FusedFixArgs& a, const bword* rprev,
+                                              bword* rnext, uint64_t e, uint32_t it, unsigned long long& nr,
+                                              unsigned long long& nc) {
+    const bword rp = rprev[e];
+    const bword h = a.hit[e];
+    const bword rn = rp | h;
+    rnext[e] = rn;
+    a.dp[e] = (a.validb[e] & ~rn) | a.unsafeb[e];
+    if (h) {
+        a.hit[e] = 0;
+        a.active[e] &= ~h;
+        const bword c = a.candb[e];
+        nr += __popc(h & ~rp);
+        nc += __popc(h & c);
+        const uint64_t r = e / g.W;
+        const uint64_t sbase = r * g.n[0] + (e - r * g.W) * kBits;
+        bword m = h;
+        while (m) {
+            const uint32_t b = __ffs(m) - 1;
+            m &= m - 1;
+            const uint64_t s = sbase + b;
+            a.controller[s] = a.best[s];
+            a.best[s] = kInvalid32;
+            if (!((c >> b) & 1u)) a.reach_step[s] = it;
+        }
+    }
+}
+
+// Block-wide: add the block's counters to the iteration's stats row.
+__device__ __forceinline__ void add_counters(unsigned long long* row, unsigned long long nr, unsigned long long nc) {
+    for (int off = 16; off > 0; off >>= 1) {
+        nr += __shfl_down_sync(0xFFFFFFFFu, nr, off);
+        nc += __shfl_down_sync(0xFFFFFFFFu, nc, off);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (nr) atomicAdd(row, nr);
+        if (nc) atomicAdd(row + 1, nc);
+    }
+}
+
+// The stop rules after iteration `it` (reachability.hpp:133-144), by one
+// thread once every counter of the iteration is in.
+__device__ __forceinline__ void control_step(FixControl* fc, unsigned long long* row, uint32_t it) {
+    const unsigned long long tnr = atomicAdd(row, 0ull);
+    const unsigned long long tnc = atomicAdd(row + 1, 0ull);
+    fc->certified += tnc;
+    fc->reachable += tnr;
+    fc->iter = it;
+    if (fc->certified == fc->candidate_count) {
+        fc->converged = 1;
+        fc->message = 1;
+        fc->stop = 1;
+    } else if (tnr == 0 && tnc == 0) {
+        fc->message = 2;
+        fc->stop = 1;
+    } else if (it >= fc->max_iterations || it + 1 >= fc->stats_cap) {
+        fc->message = 3;
+        fc->stop = 1;
+    }
+}
+
+}  // namespace fused
+}  // namespace gsc_b200

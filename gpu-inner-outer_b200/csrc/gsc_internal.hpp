@@ -184,4 +184,16 @@ int problem_stage2(gsc_problem* p);
 gsc_b200::FusedFixArgs fused_args(const gsc_problem* p, cudaGraphConditionalHandle cond, int use_cond);
 int sm_count(gsc_context* ctx);
 
+// Batched execution of fused problems (gsc_batch.cu).
+gsc_b200::InstanceDesc make_instance(const gsc_problem* p);
+size_t instance_smem(const gsc_problem* p);
+// Host work list [slot | sat_off | dil_off | fin_off | ini_off] of probs[k]
+// placed at slots[k].
+void build_work_list(const std::vector<const gsc_problem*>& probs, const std::vector<uint32_t>& slots,
+                     uint32_t chunk, std::vector<uint32_t>& buf, gsc_b200::WorkTotals& tot);
+gsc_b200::WorkList device_work_list(const uint32_t* dbuf, uint32_t n, uint32_t chunk, uint32_t* status,
+                                    uint32_t* running);
+// Register words of the batched satisfaction kernel for rows of w words.
+uint32_t wmax_of(uint32_t w);
+
 }  // namespace gsc_api

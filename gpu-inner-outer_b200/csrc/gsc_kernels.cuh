@@ -164,6 +164,57 @@ cudaError_t launch_dilate(const GridInfo& g, const bword* src, bword* dst, const
 cudaError_t launch_plan(const GridInfo& g, const uint32_t* zt, const uint32_t* wt, const uint8_t* xrep,
                         const unsigned long long* counts, const unsigned int* flags, uint8_t* kidx, uint8_t* lidx,
                         PlanRecord* out, cudaStream_t st);
+// One instance of a batched solve (or of the serving loop), resident in
+// device memory and indexed by slot.
+struct InstanceDesc {
+    GridInfo g;
+    FusedFixArgs a;
+    const uint8_t* cand;
+    const unsigned long long* counts;
+    uint32_t max_iterations;
+    uint32_t stats_cap;
+    uint32_t sat_tasks;   // slices * mw
+    uint32_t words;       // rows * W
+};
+
+// The instances one launch works on: slot[k] and, per task kind, the prefix
+// offsets of their tasks (off[0] = 0, off[n] = total).  A dilate / finalize
+// task covers `chunk` word positions; an init task `chunk` words, states and
+// stats entries.
+struct WorkList {
+    const uint32_t* slot;
+    const uint32_t* sat_off;
+    const uint32_t* dil_off;
+    const uint32_t* fin_off;
+    const uint32_t* ini_off;
+    uint32_t n;
+    uint32_t chunk;
+    uint32_t* status;     // [n]: 1 once the instance stopped (optional)
+    uint32_t* running;    // instances still running after the iteration (optional)
+};
+
+// Launch shapes of the batched kernels.
+struct BatchShape {
+    uint32_t sat_threads;   // threads per satisfaction block
+    uint32_t sat_blocks;    // persistent satisfaction blocks (0 = one per task)
+    uint32_t chunk;         // word positions per dilate / finalize task
+};
+
+// Host-side task counts of one list (matching WorkList's offsets).
+struct WorkTotals {
+    uint32_t sat, dil, fin, ini;
+};
+
+cudaError_t launch_batch_init(const InstanceDesc* descs, const WorkList& wl, const WorkTotals& tot, int sms,
+                              cudaStream_t st);
+// One fixpoint iteration of every listed instance: dilate, satisfaction,
+// finalize and status (which also sets the graph condition when use_cond).
+cudaError_t launch_batch_iteration(const InstanceDesc* descs, const WorkList& wl, const WorkTotals& tot,
+                                   const BatchShape& sh, uint32_t wmax, size_t smem, int sms,
+                                   cudaGraphConditionalHandle cond, int use_cond, cudaStream_t st,
+                                   uint32_t* launches);
+size_t batch_sat_static_smem();
+
 // Class record words per plane: a 16-byte header + kClassMax * W masks.
 inline uint32_t class_words(const GridInfo& g) { return 4 + kClassMax * g.W; }
 // Per (slice, input) plane: the classes (lo - i0, hi - i0) = (a, b) of its x

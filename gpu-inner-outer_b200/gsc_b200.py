@@ -86,6 +86,21 @@ class Timings(ctypes.Structure):
     ]
 
 
+class BatchOptions(ctypes.Structure):
+    _fields_ = [("autotune", ctypes.c_uint32), ("sat_threads", ctypes.c_uint32),
+                ("sat_blocks_per_sm", ctypes.c_uint32), ("chunk_words", ctypes.c_uint32)]
+
+
+class BatchReport(ctypes.Structure):
+    _fields_ = [
+        ("create_ms", ctypes.c_double), ("tune_ms", ctypes.c_double), ("solve_ms", ctypes.c_double),
+        ("device_bytes", ctypes.c_uint64), ("instances", ctypes.c_uint32), ("max_iterations_run", ctypes.c_uint32),
+        ("kernel_launches", ctypes.c_uint32), ("sat_threads", ctypes.c_uint32),
+        ("sat_blocks_per_sm", ctypes.c_uint32), ("chunk_words", ctypes.c_uint32), ("tuned", ctypes.c_uint32),
+        ("pair_tests", ctypes.c_uint64),
+    ]
+
+
 # Every symbol include/gsc_b200.h declares, with its ctypes signature.
 _P = ctypes.c_void_p
 SIGNATURES = {
@@ -110,6 +125,12 @@ SIGNATURES = {
     "gsc_run_case": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ModelDesc), ctypes.POINTER(QueryDesc),
                                     ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(Result),
                                     ctypes.POINTER(Timings)]),
+    "gsc_batch_create": (ctypes.c_int, [_P, ctypes.c_uint32, ctypes.POINTER(ModelDesc), ctypes.POINTER(QueryDesc),
+                                        ctypes.POINTER(BatchOptions), ctypes.POINTER(_P)]),
+    "gsc_batch_solve": (ctypes.c_int, [_P, ctypes.c_uint32]),
+    "gsc_batch_read": (ctypes.c_int, [_P, ctypes.c_uint32, ctypes.POINTER(Result)]),
+    "gsc_batch_timings": (ctypes.c_int, [_P, ctypes.POINTER(BatchReport)]),
+    "gsc_batch_destroy": (None, [_P]),
     "gsc_fixpoint_noalloc": (ctypes.c_int, [ctypes.POINTER(ctypes.c_uint32), ctypes.c_uint32, ctypes.c_int32,
                                             _P, _P, _P, _P, _P, ctypes.c_uint32, _P, _P, _P,
                                             ctypes.POINTER(Result), _P]),
@@ -287,35 +308,7 @@ class Problem:
         return {k: getattr(t, k) for k, _ in Timings._fields_}
 
     def read(self, iter_capacity=4096, masks=True) -> dict:
-        r = Result()
-        probe = Result()
-        self.ctx.check(lib().gsc_problem_read(self._h, ctypes.byref(probe)))
-        S = int(probe.states)
-        out = {}
-        if masks:
-            out = {
-                "valid_mask": np.zeros(S, np.uint8), "candidate_mask": np.zeros(S, np.uint8),
-                "reachable_mask": np.zeros(S, np.uint8), "controller": np.zeros(S, np.uint32),
-                "reach_step": np.zeros(S, np.uint32),
-            }
-            for k, v in out.items():
-                setattr(r, k, _ptr(v))
-        nr = np.zeros(iter_capacity, np.uint64)
-        nc = np.zeros(iter_capacity, np.uint64)
-        r.iter_new_reachable = _ptr(nr)
-        r.iter_new_certified = _ptr(nc)
-        r.iter_capacity = iter_capacity
-        self.ctx.check(lib().gsc_problem_read(self._h, ctypes.byref(r)))
-        it = int(r.iterations)
-        out.update({
-            "shape": tuple(r.shape), "input_shape": tuple(r.input_shape), "states": int(r.states),
-            "inputs": int(r.inputs), "pairs": int(r.pairs), "iterations": it, "converged": bool(r.converged),
-            "message": MESSAGES[int(r.message)], "reachable_states": int(r.reachable_states),
-            "certified_candidates": int(r.certified_candidates), "candidate_count": int(r.candidate_count),
-            "valid_count": int(r.valid_count), "iter_new_reachable": nr[:min(it, iter_capacity)].copy(),
-            "iter_new_certified": nc[:min(it, iter_capacity)].copy(),
-        })
-        return out
+        return _read_result(lambda r: lib().gsc_problem_read(self._h, r), self.ctx, iter_capacity, masks)
 
     def export_abstraction(self):
         probe = Result()
@@ -330,6 +323,82 @@ class Problem:
     def close(self):
         if self._h:
             lib().gsc_problem_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _read_result(call, ctx, iter_capacity=4096, masks=True) -> dict:
+    """Run a gsc_*_read call twice (shape probe, then the arrays) and return
+    the result as a dict of numpy arrays and scalars."""
+    r = Result()
+    probe = Result()
+    ctx.check(call(ctypes.byref(probe)))
+    S = int(probe.states)
+    out = {}
+    if masks:
+        out = {
+            "valid_mask": np.zeros(S, np.uint8), "candidate_mask": np.zeros(S, np.uint8),
+            "reachable_mask": np.zeros(S, np.uint8), "controller": np.zeros(S, np.uint32),
+            "reach_step": np.zeros(S, np.uint32),
+        }
+        for k, v in out.items():
+            setattr(r, k, _ptr(v))
+    nr = np.zeros(iter_capacity, np.uint64)
+    nc = np.zeros(iter_capacity, np.uint64)
+    r.iter_new_reachable = _ptr(nr)
+    r.iter_new_certified = _ptr(nc)
+    r.iter_capacity = iter_capacity
+    ctx.check(call(ctypes.byref(r)))
+    it = int(r.iterations)
+    out.update({
+        "shape": tuple(r.shape), "input_shape": tuple(r.input_shape), "states": int(r.states),
+        "inputs": int(r.inputs), "pairs": int(r.pairs), "iterations": it, "converged": bool(r.converged),
+        "message": MESSAGES[int(r.message)], "reachable_states": int(r.reachable_states),
+        "certified_candidates": int(r.certified_candidates), "candidate_count": int(r.candidate_count),
+        "valid_count": int(r.valid_count), "iter_new_reachable": nr[:min(it, iter_capacity)].copy(),
+        "iter_new_certified": nc[:min(it, iter_capacity)].copy(),
+    })
+    return out
+
+
+class Batch:
+    """Many independent instances (each a case dict: model + query) set up
+    and solved together (gsc_batch_*).  ``masks`` optionally gives, per
+    instance, the keyword masks a Problem takes."""
+
+    def __init__(self, ctx: Context, cases, autotune=False, sat_threads=0, sat_blocks_per_sm=0, chunk_words=0,
+                 masks=None):
+        self.ctx = ctx
+        self._h = ctypes.c_void_p()
+        n = len(cases)
+        self.queries = [_Query(c, **((masks or [{}] * n)[i] or {})) for i, c in enumerate(cases)]
+        self.models = (ModelDesc * n)(*[model_desc(c) for c in cases])
+        self.qdescs = (QueryDesc * n)(*[q.desc for q in self.queries])
+        opt = BatchOptions(int(bool(autotune)), int(sat_threads), int(sat_blocks_per_sm), int(chunk_words))
+        ctx.check(lib().gsc_batch_create(ctx._h, n, self.models, self.qdescs, ctypes.byref(opt),
+                                         ctypes.byref(self._h)))
+        self.count = n
+        ctx._children.add(self)
+
+    def solve(self, graph=True):
+        self.ctx.check(lib().gsc_batch_solve(self._h, SOLVE_GRAPH if graph else 0))
+
+    def read(self, index, iter_capacity=4096, masks=True) -> dict:
+        return _read_result(lambda r: lib().gsc_batch_read(self._h, int(index), r), self.ctx, iter_capacity, masks)
+
+    def report(self) -> dict:
+        t = BatchReport()
+        self.ctx.check(lib().gsc_batch_timings(self._h, ctypes.byref(t)))
+        return {k: getattr(t, k) for k, _ in BatchReport._fields_}
+
+    def close(self):
+        if self._h:
+            lib().gsc_batch_destroy(self._h)
             self._h = ctypes.c_void_p()
 
     def __del__(self):

@@ -19,7 +19,11 @@
  *                      successors of every (cell, input), kept on the device;
  *   gsc_problem_*      one K-invariance query against a resident abstraction:
  *                      masks, quantised successor boxes, and the fixpoint;
- *   gsc_run_case       the whole reference call in one step.
+ *   gsc_run_case       the whole reference call in one step;
+ *   gsc_batch_*        many independent instances solved together (no
+ *                      counterpart in the reference);
+ *   gsc_server_*       a request loop of K-invariance queries against
+ *                      resident abstractions (no counterpart in the reference).
  *
  * Every entry point returns a gsc_status.  Results go to caller-provided host
  * buffers.  Device memory is owned by the handles.  There is no CPU fallback:
@@ -264,6 +268,52 @@ int gsc_fixpoint_noalloc(const uint32_t shape[4], uint32_t inputs, int32_t wrap_
                          const uint32_t* max_flat, const uint8_t* pair_valid, const uint8_t* valid_mask,
                          const uint8_t* candidate_mask, uint32_t max_iterations, uint8_t* reachable_mask,
                          uint32_t* controller, uint32_t* reach_step, gsc_result* summary, void* cuda_stream);
+
+/* ---- Batched instances --------------------------------------------------
+ * No counterpart in the reference (which solves one case per call).  Many
+ * independent instances -- each its own model and query, of any grid and
+ * input size the fused method takes -- are set up together and solved
+ * together: every fixpoint iteration of every instance is one pass of four
+ * kernels over all instances (persistent blocks walking a task list), and
+ * with GSC_SOLVE_GRAPH the whole loop is one CUDA graph whose while-node
+ * reads a device flag cleared when no instance is left running.  Each
+ * instance's result is bit-identical to its own gsc_problem solve.  Fused
+ * method only: an instance the fused method cannot take fails the create
+ * with GSC_ERR_UNSUPPORTED and the instance index in gsc_last_error. */
+typedef struct gsc_batch gsc_batch;
+
+typedef struct {
+    uint32_t autotune;            /* 1: time launch shapes on this batch, keep the fastest
+                                     (cached per batch shape class in the process)        */
+    uint32_t sat_threads;         /* threads per satisfaction block: 64, 128, 256 (0 = 128)  */
+    uint32_t sat_blocks_per_sm;   /* persistent satisfaction blocks per SM (0 = one block
+                                     per task)                                             */
+    uint32_t chunk_words;         /* word positions per dilate / finalize task (0 = 2048)  */
+} gsc_batch_options;
+
+typedef struct {
+    double create_ms;             /* host wall clock of gsc_batch_create (set-up of all)   */
+    double tune_ms;               /* of which autotuning trials                            */
+    double solve_ms;              /* last gsc_batch_solve, device events                   */
+    uint64_t device_bytes;        /* device memory held by the batch                       */
+    uint32_t instances;
+    uint32_t max_iterations_run;  /* most fixpoint iterations of one instance, last solve  */
+    uint32_t kernel_launches;     /* kernels launched by the last solve                    */
+    uint32_t sat_threads;         /* launch shapes in use                                  */
+    uint32_t sat_blocks_per_sm;
+    uint32_t chunk_words;
+    uint32_t tuned;               /* 1 = shapes from trials, 2 = from the process cache    */
+    uint64_t pair_tests;          /* (state, input) tests of the last solve, all instances */
+} gsc_batch_report;
+
+int gsc_batch_create(gsc_context* ctx, uint32_t count, const gsc_model_desc* models, const gsc_query_desc* queries,
+                     const gsc_batch_options* options, gsc_batch** out);
+/* flags: GSC_SOLVE_GRAPH (else a host loop that checks the device flag). */
+int gsc_batch_solve(gsc_batch* batch, uint32_t flags);
+/* Instance `index` of the last solve, as gsc_problem_read. */
+int gsc_batch_read(gsc_batch* batch, uint32_t index, gsc_result* out);
+int gsc_batch_timings(gsc_batch* batch, gsc_batch_report* out);
+void gsc_batch_destroy(gsc_batch* batch);
 
 #ifdef __cplusplus
 }
