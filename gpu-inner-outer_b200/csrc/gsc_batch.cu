@@ -70,7 +70,7 @@ void build_work_list(const std::vector<const gsc_problem*>& probs, const std::ve
     tot.ini = ini[n];
 }
 
-WorkList device_work_list(const uint32_t* dbuf, uint32_t n, uint32_t chunk, uint32_t* status, uint32_t* running) {
+WorkList device_work_list(const uint32_t* dbuf, uint32_t n, uint32_t chunk, FixControl* status, uint32_t* running) {
     WorkList wl{};
     wl.slot = dbuf;
     wl.sat_off = dbuf + n;

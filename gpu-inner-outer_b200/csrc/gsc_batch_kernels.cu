@@ -9,8 +9,9 @@
 //   k_batch_sat       slice x omega-column tasks of every running instance;
 //   k_batch_finalize  word chunks; the last chunk of an instance (ticket)
 //                     applies its stop rules;
-//   k_batch_status    one block: per-instance stop flags, the number still
-//                     running, and the CUDA-graph loop condition.
+//   k_batch_status    one block: a copy of every instance's control record,
+//                     the number still running, and the CUDA-graph loop
+//                     condition.
 #include "gsc_fused_body.cuh"
 
 namespace gsc_b200 {
@@ -124,9 +125,9 @@ __global__ void __launch_bounds__(256) k_batch_status(const InstanceDesc* __rest
     __syncthreads();
     uint32_t mine = 0;
     for (uint32_t k = threadIdx.x; k < wl.n; k += blockDim.x) {
-        const uint32_t stop = descs[wl.slot[k]].a.fc->stop;
-        if (wl.status) wl.status[k] = stop ? 1u : 0u;
-        mine += stop ? 0u : 1u;
+        const FixControl* fc = descs[wl.slot[k]].a.fc;
+        if (wl.status) wl.status[k] = *fc;
+        mine += fc->stop ? 0u : 1u;
     }
     if (mine) atomicAdd(&running, mine);
     __syncthreads();

@@ -191,7 +191,7 @@ size_t instance_smem(const gsc_problem* p);
 // placed at slots[k].
 void build_work_list(const std::vector<const gsc_problem*>& probs, const std::vector<uint32_t>& slots,
                      uint32_t chunk, std::vector<uint32_t>& buf, gsc_b200::WorkTotals& tot);
-gsc_b200::WorkList device_work_list(const uint32_t* dbuf, uint32_t n, uint32_t chunk, uint32_t* status,
+gsc_b200::WorkList device_work_list(const uint32_t* dbuf, uint32_t n, uint32_t chunk, gsc_b200::FixControl* status,
                                     uint32_t* running);
 // Register words of the batched satisfaction kernel for rows of w words.
 uint32_t wmax_of(uint32_t w);

@@ -189,7 +189,7 @@ struct WorkList {
     const uint32_t* ini_off;
     uint32_t n;
     uint32_t chunk;
-    uint32_t* status;     // [n]: 1 once the instance stopped (optional)
+    FixControl* status;   // [n]: copy of each instance's FixControl after the iteration (optional)
     uint32_t* running;    // instances still running after the iteration (optional)
 };
 

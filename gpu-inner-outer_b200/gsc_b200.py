@@ -101,6 +101,18 @@ class BatchReport(ctypes.Structure):
     ]
 
 
+class ServerOptions(ctypes.Structure):
+    _fields_ = [("memory_budget", ctypes.c_uint64), ("max_slots", ctypes.c_uint32),
+                ("iterations_per_step", ctypes.c_uint32), ("sat_threads", ctypes.c_uint32),
+                ("sat_blocks_per_sm", ctypes.c_uint32), ("chunk_words", ctypes.c_uint32)]
+
+
+class ServerReport(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_uint64) for k in (
+        "submitted", "completed", "failed", "queued", "in_flight", "steps", "max_running",
+        "device_bytes_budget", "device_bytes_in_use", "peak_device_bytes")]
+
+
 # Every symbol include/gsc_b200.h declares, with its ctypes signature.
 _P = ctypes.c_void_p
 SIGNATURES = {
@@ -131,6 +143,13 @@ SIGNATURES = {
     "gsc_batch_read": (ctypes.c_int, [_P, ctypes.c_uint32, ctypes.POINTER(Result)]),
     "gsc_batch_timings": (ctypes.c_int, [_P, ctypes.POINTER(BatchReport)]),
     "gsc_batch_destroy": (None, [_P]),
+    "gsc_server_create": (ctypes.c_int, [_P, ctypes.POINTER(ServerOptions), ctypes.POINTER(_P)]),
+    "gsc_server_submit": (ctypes.c_int, [_P, _P, ctypes.POINTER(QueryDesc), ctypes.POINTER(Result),
+                                         ctypes.POINTER(ctypes.c_uint64)]),
+    "gsc_server_wait": (ctypes.c_int, [_P, ctypes.c_uint64, ctypes.c_int32, ctypes.POINTER(ctypes.c_int),
+                                       ctypes.POINTER(ctypes.c_double)]),
+    "gsc_server_stats": (ctypes.c_int, [_P, ctypes.POINTER(ServerReport)]),
+    "gsc_server_destroy": (None, [_P]),
     "gsc_fixpoint_noalloc": (ctypes.c_int, [ctypes.POINTER(ctypes.c_uint32), ctypes.c_uint32, ctypes.c_int32,
                                             _P, _P, _P, _P, _P, ctypes.c_uint32, _P, _P, _P,
                                             ctypes.POINTER(Result), _P]),
@@ -248,7 +267,7 @@ class Context:
         if self._h:
             kids = list(self._children)
             for k in kids:
-                if isinstance(k, Problem):
+                if isinstance(k, (Problem, Server, Batch)):
                     k.close()
             for k in kids:
                 k.close()
@@ -400,6 +419,90 @@ class Batch:
         if self._h:
             lib().gsc_batch_destroy(self._h)
             self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """The serving loop (gsc_server_*): K-invariance queries against resident
+    abstractions, admitted by a device-memory budget and iterated together
+    as they arrive.  ``submit`` returns a ticket; ``wait`` returns the result
+    dict (as Problem.read) plus ``status`` and ``latency_ms``.  Result arrays
+    may be supplied through ``out`` (e.g. views of pinned host memory, which
+    lets the copies overlap the device work); they must stay alive until the
+    ticket is waited for, which this object guarantees for the arrays it
+    allocates itself."""
+
+    def __init__(self, ctx: Context, memory_budget=0, max_slots=0, iterations_per_step=0, sat_threads=0,
+                 sat_blocks_per_sm=0, chunk_words=0):
+        self.ctx = ctx
+        self._h = ctypes.c_void_p()
+        opt = ServerOptions(int(memory_budget), int(max_slots), int(iterations_per_step), int(sat_threads),
+                            int(sat_blocks_per_sm), int(chunk_words))
+        ctx.check(lib().gsc_server_create(ctx._h, ctypes.byref(opt), ctypes.byref(self._h)))
+        self._pending = {}
+        ctx._children.add(self)
+
+    def submit(self, abstraction: Abstraction, case, out=None, iter_capacity=4096, **masks) -> int:
+        q = _Query(case, **masks)
+        s, _ = grid_shape(case)
+        S = int(np.prod(s, dtype=np.uint64))
+        if out is None:
+            out = {
+                "valid_mask": np.zeros(S, np.uint8), "candidate_mask": np.zeros(S, np.uint8),
+                "reachable_mask": np.zeros(S, np.uint8), "controller": np.zeros(S, np.uint32),
+                "reach_step": np.zeros(S, np.uint32),
+            }
+        r = Result()
+        for k, v in out.items():
+            setattr(r, k, _ptr(v))
+        nr = np.zeros(iter_capacity, np.uint64)
+        nc = np.zeros(iter_capacity, np.uint64)
+        r.iter_new_reachable = _ptr(nr)
+        r.iter_new_certified = _ptr(nc)
+        r.iter_capacity = iter_capacity
+        t = ctypes.c_uint64()
+        self.ctx.check(lib().gsc_server_submit(self._h, abstraction._h, ctypes.byref(q.desc), ctypes.byref(r),
+                                               ctypes.byref(t)))
+        self._pending[int(t.value)] = (q, r, out, nr, nc)
+        return int(t.value)
+
+    def wait(self, ticket, timeout_ms=-1, check=True) -> dict:
+        st = ctypes.c_int()
+        lat = ctypes.c_double()
+        rc = lib().gsc_server_wait(self._h, int(ticket), int(timeout_ms), ctypes.byref(st), ctypes.byref(lat))
+        if rc != 0:
+            raise GscError(rc)
+        q, r, out, nr, nc = self._pending.pop(int(ticket))
+        if check and st.value != 0:
+            raise GscError(st.value)
+        it = int(r.iterations)
+        res = dict(out)
+        res.update({
+            "status": int(st.value), "latency_ms": float(lat.value),
+            "shape": tuple(r.shape), "input_shape": tuple(r.input_shape), "states": int(r.states),
+            "inputs": int(r.inputs), "pairs": int(r.pairs), "iterations": it, "converged": bool(r.converged),
+            "message": MESSAGES.get(int(r.message), ""), "reachable_states": int(r.reachable_states),
+            "certified_candidates": int(r.certified_candidates), "candidate_count": int(r.candidate_count),
+            "valid_count": int(r.valid_count), "iter_new_reachable": nr[:min(it, len(nr))].copy(),
+            "iter_new_certified": nc[:min(it, len(nc))].copy(),
+        })
+        return res
+
+    def stats(self) -> dict:
+        t = ServerReport()
+        self.ctx.check(lib().gsc_server_stats(self._h, ctypes.byref(t)))
+        return {k: getattr(t, k) for k, _ in ServerReport._fields_}
+
+    def close(self):
+        if self._h:
+            lib().gsc_server_destroy(self._h)
+            self._h = ctypes.c_void_p()
+            self._pending.clear()
 
     def __del__(self):
         try:

@@ -237,3 +237,28 @@ def random_instance(seed: int, index: int, n_lo=(16, 16, 16, 16), n_hi=(48, 48, 
     ax, ay = (float(v) for v in rng.uniform(0.3, 0.8, size=2))
     c["candidate_ellipse"] = [cx, cy, 1.0 / (ax * ax), 1.0 / (ay * ay), 1.0]
     return checked(c)
+
+
+def random_query(case: dict, seed: int, index: int, iter_lo=8, iter_hi=64) -> dict:
+    """One seeded K-invariance query against the model of `case` (same grid,
+    inputs and dynamics): safe set x^2/alpha - y^2/beta <= 1 and |y| <= gamma,
+    an elliptical candidate set centred inside it (within the valid set), a
+    disturbance bound in U[0.005, 0.02] on every dimension, and an iteration
+    cap in [iter_lo, iter_hi]."""
+    import numpy as np
+
+    rng = np.random.default_rng([int(seed), int(index), 7])
+    q = clone(case)
+    q["name"] = f"{case['name']}_q{seed}_{index}"
+    q["disturbance_half_width"] = [float(rng.uniform(0.005, 0.02))] * 4
+    alpha = float(rng.uniform(0.5, 2.0))
+    beta = float(rng.uniform(0.5, 2.0))
+    gamma = float(rng.uniform(1.2, 1.9))
+    q["constraint"] = "quadric"
+    q["constraint_params"] = [1.0 / alpha, 1.0 / beta, 1.0, gamma]
+    cx, cy = (float(v) for v in rng.uniform(-0.5, 0.5, size=2))
+    ax, ay = (float(v) for v in rng.uniform(0.3, 0.8, size=2))
+    q["candidate"] = "ellipse"
+    q["candidate_ellipse"] = [cx, cy, 1.0 / (ax * ax), 1.0 / (ay * ay), 1.0]
+    q["max_iterations"] = int(rng.integers(iter_lo, iter_hi + 1))
+    return q

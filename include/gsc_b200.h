@@ -315,6 +315,60 @@ int gsc_batch_read(gsc_batch* batch, uint32_t index, gsc_result* out);
 int gsc_batch_timings(gsc_batch* batch, gsc_batch_report* out);
 void gsc_batch_destroy(gsc_batch* batch);
 
+/* ---- Serving loop ---------------------------------------------------------
+ * No counterpart in the reference.  A loop thread serves K-invariance
+ * queries (safe set, candidate set, disturbance bound, iteration cap: a
+ * gsc_query_desc) against abstractions kept resident on the device.  Queries
+ * are admitted in arrival order while a slot is free and their device memory
+ * fits the server's budget; admitted queries are set up on a second stream
+ * while the running ones iterate, and join the running set at the next
+ * iteration step (continuous batching: every step runs one batched fixpoint
+ * iteration -- or iterations_per_step -- of every running query in four
+ * launches).  A query that stops leaves the set, its results are copied to
+ * the caller's buffers on a third stream, and its memory and slot go to the
+ * next query.  Each query's result is bit-identical to its own gsc_problem
+ * solve (fused method).  All gsc_server_* calls are thread-safe. */
+typedef struct gsc_server gsc_server;
+
+typedef struct {
+    uint64_t memory_budget;         /* device bytes for queries in flight (0 = half the free memory) */
+    uint32_t max_slots;             /* queries on the device at once (0 = 256)                        */
+    uint32_t iterations_per_step;   /* fixpoint iterations between host checks (0 = 2)               */
+    uint32_t sat_threads;           /* as gsc_batch_options (0 = 64)                                  */
+    uint32_t sat_blocks_per_sm;     /* (0 = 16)                                                       */
+    uint32_t chunk_words;           /* (0 = 1024)                                                     */
+} gsc_server_options;
+
+typedef struct {
+    uint64_t submitted;
+    uint64_t completed;             /* finished, successfully or not                */
+    uint64_t failed;
+    uint64_t queued;                /* waiting for admission                        */
+    uint64_t in_flight;             /* admitted, not yet completed                  */
+    uint64_t steps;                 /* batched iteration steps launched             */
+    uint64_t max_running;           /* most queries iterating in one step           */
+    uint64_t device_bytes_budget;
+    uint64_t device_bytes_in_use;
+    uint64_t peak_device_bytes;
+} gsc_server_report;
+
+int gsc_server_create(gsc_context* ctx, const gsc_server_options* options, gsc_server** out);
+/* Queues one query against `abs` (an abstraction of the server's context).
+ * The query's host arrays (obstacles, masks) and every buffer of `out` must
+ * stay valid until the query completes; `out` is then filled as by
+ * gsc_problem_read (result buffers in pinned host memory let the copies
+ * overlap the device work).  *ticket identifies the query. */
+int gsc_server_submit(gsc_server* server, const gsc_abstraction* abs, const gsc_query_desc* query,
+                      gsc_result* out, uint64_t* ticket);
+/* Waits for a ticket (timeout_ms < 0: no limit).  Returns GSC_ERR_TIMEOUT if
+ * it has not completed in time, else GSC_OK with *status = the query's own
+ * gsc_status and *latency_ms = submit-to-completion time; a completed ticket
+ * is then forgotten (wait once per ticket). */
+int gsc_server_wait(gsc_server* server, uint64_t ticket, int32_t timeout_ms, int* status, double* latency_ms);
+int gsc_server_stats(gsc_server* server, gsc_server_report* out);
+/* Completes every submitted query, then stops the loop and frees the server. */
+void gsc_server_destroy(gsc_server* server);
+
 #ifdef __cplusplus
 }
 #endif
