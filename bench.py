@@ -47,11 +47,20 @@ def parse():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(C.PRESETS), default="demo_scale")
+    ap.add_argument("--workload", choices=sorted(C.PRESETS) + ["batched", "served"], default="demo_scale")
     ap.add_argument("--method", choices=["auto", "stored", "fused"], default="auto")
     ap.add_argument("--cpu-sample-states", type=int, default=160000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=5)
+    # batched / served workloads
+    ap.add_argument("--instances", type=int, default=64)
+    ap.add_argument("--seed", type=int, default=20261203)
+    ap.add_argument("--queries", type=int, default=10000)
+    ap.add_argument("--rates", type=str, default="0.5,0.75,0.9",
+                    help="Poisson arrival rates as fractions of the measured saturation throughput")
+    ap.add_argument("--serve-budget-gb", type=float, default=24.0)
+    ap.add_argument("--plain-queries", type=int, default=0,
+                    help="queries timed through the plain API for the sequential baseline (0 = all)")
     return ap.parse_args()
 
 
@@ -227,8 +236,289 @@ def algorithmic_bytes(method, g, timings):
     return (4.0 * (n0 + n1) * timings["aux_count"] + 16.0 * words * L) / L
 
 
+def gpu_uuid(torch, dev):
+    try:
+        return "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:   # noqa: BLE001
+        return None
+
+
+def pinned_outputs(torch, S):
+    """The five result arrays of one problem as numpy views of pinned memory."""
+    import numpy as np
+
+    bufs = {k: torch.empty(S * sz, dtype=torch.uint8, pin_memory=True)
+            for k, sz in (("valid_mask", 1), ("candidate_mask", 1), ("reachable_mask", 1), ("controller", 4),
+                          ("reach_step", 4))}
+    return {k: (v.numpy() if k.endswith("mask") else v.numpy().view(np.uint32)) for k, v in bufs.items()}
+
+
+def percentile(xs, q):
+    import numpy as np
+
+    return float(np.percentile(np.asarray(xs, dtype=np.float64), q)) if len(xs) else None
+
+
+def plain_solve(G, ctx, absn, case, out):
+    """One query through the plain API: problem set-up, graph solve, read."""
+    p = G.Problem(ctx, absn, case, G.METHOD_FUSED)
+    p.solve(graph=True)
+    r = p.read(out=out)
+    p.close()
+    return r
+
+
+def bench_batched(args):
+    """64 seeded instances of uneven grid and input size (random_instance):
+    value = instances/s of the batched fixpoint with everything resident
+    (one step = one gsc_batch_solve of all instances, L2 flushed before each);
+    e2e = instances/s of gsc_batch_create + solve + reads into pinned host
+    memory; beside it the same instances one by one through the plain API
+    (abstraction, problem, graph solve, read)."""
+    import numpy as np
+    import torch
+    import gsc_b200 as G
+
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.current_stream(dev)
+    cases = [C.random_instance(args.seed, i) for i in range(args.instances)]
+    sizes = [int(np.prod(C.grid_shape(c)[0])) for c in cases]
+    outs = [pinned_outputs(torch, S) for S in sizes]
+    ctx = G.Context(0, stream.cuda_stream)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    b = G.Batch(ctx, cases, autotune=True)     # tunes once; later batches of this class reuse the shapes
+    rep0 = b.report()
+    for _ in range(args.warmup):
+        flush.fill_(1)
+        b.solve(graph=True)
+    torch.cuda.synchronize(dev)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    launches = 0
+    with ClockSampler(gpu_uuid(torch, dev)) as clocks:
+        for k in range(args.steps):
+            flush.fill_(k & 0xFF)
+            evs[k][0].record(stream)
+            b.solve(graph=True)
+            evs[k][1].record(stream)
+        torch.cuda.synchronize(dev)
+    rep = b.report()
+    launches = rep["kernel_launches"] * args.steps
+    step_ms = statistics.median(a.elapsed_time(c) for a, c in evs)
+    b.close()
+
+    # End to end: create + solve + read all, host wall clock.
+    e2e = []
+    for k in range(args.e2e_steps + 1):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        bb = G.Batch(ctx, cases, autotune=True)
+        bb.solve(graph=True)
+        for i in range(len(cases)):
+            bb.read(i, out=outs[i])
+        bb.close()
+        if k:
+            e2e.append((time.perf_counter() - t0) * 1e3)
+    e2e_ms = statistics.median(e2e)
+
+    # Sequential plain solves of the same instances (one warm pass first).
+    plain_ms, plain_dev = [], []
+    for rnd in range(2):
+        plain_ms, plain_dev = [], []
+        for c, o in zip(cases, outs):
+            torch.cuda.synchronize(dev)
+            t0 = time.perf_counter()
+            a = G.Abstraction(ctx, c)
+            p = G.Problem(ctx, a, c, G.METHOD_FUSED)
+            p.solve(graph=True)
+            p.read(out=o)
+            plain_dev.append(p.timings()["solve_ms"])
+            p.close()
+            a.close()
+            plain_ms.append((time.perf_counter() - t0) * 1e3)
+    plain_total = sum(plain_ms)
+    n = len(cases)
+    h2d = 0
+    d2h = sum(11 * S for S in sizes)
+    line = {
+        "metric": "batched instances/s", "value": n / (step_ms * 1e-3), "unit": "instances/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32 bit-sliced sets / int32 counts (f64 boxes)",
+        "data": "synthetic",
+        "config": {"workload": f"batched_{n}_random_instances_seed{args.seed}", "instances": n,
+                   "states_total": sum(sizes), "max_iterations_run": rep["max_iterations_run"],
+                   "shapes": {"sat_threads": rep["sat_threads"], "sat_blocks_per_sm": rep["sat_blocks_per_sm"],
+                              "chunk_words": rep["chunk_words"], "tuned": rep0["tuned"],
+                              "tune_ms": rep0["tune_ms"]},
+                   "l2": "flushed before every step (256 MiB write)"},
+        "e2e": {"value": n / (e2e_ms * 1e-3), "unit": "instances/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
+                "note": "gsc_batch_create (abstractions + set-up) + graph solve + reads into pinned memory"},
+        "plain_sequential": {
+            "e2e_instances_per_s": n / (plain_total * 1e-3), "e2e_ms_total": plain_total,
+            "device_solve_ms_total": sum(plain_dev), "p50_ms": percentile(plain_ms, 50),
+            "p99_ms": percentile(plain_ms, 99),
+            "note": "per instance: abstraction + problem set-up + graph solve + read into pinned memory"},
+        "speedup_vs_plain": {"e2e": plain_total / e2e_ms, "fixpoint": sum(plain_dev) / step_ms},
+        "gpu_launches": launches,
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line))
+    ctx.close()
+
+
+def bench_served(args):
+    """A Poisson stream of seeded K-invariance queries (random_query: safe
+    set, candidate ellipse, disturbance bound, iteration cap) against three
+    resident abstractions (20x20x16x10 x 25, 65x65x38x25 x 100,
+    32x32x24x16 x 64 inputs).  First all queries at once (saturation), then
+    three arrival rates as fractions of that throughput; latency = scheduled
+    arrival to completion.  Beside it the same queries one at a time through
+    the plain API, and that sequential server's latencies at the same
+    arrival times (FIFO)."""
+    import queue
+    import numpy as np
+    import torch
+    import gsc_b200 as G
+
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    models = {"small": C.small_case(), "demo": C.demo_scale_case(), "mid": C.serve_mid_case()}
+    names = list(models)
+    ctx = G.Context(0)
+    absn = {k: G.Abstraction(ctx, c) for k, c in models.items()}
+    S = {k: int(np.prod(C.grid_shape(c)[0])) for k, c in models.items()}
+    rng = np.random.default_rng(args.seed)
+    pick = rng.integers(0, 3, size=args.queries)
+    qs = [(names[k], C.random_query(models[names[k]], args.seed, i)) for i, k in enumerate(pick)]
+    # Pinned result buffers, recycled: at most this many queries of a model in flight.
+    depth = {"small": 128, "demo": 24, "mid": 96}
+    pools = {k: queue.Queue() for k in names}
+    for k in names:
+        for _ in range(depth[k]):
+            pools[k].put(pinned_outputs(torch, S[k]))
+
+    def run_stream(srv, arrivals):
+        n = len(qs)
+        submit_t = [0.0] * n
+        server_lat = [0.0] * n
+        tickets = [None] * n
+        per_model = {k: queue.Queue() for k in names}
+        errors = []
+
+        def waiter(k):
+            while True:
+                item = per_model[k].get()
+                if item is None:
+                    return
+                i, t, buf = item
+                try:
+                    r = srv.wait(t)
+                    server_lat[i] = r["latency_ms"]
+                except Exception as e:   # noqa: BLE001
+                    errors.append(e)
+                pools[k].put(buf)
+
+        ths = [threading.Thread(target=waiter, args=(k,), daemon=True) for k in names]
+        for th in ths:
+            th.start()
+        t0 = time.perf_counter()
+        for i, (k, q) in enumerate(qs):
+            dt = arrivals[i] - (time.perf_counter() - t0)
+            if dt > 0:
+                time.sleep(dt)
+            buf = pools[k].get()
+            submit_t[i] = time.perf_counter() - t0
+            tickets[i] = srv.submit(absn[k], q, out=buf)
+            per_model[k].put((i, tickets[i], buf))
+        for k in names:
+            per_model[k].put(None)
+        for th in ths:
+            th.join()
+        total = time.perf_counter() - t0
+        if errors:
+            raise errors[0]
+        lat = [(submit_t[i] - arrivals[i]) * 1e3 + server_lat[i] for i in range(n)]
+        return total, lat
+
+    srv = G.Server(ctx, memory_budget=int(args.serve_budget_gb * (1 << 30)), max_slots=256)
+    # warm-up: a few queries of each model
+    warm = [srv.submit(absn[k], C.random_query(models[k], args.seed + 1, i)) for i, k in enumerate(names * 4)]
+    for t in warm:
+        srv.wait(t)
+    n = len(qs)
+    with ClockSampler(gpu_uuid(torch, dev)) as clocks:
+        sat_s, sat_lat = run_stream(srv, [0.0] * n)
+        X = n / sat_s
+        rates = []
+        for f in [float(v) for v in args.rates.split(",") if v]:
+            lam = f * X
+            arr = np.cumsum(np.random.default_rng(args.seed + 17).exponential(1.0 / lam, size=n)).tolist()
+            tot, lat = run_stream(srv, arr)
+            rates.append({"fraction_of_saturation": f, "rate_qps": lam, "throughput_qps": n / tot,
+                          "p50_ms": percentile(lat, 50), "p99_ms": percentile(lat, 99), "arrivals": arr})
+    st = srv.stats()
+    srv.close()
+
+    # Sequential plain solves: service time of every query (or a prefix).
+    m = args.plain_queries or n
+    plain_out = {k: pinned_outputs(torch, S[k]) for k in names}
+    for k in names:   # warm
+        plain_solve(G, ctx, absn[k], models[k], plain_out[k])
+    svc = []
+    for k, q in qs[:m]:
+        t0 = time.perf_counter()
+        plain_solve(G, ctx, absn[k], q, plain_out[k])
+        svc.append(time.perf_counter() - t0)
+    plain_qps = m / sum(svc)
+    full_svc = [svc[i % m] for i in range(n)]
+
+    def fifo(arr):
+        done, lat = 0.0, []
+        for a, s_ in zip(arr, full_svc):
+            done = max(done, a) + s_
+            lat.append((done - a) * 1e3)
+        return lat
+
+    for r in rates:
+        pl = fifo(r.pop("arrivals"))
+        r["plain_p50_ms"] = percentile(pl, 50)
+        r["plain_p99_ms"] = percentile(pl, 99)
+    line = {
+        "metric": "served queries/s", "value": X, "unit": "queries/s", "n_gpus": 1, "steps": 1,
+        "warmup": len(warm), "ms_per_step": sat_s * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32 bit-sliced sets / int32 counts (f64 boxes)", "data": "synthetic",
+        "config": {"workload": f"served_{n}_queries_3_models_seed{args.seed}",
+                   "models": {k: models[k]["name"] for k in names}, "queries": n,
+                   "budget_gb": args.serve_budget_gb, "result_buffers_in_flight": depth},
+        "saturation": {"throughput_qps": X, "p50_ms": percentile(sat_lat, 50), "p99_ms": percentile(sat_lat, 99)},
+        "rates": rates,
+        "e2e": {"value": X, "unit": "queries/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": int(sum(11 * S[k] for k, _ in qs)),
+                "note": "submit to results in pinned host memory, all queries"},
+        "plain_sequential": {"throughput_qps": plain_qps, "queries_timed": m,
+                             "p50_service_ms": percentile([x * 1e3 for x in svc], 50),
+                             "p99_service_ms": percentile([x * 1e3 for x in svc], 99)},
+        "speedup_vs_plain": X / plain_qps,
+        "server": st,
+        "gpu_launches": None,
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line))
+    for a in absn.values():
+        a.close()
+    ctx.close()
+
+
 def main():
     args = parse()
+    if args.workload in ("batched", "served") and args.impl != "reference":
+        (bench_batched if args.workload == "batched" else bench_served)(args)
+        return
+    if args.workload in ("batched", "served"):
+        print(json.dumps({"impl": "reference", "unavailable": "the reference has no batched or served mode"}))
+        return
     case = C.checked(C.PRESETS[args.workload]())
     if args.impl == "reference":
         run_reference_arm(args, case)

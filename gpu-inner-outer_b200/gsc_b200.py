@@ -326,8 +326,8 @@ class Problem:
         self.ctx.check(lib().gsc_problem_timings(self._h, ctypes.byref(t)))
         return {k: getattr(t, k) for k, _ in Timings._fields_}
 
-    def read(self, iter_capacity=4096, masks=True) -> dict:
-        return _read_result(lambda r: lib().gsc_problem_read(self._h, r), self.ctx, iter_capacity, masks)
+    def read(self, iter_capacity=4096, masks=True, out=None) -> dict:
+        return _read_result(lambda r: lib().gsc_problem_read(self._h, r), self.ctx, iter_capacity, masks, out)
 
     def export_abstraction(self):
         probe = Result()
@@ -351,15 +351,21 @@ class Problem:
             pass
 
 
-def _read_result(call, ctx, iter_capacity=4096, masks=True) -> dict:
+def _read_result(call, ctx, iter_capacity=4096, masks=True, out=None) -> dict:
     """Run a gsc_*_read call twice (shape probe, then the arrays) and return
-    the result as a dict of numpy arrays and scalars."""
+    the result as a dict of numpy arrays and scalars.  ``out`` may supply the
+    five arrays (e.g. views of pinned host memory)."""
     r = Result()
     probe = Result()
     ctx.check(call(ctypes.byref(probe)))
     S = int(probe.states)
-    out = {}
-    if masks:
+    if out is not None:
+        out = dict(out)
+        for k, v in out.items():
+            if v.size != S or not v.flags["C_CONTIGUOUS"]:
+                raise ValueError(f"out[{k}] must be a contiguous array of {S} elements")
+            setattr(r, k, _ptr(v))
+    elif masks:
         out = {
             "valid_mask": np.zeros(S, np.uint8), "candidate_mask": np.zeros(S, np.uint8),
             "reachable_mask": np.zeros(S, np.uint8), "controller": np.zeros(S, np.uint32),
@@ -367,6 +373,8 @@ def _read_result(call, ctx, iter_capacity=4096, masks=True) -> dict:
         }
         for k, v in out.items():
             setattr(r, k, _ptr(v))
+    else:
+        out = {}
     nr = np.zeros(iter_capacity, np.uint64)
     nc = np.zeros(iter_capacity, np.uint64)
     r.iter_new_reachable = _ptr(nr)
@@ -407,8 +415,9 @@ class Batch:
     def solve(self, graph=True):
         self.ctx.check(lib().gsc_batch_solve(self._h, SOLVE_GRAPH if graph else 0))
 
-    def read(self, index, iter_capacity=4096, masks=True) -> dict:
-        return _read_result(lambda r: lib().gsc_batch_read(self._h, int(index), r), self.ctx, iter_capacity, masks)
+    def read(self, index, iter_capacity=4096, masks=True, out=None) -> dict:
+        return _read_result(lambda r: lib().gsc_batch_read(self._h, int(index), r), self.ctx, iter_capacity, masks,
+                            out)
 
     def report(self) -> dict:
         t = BatchReport()
