@@ -8,7 +8,9 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -255,16 +257,29 @@ void* DevicePool::alloc(uint64_t bytes) {
         }
         if (slab_bytes == 0) return nullptr;
     }
-    uint64_t n = gsc_b200::RangePool::rounded(bytes);
-    if (n < slab_bytes) n = slab_bytes;
-    if (cap && total + n > cap) {
-        if (total + gsc_b200::RangePool::rounded(bytes) > cap) return nullptr;
-        n = cap - total;
-    }
-    if (!reserve(n)) return nullptr;
+    const uint64_t need = gsc_b200::RangePool::rounded(bytes);
+    if (cap && total + need > cap) return nullptr;
+    uint64_t n = std::max(need, slab_bytes);
+    if (cap && total + n > cap) n = cap - total;
+    // A full-size region when the budget allows it, else one of just this size.
+    if (!reserve(n) && (n == need || !reserve(need))) return nullptr;
     std::lock_guard<std::mutex> lk(mu);
     const uint64_t off = slabs.back().ranges.alloc(bytes);
     return off == gsc_b200::RangePool::kNone ? nullptr : slabs.back().base + off;
+}
+
+void DevicePool::trim() {
+    std::lock_guard<std::mutex> lk(mu);
+    for (size_t i = 0; i < slabs.size();) {
+        if (slabs[i].ranges.used() != 0) {
+            ++i;
+            continue;
+        }
+        cudaFree(slabs[i].base);
+        if (ctx) ctx->in_use -= slabs[i].bytes;
+        total -= slabs[i].bytes;
+        slabs.erase(slabs.begin() + i);
+    }
 }
 
 void DevicePool::release(void* p, uint64_t bytes) {
@@ -285,9 +300,13 @@ uint64_t DevicePool::used() {
     return u;
 }
 
-gsc_abstraction::~gsc_abstraction() { device_release_all(ctx, pool, allocs, bytes); }
+gsc_abstraction::~gsc_abstraction() {
+    if (sync_release && ctx) cudaStreamSynchronize(ctx->stream);
+    device_release_all(ctx, pool, allocs, bytes);
+}
 
 gsc_problem::~gsc_problem() {
+    if (sync_release && stream) cudaStreamSynchronize(stream);
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
     device_release_all(ctx, pool, allocs, bytes);
@@ -357,6 +376,12 @@ int gsc_context_create(int device, void* cuda_stream, gsc_context** out) {
         ctx->own_stream = true;
     }
     cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device);
+    ctx->pool.reset(new (std::nothrow) DevicePool(ctx, 64ull << 20, 0));
+    if (!ctx->pool) {
+        if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
+        delete ctx;
+        return GSC_ERR_OUT_OF_MEMORY;
+    }
     if (cudaEventCreate(&ctx->ev[0]) != cudaSuccess || cudaEventCreate(&ctx->ev[1]) != cudaSuccess) {
         if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
         delete ctx;
@@ -371,8 +396,16 @@ void gsc_context_destroy(gsc_context* ctx) {
     cudaSetDevice(ctx->device);
     if (ctx->ev[0]) cudaEventDestroy(ctx->ev[0]);
     if (ctx->ev[1]) cudaEventDestroy(ctx->ev[1]);
+    ctx->pool.reset();
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
+}
+
+int gsc_context_trim(gsc_context* ctx) {
+    if (!ctx) return GSC_ERR_INVALID_ARGUMENT;
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return GSC_ERR_CUDA;
+    if (ctx->pool) ctx->pool->trim();
+    return GSC_OK;
 }
 
 const char* gsc_last_error(const gsc_context* ctx) { return ctx ? ctx->last_error.c_str() : ""; }
@@ -394,6 +427,8 @@ int gsc_abstraction_create(gsc_context* ctx, const gsc_model_desc* model, gsc_ab
     if (!a) return GSC_ERR_OUT_OF_MEMORY;
     a->ctx = ctx;
     a->model = *model;
+    a->pool = ctx->pool.get();
+    a->sync_release = true;
     std::string err;
     const int s = grid_from_model(model, &a->g, &err);
     if (s != GSC_OK) return fail(ctx, s, err);
@@ -405,7 +440,7 @@ int gsc_abstraction_create(gsc_context* ctx, const gsc_model_desc* model, gsc_ab
     if (st == GSC_OK) e = cudaEventRecord(ctx->ev[1], ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     for (auto& t : tmp) tmp_bytes += t.second;
-    device_release_all(ctx, nullptr, tmp, tmp_bytes);
+    device_release_all(ctx, a->pool, tmp, tmp_bytes);
     if (st != GSC_OK) return st;
     float ms = 0.f;
     if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);
@@ -770,6 +805,8 @@ int gsc_problem_create(gsc_context* ctx, const gsc_abstraction* abs, const gsc_q
     p->g = abs->g;
     p->stream = ctx->stream;
     p->method = method;
+    p->pool = ctx->pool.get();
+    p->sync_release = true;
     GSC_CU(ctx, cudaEventRecord(ctx->ev[0], ctx->stream));
     GSC_TRY(problem_stage1(p.get(), query));
     GSC_CU(ctx, cudaStreamSynchronize(ctx->stream));
@@ -1001,19 +1038,34 @@ int gsc_problem_timings(const gsc_problem* p, gsc_timings* out) {
 int gsc_run_case(int device, const gsc_model_desc* model, const gsc_query_desc* query, uint32_t method,
                  uint32_t flags, gsc_result* out, gsc_timings* timings) {
     if (!model || !query || !out) return GSC_ERR_INVALID_ARGUMENT;
+    // One context per device for the one-shot call, kept for the process, so
+    // repeated calls reuse its stream and its memory pool; calls on one
+    // device are serialised.
+    static std::mutex cache_mu;
+    static std::map<int, std::pair<gsc_context*, std::unique_ptr<std::mutex>>> cache;
     gsc_context* ctx = nullptr;
-    int s = gsc_context_create(device, nullptr, &ctx);
-    if (s != GSC_OK) return s;
+    std::mutex* dev_mu = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(cache_mu);
+        auto it = cache.find(device);
+        if (it == cache.end()) {
+            const int s = gsc_context_create(device, nullptr, &ctx);
+            if (s != GSC_OK) return s;
+            it = cache.emplace(device, std::make_pair(ctx, std::unique_ptr<std::mutex>(new std::mutex()))).first;
+        }
+        ctx = it->second.first;
+        dev_mu = it->second.second.get();
+    }
+    std::lock_guard<std::mutex> lk(*dev_mu);
     gsc_abstraction* abs = nullptr;
     gsc_problem* p = nullptr;
-    s = gsc_abstraction_create(ctx, model, &abs);
+    int s = gsc_abstraction_create(ctx, model, &abs);
     if (s == GSC_OK) s = gsc_problem_create(ctx, abs, query, method, &p);
     if (s == GSC_OK) s = gsc_problem_solve(p, flags);
     if (s == GSC_OK) s = gsc_problem_read(p, out);
     if (s == GSC_OK && timings) gsc_problem_timings(p, timings);
     gsc_problem_destroy(p);
     gsc_abstraction_destroy(abs);
-    gsc_context_destroy(ctx);
     return s;
 }
 

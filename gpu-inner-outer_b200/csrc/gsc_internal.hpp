@@ -5,6 +5,7 @@
 
 #include <atomic>
 #include <cstdint>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <utility>
@@ -38,6 +39,7 @@ struct DevicePool {
     void* alloc(uint64_t bytes);   // nullptr when no region fits and none may be added
     void release(void* p, uint64_t bytes);
     uint64_t used();
+    void trim();   // frees the regions nothing is allocated from
 };
 
 struct gsc_context {
@@ -50,6 +52,7 @@ struct gsc_context {
     std::mutex mem_mu;   // budget check + in_use update
     cudaEvent_t ev[2] = {nullptr, nullptr};
     int sm_count = 0;
+    std::unique_ptr<DevicePool> pool;   // caching pool of the context's problems and abstractions
 };
 
 struct gsc_abstraction {
@@ -64,6 +67,7 @@ struct gsc_abstraction {
     std::vector<std::pair<void*, uint64_t>> allocs;
     uint64_t bytes = 0;
     double build_ms = 0.0;
+    bool sync_release = false;   // wait for the context stream before the memory is reused
     ~gsc_abstraction();
 };
 
@@ -75,6 +79,7 @@ struct gsc_problem {
     uint32_t method = 0;          // requested, then the one chosen
     DevicePool* pool = nullptr;   // nullptr: every buffer cudaMalloc'd
     cudaStream_t stream = nullptr;
+    bool sync_release = false;    // wait for `stream` before the memory is reused
     std::vector<std::pair<void*, uint64_t>> allocs;
     uint64_t bytes = 0;
     // masks and tables

@@ -126,6 +126,7 @@ SIGNATURES = {
     "gsc_last_error": (ctypes.c_char_p, [_P]),
     "gsc_context_set_memory_budget": (ctypes.c_int, [_P, ctypes.c_uint64]),
     "gsc_context_memory_in_use": (ctypes.c_uint64, [_P]),
+    "gsc_context_trim": (ctypes.c_int, [_P]),
     "gsc_abstraction_create": (ctypes.c_int, [_P, ctypes.POINTER(ModelDesc), ctypes.POINTER(_P)]),
     "gsc_abstraction_destroy": (None, [_P]),
     "gsc_problem_create": (ctypes.c_int, [_P, _P, ctypes.POINTER(QueryDesc), ctypes.c_uint32, ctypes.POINTER(_P)]),
@@ -262,6 +263,10 @@ class Context:
 
     def memory_in_use(self):
         return int(lib().gsc_context_memory_in_use(self._h))
+
+    def trim(self):
+        """Return the pool regions no handle uses to the driver."""
+        self.check(lib().gsc_context_trim(self._h))
 
     def close(self):
         if self._h:

@@ -197,15 +197,23 @@ const char* gsc_message_string(int message);
 int gsc_grid_shape(const gsc_model_desc* model, uint32_t shape[4], uint32_t input_shape[2]);
 
 /* A context binds a device and a stream (NULL stream = a private stream).
- * Mirrors the device checks of kernels.cu:496-502. */
+ * Mirrors the device checks of kernels.cu:496-502.  Problems and
+ * abstractions of a context take their device memory from the context's
+ * caching pool (regions of 64 MB or more, sub-allocated first-fit), so a
+ * create / destroy cycle costs no cudaMalloc / cudaFree once warm; memory
+ * returns to the driver at gsc_context_trim or gsc_context_destroy. */
 int gsc_context_create(int device, void* cuda_stream, gsc_context** out);
-/* Destroy every problem and abstraction of a context before the context. */
+/* Destroy every problem, abstraction, batch and server of a context before
+ * the context. */
 void gsc_context_destroy(gsc_context* ctx);
 const char* gsc_last_error(const gsc_context* ctx);
-/* Device memory the context may hold in problems and abstractions (0 = no
- * limit).  Creation fails with GSC_ERR_OUT_OF_MEMORY beyond it. */
+/* Device memory the context may hold: its pool regions plus batches and
+ * servers (0 = no limit).  Creation fails with GSC_ERR_OUT_OF_MEMORY beyond it. */
 int gsc_context_set_memory_budget(gsc_context* ctx, uint64_t bytes);
+/* Device memory the context holds now (pool regions, in use or cached). */
 uint64_t gsc_context_memory_in_use(const gsc_context* ctx);
+/* Returns the pool regions no handle uses to the driver. */
+int gsc_context_trim(gsc_context* ctx);
 
 /* The nominal successor tables of abstraction_kernel (kernels.cu:164-217,
  * model.hpp:26-46) for every (cell, input), built once and kept resident. */

@@ -155,3 +155,35 @@ def test_resolve_same_problem_twice(ctx):
         assert_same_result(r1, golden_arrays("hyperbolic_mid_a"), "first")
         assert_same_result(r2, r1, "graph relaunch")
         assert_same_result(r3, r1, "host loop after graph")
+
+
+def test_context_pool_reuse_budget_and_trim():
+    """Problems of a context draw on its caching pool: a second create/destroy
+    cycle needs no new device memory, trim returns every unused region, and a
+    budget below an abstraction's needs is refused with GSC_ERR_OUT_OF_MEMORY."""
+    case = INDEX["small"]["case"]
+    with G.Context(0) as c:
+        a = G.Abstraction(c, case)
+        p = G.Problem(c, a, case, G.METHOD_FUSED)
+        p.solve(graph=True)
+        first = p.read()
+        p.close()
+        held = c.memory_in_use()
+        assert held > 0
+        for _ in range(3):
+            p = G.Problem(c, a, case, G.METHOD_FUSED)
+            p.solve(graph=True)
+            assert_same_result(p.read(), first, "reuse")
+            p.close()
+        assert c.memory_in_use() == held
+        a.close()
+        c.trim()
+        assert c.memory_in_use() == 0
+        c.set_memory_budget(1 << 20)   # below the abstraction's 1.3 MB of tables
+        with pytest.raises(G.GscError) as e:
+            G.Abstraction(c, case)
+        assert e.value.status == 3
+        assert c.memory_in_use() <= 1 << 20
+        c.set_memory_budget(0)
+        got = solve(c, case, G.METHOD_FUSED, True)
+        assert_same_result(got, first, "after budget")
