@@ -533,6 +533,8 @@ int problem_stage1(gsc_problem* p, const gsc_query_desc* qd) {
     ma.build_cand = qd->candidate_mask ? 0 : 1;
     ma.safe = qd->safe_mask ? p->safe : nullptr;
     ma.safe_rank = p->safe_rank;
+    ma.cmp_safe = p->safe;
+    ma.cmp_rank = p->safe_rank;
     ma.counts = p->counts;
     GSC_CU(ctx, launch_masks(g, q, ma, st));
 
@@ -544,18 +546,18 @@ int problem_stage1(gsc_problem* p, const gsc_query_desc* qd) {
     GSC_TRY(palloc(p, &p->wt, static_cast<uint64_t>(g.n[3]) * g.ma));
     GSC_CU(ctx, launch_axis_tables(g, q, p->abs->xn, p->abs->yn, p->abs->thf, p->abs->vf, p->xt, p->yt, p->zt, p->wt,
                                    p->flags, st));
-    if (p->safe) GSC_CU(ctx, launch_valid_vs_safe(g, p->valid, p->safe, p->safe_rank, p->counts + 4, st));
 
     // Fused tables that do not depend on the sets, and the plan.
+    GSC_TRY(palloc(p, &p->dplan, 1));
+    GSC_CU(ctx, cudaMemsetAsync(p->dplan, 0, sizeof(PlanRecord), st));
     if (p->fused_candidate) {
         GSC_TRY(palloc(p, &p->xcls, planes * class_words(g)));
         GSC_CU(ctx, launch_x_classes(g, p->xt, p->xcls, st));
         GSC_TRY(palloc(p, &p->xrep, planes));
-        GSC_CU(ctx, launch_plane_reps(g, p->xt, p->yt, p->wt, p->xrep, st));
+        GSC_CU(ctx, launch_plane_reps(g, p->xt, p->yt, p->wt, p->xrep, &p->dplan->max_reps, st));
         GSC_TRY(palloc(p, &p->kidx, static_cast<uint64_t>(g.n[2]) + 1));
         GSC_TRY(palloc(p, &p->lidx, static_cast<uint64_t>(g.n[3]) + 1));
     }
-    GSC_TRY(palloc(p, &p->dplan, 1));
     GSC_CU(ctx, launch_plan(g, p->zt, p->wt, p->fused_candidate ? p->xrep : nullptr, p->counts, p->flags, p->kidx,
                             p->lidx, p->dplan, st));
     if (!p->hplan) p->hplan = &p->hplan_own;

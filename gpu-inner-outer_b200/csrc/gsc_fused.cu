@@ -56,15 +56,14 @@ __global__ void k_dilate(GridInfo g, const bword* __restrict__ src, bword* __res
 
 // The set-up plan (one block): which theta widths (wrapped lengths of the
 // omega columns' theta boxes) and v widths (of the accelerations' v boxes)
-// occur, numbered in increasing order, and the most representative
-// accelerations of one omega column.
+// occur, numbered in increasing order.  out->max_reps (zeroed before, then
+// raised by k_plane_reps) becomes at least 1.
 __global__ void __launch_bounds__(256) k_plan(GridInfo g, const uint32_t* __restrict__ zt,
                                               const uint32_t* __restrict__ wt, const uint8_t* __restrict__ xrep,
                                               const unsigned long long* __restrict__ counts,
                                               const unsigned int* __restrict__ flags, uint8_t* __restrict__ kidx,
                                               uint8_t* __restrict__ lidx, PlanRecord* __restrict__ out) {
     __shared__ uint32_t kbits[2048], lbits[2048];   // widths 1 .. 65535
-    __shared__ uint32_t s_maxrep;
     __shared__ DilateArgs s_dil;
     const uint32_t tid = threadIdx.x;
     if (tid < 8) out->counts[tid] = counts[tid];
@@ -82,7 +81,6 @@ __global__ void __launch_bounds__(256) k_plan(GridInfo g, const uint32_t* __rest
     }
     const uint32_t n2 = g.n[2], n3 = g.n[3];
     for (uint32_t i = tid; i < 2048; i += blockDim.x) kbits[i] = lbits[i] = 0;
-    if (tid == 0) s_maxrep = 1;
     __syncthreads();
     for (uint32_t e = tid; e < n2 * g.mw; e += blockDim.x) {
         const uint32_t ze = zt[e];
@@ -96,14 +94,6 @@ __global__ void __launch_bounds__(256) k_plan(GridInfo g, const uint32_t* __rest
         const uint32_t l = hi16(we) - lo16(we) + 1;
         atomicOr(&lbits[l >> 5], 1u << (l & 31));
     }
-    const uint64_t columns = static_cast<uint64_t>(g.slices) * g.mw;
-    uint32_t mr = 1;
-    for (uint64_t c = tid; c < columns; c += blockDim.x) {
-        uint32_t n = 0;
-        for (uint32_t ja = 0; ja < g.ma; ++ja) n += xrep[c * g.ma + ja] == ja;
-        mr = max(mr, n);
-    }
-    atomicMax(&s_maxrep, mr);
     __syncthreads();
     if (tid == 0) {
         DilateArgs d{};
@@ -128,7 +118,7 @@ __global__ void __launch_bounds__(256) k_plan(GridInfo g, const uint32_t* __rest
         s_dil = d;
         out->dil = d;
         out->width_overflow = over;
-        out->max_reps = s_maxrep;
+        out->max_reps = max(out->max_reps, 1u);   // raised by k_plane_reps
     }
     __syncthreads();
     for (uint32_t k = tid; k <= n2; k += blockDim.x) {

@@ -23,7 +23,9 @@ struct MaskArgs {
     int build_cand;
     const uint8_t* safe;      // caller's constraint mask (rank 2 or 4), or null: use the constraint kind
     int safe_rank;
-    unsigned long long* counts;  // [0] valid, [1] candidate, [2] candidate-not-valid
+    const uint8_t* cmp_safe;  // safety at the centres (rank cmp_rank), to count cells whose validity differs
+    int cmp_rank;
+    unsigned long long* counts;  // [0] valid, [1] candidate, [2] candidate-not-valid, [4] valid != safe
 };
 cudaError_t launch_masks(const GridInfo& g, const QueryInfo& q, const MaskArgs& a, cudaStream_t st);
 cudaError_t launch_safe2(const GridInfo& g, const QueryInfo& q, uint8_t* safe2, cudaStream_t st);
@@ -41,10 +43,6 @@ cudaError_t launch_axis_tables(const GridInfo& g, const QueryInfo& q, const doub
 cudaError_t launch_pack_bits(const GridInfo& g, int mode, const uint8_t* src, const uint8_t* src2, bword* out,
                              cudaStream_t st);
 cudaError_t launch_unpack_bits(const GridInfo& g, const bword* bits, uint8_t* out, cudaStream_t st);
-
-// Counts cells with valid != safe (safe rank 2 or 4) into *count.
-cudaError_t launch_valid_vs_safe(const GridInfo& g, const uint8_t* valid, const uint8_t* safe, int safe_rank,
-                                 unsigned long long* count, cudaStream_t st);
 
 // ---- 4-D inclusive prefix tables (int32, zero first plane per dimension) -----------------
 // mode 0: valid; 1: valid && !reach (b = reach); 2: !safe (4-D safe mask).
@@ -225,8 +223,9 @@ cudaError_t launch_x_classes(const GridInfo& g, const uint32_t* xt, bword* xcls,
 // whose x row, y row and v box equal those of ja, so the two inputs test every
 // state alike (with one Euler substep the x and y successors do not depend on
 // the acceleration at all).
+// Also raises *max_reps to the most representatives of one omega column.
 cudaError_t launch_plane_reps(const GridInfo& g, const uint32_t* xt, const uint32_t* yt, const uint32_t* wt,
-                              uint8_t* xrep, cudaStream_t st);
+                              uint8_t* xrep, uint32_t* max_reps, cudaStream_t st);
 cudaError_t launch_fused_init(const GridInfo& g, const FusedFixArgs& a, const uint8_t* cand, cudaStream_t st);
 cudaError_t launch_fused_iteration(const GridInfo& g, const FusedFixArgs& a, cudaStream_t st, uint32_t* launches,
                                    cudaEvent_t* ev = nullptr);

@@ -25,6 +25,14 @@ inline unsigned int blocks_for(uint64_t n, int threads = kThreads) {
     return static_cast<unsigned int>(b);
 }
 
+// Blocks of kPlaneThreads threads for one warp per task, at most 16 per SM
+// worth of a 148-SM part (the kernels stride over the rest).
+inline unsigned int warp_blocks(uint64_t tasks) {
+    uint64_t b = (tasks + 7) / 8;
+    if (b > 148ull * 16) b = 148ull * 16;
+    return static_cast<unsigned int>(b ? b : 1);
+}
+
 __device__ __forceinline__ void unflatten(const GridInfo& g, uint64_t s, uint32_t idx[4]) {
     uint64_t r = s / g.n[0];
     idx[0] = static_cast<uint32_t>(s - r * g.n[0]);
@@ -42,30 +50,56 @@ __device__ __forceinline__ bool in_rect(const double* lb, const double* ub, cons
 
 // ---- nominal successors -----------------------------------------------------------------
 
-// One thread per (plane, i) entry.  plane = (i2*n3 + i3)*M + j.
-__global__ void k_nominal_xy(GridInfo g, const double* __restrict__ cosT, const double* __restrict__ sinT,
-                             const double* __restrict__ vseq, double* __restrict__ xn, double* __restrict__ yn) {
+// One warp per plane (i2, i3, j), plane = (i2*n3 + i3)*M + j; lanes over
+// the x then the y cells.  The plane's trajectory terms dt * (v * cos theta)
+// and dt * (v * sin theta) do not depend on the cell, so each is computed once
+// (staged in shared memory for up to kTermsMax substeps) and added to the
+// cell centre in the reference's order (model.hpp:34-45).
+constexpr int kPlaneThreads = 256;
+constexpr uint32_t kTermsMax = 64;
+
+__global__ void __launch_bounds__(kPlaneThreads) k_nominal_xy(GridInfo g, const double* __restrict__ cosT,
+                                                             const double* __restrict__ sinT,
+                                                             const double* __restrict__ vseq,
+                                                             double* __restrict__ xn, double* __restrict__ yn) {
+    __shared__ double terms[kPlaneThreads / 32][2][kTermsMax];
+    const uint32_t lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const uint64_t planes = static_cast<uint64_t>(g.slices) * g.M;
-    const uint64_t nx = planes * g.n[0];
-    const uint64_t total = nx + planes * g.n[1];
-    for (uint64_t e = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; e < total;
-         e += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        const bool is_x = e < nx;
-        const uint64_t ee = is_x ? e : e - nx;
-        const uint32_t n = is_x ? g.n[0] : g.n[1];
-        const uint64_t plane = ee / n;
-        const uint32_t i = static_cast<uint32_t>(ee - plane * n);
+    const uint64_t wstride = static_cast<uint64_t>(gridDim.x) * (blockDim.x >> 5);
+    const uint32_t K = g.K;
+    const bool staged = K <= kTermsMax;
+    for (uint64_t plane = blockIdx.x * static_cast<uint64_t>(blockDim.x >> 5) + wib; plane < planes;
+         plane += wstride) {
         const uint32_t j = static_cast<uint32_t>(plane % g.M);
         const uint64_t q = plane / g.M;
         const uint32_t i3 = static_cast<uint32_t>(q % g.n[3]);
         const uint32_t i2 = static_cast<uint32_t>(q / g.n[3]);
         const uint32_t ja = j % g.ma, jw = j / g.ma;
-        const double* trig = (is_x ? cosT : sinT) + static_cast<uint64_t>(i2 * g.mw + jw) * g.K;
-        const double* vs = vseq + static_cast<uint64_t>(i3 * g.ma + ja) * g.K;
-        // out[d] += dt * (v * cos(theta)) per substep (model.hpp:34-45).
-        double c = centre(g, is_x ? 0 : 1, i);
-        for (uint32_t k = 0; k < g.K; ++k) c = dadd(c, dmul(g.dt, dmul(vs[k], trig[k])));
-        (is_x ? xn : yn)[ee] = c;
+        const double* cs = cosT + static_cast<uint64_t>(i2 * g.mw + jw) * K;
+        const double* sn = sinT + static_cast<uint64_t>(i2 * g.mw + jw) * K;
+        const double* vs = vseq + static_cast<uint64_t>(i3 * g.ma + ja) * K;
+        if (staged) {
+            __syncwarp();
+            for (uint32_t k = lane; k < K; k += 32) {
+                terms[wib][0][k] = dmul(g.dt, dmul(vs[k], cs[k]));
+                terms[wib][1][k] = dmul(g.dt, dmul(vs[k], sn[k]));
+            }
+            __syncwarp();
+        }
+        for (int axis = 0; axis < 2; ++axis) {
+            const uint32_t n = g.n[axis];
+            const double* trig = axis ? sn : cs;
+            double* out = (axis ? yn : xn) + plane * n;
+            for (uint32_t i = lane; i < n; i += 32) {
+                double c = centre(g, axis, i);
+                if (staged) {
+                    for (uint32_t k = 0; k < K; ++k) c = dadd(c, terms[wib][axis][k]);
+                } else {
+                    for (uint32_t k = 0; k < K; ++k) c = dadd(c, dmul(g.dt, dmul(vs[k], trig[k])));
+                }
+                out[i] = c;
+            }
+        }
     }
 }
 
@@ -73,61 +107,106 @@ __global__ void k_nominal_xy(GridInfo g, const double* __restrict__ cosT, const 
 
 // build_valid_mask / build_candidate_mask (abstraction.hpp:65-106) plus the
 // ellipse candidate; counts valid, candidate and candidate-but-invalid cells.
-__global__ void k_masks(GridInfo g, QueryInfo q, MaskArgs a) {
-    unsigned long long nv = 0, nc = 0, nbad = 0;
-    for (uint64_t s = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; s < g.S;
-         s += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        uint32_t idx[4];
-        unflatten(g, s, idx);
+// One warp per x-row (i1, i2, i3); lanes over i0.  The tests on
+// dimensions 1-3 (map, obstacles, candidate rectangle) and the y part of the
+// candidate ellipse are evaluated once per row; a rectangle test is the AND
+// of its per-dimension tests, so the split does not change any result.
+__global__ void __launch_bounds__(kPlaneThreads) k_masks(GridInfo g, QueryInfo q, MaskArgs a) {
+    unsigned long long nv = 0, nc = 0, nbad = 0, ndiff = 0;
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t wstride = static_cast<uint64_t>(gridDim.x) * (blockDim.x >> 5);
+    const bool few_obstacles = q.n_obstacles <= 32;
+    for (uint64_t r = blockIdx.x * static_cast<uint64_t>(blockDim.x >> 5) + (threadIdx.x >> 5); r < g.rows;
+         r += wstride) {
+        const uint32_t i1 = static_cast<uint32_t>(r % g.n[1]);
+        const uint64_t r2 = r / g.n[1];
+        const uint32_t i2 = static_cast<uint32_t>(r2 % g.n[2]);
+        const uint32_t i3 = static_cast<uint32_t>(r2 / g.n[2]);
         double x[4];
-        for (int d = 0; d < 4; ++d) x[d] = centre(g, d, idx[d]);
-        bool v;
-        if (a.build_valid) {
-            v = in_rect(q.map_lb, q.map_ub, x);
-            if (v) {
-                for (int o = 0; o < q.n_obstacles; ++o) {
-                    if (in_rect(a.obstacles + 8 * o, a.obstacles + 8 * o + 4, x)) {
-                        v = false;
-                        break;
+        x[1] = centre(g, 1, i1);
+        x[2] = centre(g, 2, i2);
+        x[3] = centre(g, 3, i3);
+        auto in_dims123 = [&](const double* lb, const double* ub) {
+            for (int d = 1; d < 4; ++d)
+                if (x[d] < lb[d] || x[d] > ub[d]) return false;
+            return true;
+        };
+        const bool map_row = in_dims123(q.map_lb, q.map_ub);
+        uint32_t obs_row = 0;
+        if (a.build_valid && few_obstacles)
+            for (int o = 0; o < q.n_obstacles; ++o)
+                if (in_dims123(a.obstacles + 8 * o, a.obstacles + 8 * o + 4)) obs_row |= 1u << o;
+        const bool cand_rect_row = q.cand_kind == 0 && in_dims123(q.cand, q.cand + 4);
+        const double dy = dsub(x[1], q.cand[1]);
+        const double ty = dmul(dmul(dy, dy), q.cand[3]);
+        const uint64_t base = r * g.n[0];
+        for (uint32_t i0 = lane; i0 < g.n[0]; i0 += 32) {
+            const uint64_t s = base + i0;
+            x[0] = centre(g, 0, i0);
+            bool v;
+            if (a.build_valid) {
+                v = map_row && !(x[0] < q.map_lb[0] || x[0] > q.map_ub[0]);
+                if (v) {
+                    if (few_obstacles) {
+                        for (uint32_t m = obs_row; m; m &= m - 1) {
+                            const int o = __ffs(m) - 1;
+                            if (!(x[0] < a.obstacles[8 * o] || x[0] > a.obstacles[8 * o + 4])) {
+                                v = false;
+                                break;
+                            }
+                        }
+                    } else {
+                        for (int o = 0; o < q.n_obstacles; ++o) {
+                            if (in_rect(a.obstacles + 8 * o, a.obstacles + 8 * o + 4, x)) {
+                                v = false;
+                                break;
+                            }
+                        }
                     }
                 }
-            }
-            // The constraint (abstraction.hpp:96-99): the caller's mask when given
-            // (a kCustom predicate evaluated at the centres), else the built-in kind.
-            if (v && a.safe)
-                v = (a.safe_rank == 4 ? a.safe[s] : a.safe[idx[1] * g.n[0] + idx[0]]) != 0;
-            else if (v && q.ckind != 0)
-                v = satisfies(q, x[0], x[1]);
-            a.valid[s] = v ? 1 : 0;
-        } else {
-            v = a.valid[s] != 0;
-        }
-        bool k;
-        if (a.build_cand) {
-            if (q.cand_kind == 0) {
-                k = in_rect(q.cand, q.cand + 4, x);
+                // The constraint (abstraction.hpp:96-99): the caller's mask when given
+                // (a kCustom predicate evaluated at the centres), else the built-in kind.
+                if (v && a.safe)
+                    v = (a.safe_rank == 4 ? a.safe[s] : a.safe[static_cast<uint64_t>(i1) * g.n[0] + i0]) != 0;
+                else if (v && q.ckind != 0)
+                    v = satisfies(q, x[0], x[1]);
+                a.valid[s] = v ? 1 : 0;
             } else {
-                const double dx = dsub(x[0], q.cand[0]);
-                const double dy = dsub(x[1], q.cand[1]);
-                k = v && (dadd(dmul(dmul(dx, dx), q.cand[2]), dmul(dmul(dy, dy), q.cand[3])) <= q.cand[4]);
+                v = a.valid[s] != 0;
             }
-            a.cand[s] = k ? 1 : 0;
-        } else {
-            k = a.cand[s] != 0;
+            bool k;
+            if (a.build_cand) {
+                if (q.cand_kind == 0) {
+                    k = cand_rect_row && !(x[0] < q.cand[0] || x[0] > q.cand[4]);
+                } else {
+                    const double dx = dsub(x[0], q.cand[0]);
+                    k = v && (dadd(dmul(dmul(dx, dx), q.cand[2]), ty) <= q.cand[4]);
+                }
+                a.cand[s] = k ? 1 : 0;
+            } else {
+                k = a.cand[s] != 0;
+            }
+            if (a.cmp_safe) {
+                const uint8_t sf =
+                    a.cmp_rank == 4 ? a.cmp_safe[s] : a.cmp_safe[static_cast<uint64_t>(i1) * g.n[0] + i0];
+                ndiff += (v != (sf != 0));
+            }
+            nv += v;
+            nc += k;
+            nbad += (k && !v);
         }
-        nv += v;
-        nc += k;
-        nbad += (k && !v);
     }
     for (int off = 16; off > 0; off >>= 1) {
         nv += __shfl_down_sync(0xFFFFFFFFu, nv, off);
         nc += __shfl_down_sync(0xFFFFFFFFu, nc, off);
         nbad += __shfl_down_sync(0xFFFFFFFFu, nbad, off);
+        ndiff += __shfl_down_sync(0xFFFFFFFFu, ndiff, off);
     }
     if ((threadIdx.x & 31) == 0) {
         if (nv) atomicAdd(&a.counts[0], nv);
         if (nc) atomicAdd(&a.counts[1], nc);
         if (nbad) atomicAdd(&a.counts[2], nbad);
+        if (ndiff) atomicAdd(&a.counts[4], ndiff);
     }
 }
 
@@ -144,39 +223,49 @@ __global__ void k_safe2(GridInfo g, QueryInfo q, uint8_t* safe2) {
 
 // ---- per-axis boxes ---------------------------------------------------------------------
 
-__global__ void k_axis_tables(GridInfo g, QueryInfo q, const double* __restrict__ xn, const double* __restrict__ yn,
-                              const double* __restrict__ thf, const double* __restrict__ vf, uint32_t* xt,
-                              uint32_t* yt, uint32_t* zt, uint32_t* wt, unsigned int* flags) {
+// x and y boxes: one warp per plane, radius once per plane (it depends on
+// the v cell only); theta and v boxes: one thread per entry after that.
+__global__ void __launch_bounds__(kPlaneThreads) k_axis_tables(GridInfo g, QueryInfo q,
+                                                              const double* __restrict__ xn,
+                                                              const double* __restrict__ yn,
+                                                              const double* __restrict__ thf,
+                                                              const double* __restrict__ vf, uint32_t* xt,
+                                                              uint32_t* yt, uint32_t* zt, uint32_t* wt,
+                                                              unsigned int* flags) {
     const uint64_t planes = static_cast<uint64_t>(g.slices) * g.M;
-    const uint64_t nx = planes * g.n[0];
-    const uint64_t ny = planes * g.n[1];
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t wstride = static_cast<uint64_t>(gridDim.x) * (blockDim.x >> 5);
+    unsigned int fl = 0;
+    for (uint64_t plane = blockIdx.x * static_cast<uint64_t>(blockDim.x >> 5) + (threadIdx.x >> 5);
+         plane < planes; plane += wstride) {
+        const uint32_t i3 = static_cast<uint32_t>((plane / g.M) % g.n[3]);
+        const double vc = centre(g, 3, i3);
+        for (int d = 0; d < 2; ++d) {
+            const uint32_t n = g.n[d];
+            const double r = box_radius(g, q, d, vc);
+            const double* nom = (d ? yn : xn) + plane * n;
+            uint32_t* out = (d ? yt : xt) + plane * n;
+            for (uint32_t i = lane; i < n; i += 32) {
+                uint32_t lo, hi;
+                const bool ok = axis_box(g, d, nom[i], r, &lo, &hi);
+                out[i] = ok ? pack16(lo, hi) : kReject;
+                if (ok && hi < lo) fl |= 1u;
+                if (ok && hi >= lo && hi - lo >= kBits) fl |= 2u;
+            }
+        }
+    }
     const uint64_t nz = static_cast<uint64_t>(g.n[2]) * g.mw;
     const uint64_t nw = static_cast<uint64_t>(g.n[3]) * g.ma;
-    const uint64_t total = nx + ny + nz + nw;
-    unsigned int fl = 0;
-    for (uint64_t e = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; e < total;
+    for (uint64_t e = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; e < nz + nw;
          e += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        if (e < nx + ny) {
-            const bool is_x = e < nx;
-            const uint64_t ee = is_x ? e : e - nx;
-            const uint32_t n = is_x ? g.n[0] : g.n[1];
-            const uint64_t plane = ee / n;
-            const uint32_t i3 = static_cast<uint32_t>((plane / g.M) % g.n[3]);
-            const int d = is_x ? 0 : 1;
-            const double r = box_radius(g, q, d, centre(g, 3, i3));
-            uint32_t lo, hi;
-            const bool ok = axis_box(g, d, (is_x ? xn : yn)[ee], r, &lo, &hi);
-            (is_x ? xt : yt)[ee] = ok ? pack16(lo, hi) : kReject;
-            if (ok && hi < lo) fl |= 1u;
-            if (ok && hi >= lo && hi - lo >= kBits) fl |= 2u;
-        } else if (e < nx + ny + nz) {
-            const uint32_t ee = static_cast<uint32_t>(e - nx - ny);   // i2 * mw + jw
+        if (e < nz) {
+            const uint32_t ee = static_cast<uint32_t>(e);   // i2 * mw + jw
             const double r = box_radius(g, q, 2, 0.0);
             uint32_t lo, hi;
             wrap_box(g, thf[ee], r, &lo, &hi);
             zt[ee] = pack16(lo, hi);
         } else {
-            const uint32_t ee = static_cast<uint32_t>(e - nx - ny - nz);   // i3 * ma + ja
+            const uint32_t ee = static_cast<uint32_t>(e - nz);   // i3 * ma + ja
             const double r = box_radius(g, q, 3, 0.0);
             uint32_t lo, hi;
             const bool ok = axis_box(g, 3, vf[ee], r, &lo, &hi);
@@ -189,6 +278,7 @@ __global__ void k_axis_tables(GridInfo g, QueryInfo q, const double* __restrict_
 
 // ---- bit-sliced sets --------------------------------------------------------------------
 
+// One thread per word: the 32 cells of word w of x-row r.
 __global__ void k_pack_bits(GridInfo g, int mode, const uint8_t* __restrict__ src, const uint8_t* __restrict__ src2,
                             bword* __restrict__ out) {
     const uint64_t words = g.rows * g.W;
@@ -216,32 +306,17 @@ __global__ void k_pack_bits(GridInfo g, int mode, const uint8_t* __restrict__ sr
     }
 }
 
-__global__ void k_unpack_bits(GridInfo g, const bword* __restrict__ bits, uint8_t* __restrict__ out) {
-    for (uint64_t s = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; s < g.S;
-         s += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        const uint64_t r = s / g.n[0];
-        const uint32_t i0 = static_cast<uint32_t>(s - r * g.n[0]);
-        out[s] = static_cast<uint8_t>((bits[r * g.W + i0 / kBits] >> (i0 % kBits)) & 1u);
+// One warp per x-row.
+__global__ void __launch_bounds__(kPlaneThreads) k_unpack_bits(GridInfo g, const bword* __restrict__ bits,
+                                                              uint8_t* __restrict__ out) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t wstride = static_cast<uint64_t>(gridDim.x) * (blockDim.x >> 5);
+    for (uint64_t r = blockIdx.x * static_cast<uint64_t>(blockDim.x >> 5) + (threadIdx.x >> 5); r < g.rows;
+         r += wstride) {
+        const bword* row = bits + r * g.W;
+        uint8_t* o = out + r * g.n[0];
+        for (uint32_t i0 = lane; i0 < g.n[0]; i0 += 32) o[i0] = static_cast<uint8_t>((row[i0 / kBits] >> (i0 % kBits)) & 1u);
     }
-}
-
-__global__ void k_valid_vs_safe(GridInfo g, const uint8_t* __restrict__ valid, const uint8_t* __restrict__ safe,
-                                int rank, unsigned long long* count) {
-    unsigned long long c = 0;
-    for (uint64_t s = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; s < g.S;
-         s += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        uint8_t sf;
-        if (rank == 4) {
-            sf = safe[s];
-        } else {
-            const uint64_t r = s / g.n[0];
-            const uint32_t i0 = static_cast<uint32_t>(s - r * g.n[0]);
-            sf = safe[(r % g.n[1]) * g.n[0] + i0];
-        }
-        c += ((valid[s] != 0) != (sf != 0));
-    }
-    for (int off = 16; off > 0; off >>= 1) c += __shfl_down_sync(0xFFFFFFFFu, c, off);
-    if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, c);
 }
 
 // ---- box counts on prefix tables --------------------------------------------------------
@@ -425,7 +500,7 @@ __global__ void k_x_classes(GridInfo g, const uint32_t* __restrict__ xt, bword* 
 constexpr int kThreadsReps = 128;
 
 __global__ void k_plane_reps(GridInfo g, const uint32_t* __restrict__ xt, const uint32_t* __restrict__ yt,
-                             const uint32_t* __restrict__ wt, uint8_t* __restrict__ rep) {
+                             const uint32_t* __restrict__ wt, uint8_t* __restrict__ rep, uint32_t* max_reps) {
     // One warp per column; the lanes compare a pair of planes' x and y rows
     // together.  Representatives are kept in increasing order, so an input
     // maps to the lowest earlier input with the same rows and v box.
@@ -434,6 +509,7 @@ __global__ void k_plane_reps(GridInfo g, const uint32_t* __restrict__ xt, const 
     uint8_t* reps = s_reps[wib];
     const uint64_t columns = static_cast<uint64_t>(g.slices) * g.mw;
     const uint64_t wstride = static_cast<uint64_t>(gridDim.x) * (blockDim.x >> 5);
+    uint32_t most = 0;
     for (uint64_t col = blockIdx.x * static_cast<uint64_t>(blockDim.x >> 5) + wib; col < columns; col += wstride) {
         // Planes are ((i2 * n3 + i3) * M + j) with j = ja + ma * jw, so column
         // col = (i2 * n3 + i3) * mw + jw starts at plane col * ma.
@@ -463,7 +539,9 @@ __global__ void k_plane_reps(GridInfo g, const uint32_t* __restrict__ xt, const 
             if (lane == 0) rep[p0 + ja] = static_cast<uint8_t>(r);
             __syncwarp();
         }
+        most = max(most, nrep);
     }
+    if (lane == 0 && most) atomicMax(max_reps, most);
 }
 
 // 2-D prefix of unsafe (x, y) centres; one block: rows, then columns.
@@ -491,13 +569,13 @@ __global__ void k_prefix2(GridInfo g, const uint8_t* __restrict__ safe2, int32_t
 
 cudaError_t launch_nominal_xy(const GridInfo& g, const double* cosT, const double* sinT, const double* vseq,
                               double* xn, double* yn, cudaStream_t st) {
-    const uint64_t total = static_cast<uint64_t>(g.slices) * g.M * (g.n[0] + g.n[1]);
-    k_nominal_xy<<<blocks_for(total), kThreads, 0, st>>>(g, cosT, sinT, vseq, xn, yn);
+    k_nominal_xy<<<warp_blocks(static_cast<uint64_t>(g.slices) * g.M), kPlaneThreads, 0, st>>>(g, cosT, sinT, vseq,
+                                                                                            xn, yn);
     return cudaGetLastError();
 }
 
 cudaError_t launch_masks(const GridInfo& g, const QueryInfo& q, const MaskArgs& a, cudaStream_t st) {
-    k_masks<<<blocks_for(g.S), kThreads, 0, st>>>(g, q, a);
+    k_masks<<<warp_blocks(g.rows), kPlaneThreads, 0, st>>>(g, q, a);
     return cudaGetLastError();
 }
 
@@ -509,10 +587,9 @@ cudaError_t launch_safe2(const GridInfo& g, const QueryInfo& q, uint8_t* safe2, 
 cudaError_t launch_axis_tables(const GridInfo& g, const QueryInfo& q, const double* xn, const double* yn,
                                const double* thf, const double* vf, uint32_t* xt, uint32_t* yt, uint32_t* zt,
                                uint32_t* wt, unsigned int* flags, cudaStream_t st) {
-    const uint64_t planes = static_cast<uint64_t>(g.slices) * g.M;
-    const uint64_t total = planes * (g.n[0] + g.n[1]) + static_cast<uint64_t>(g.n[2]) * g.mw +
-                           static_cast<uint64_t>(g.n[3]) * g.ma;
-    k_axis_tables<<<blocks_for(total), kThreads, 0, st>>>(g, q, xn, yn, thf, vf, xt, yt, zt, wt, flags);
+    k_axis_tables<<<warp_blocks(static_cast<uint64_t>(g.slices) * g.M), kPlaneThreads, 0, st>>>(g, q, xn, yn, thf,
+                                                                                             vf, xt, yt, zt, wt,
+                                                                                             flags);
     return cudaGetLastError();
 }
 
@@ -523,13 +600,7 @@ cudaError_t launch_pack_bits(const GridInfo& g, int mode, const uint8_t* src, co
 }
 
 cudaError_t launch_unpack_bits(const GridInfo& g, const bword* bits, uint8_t* out, cudaStream_t st) {
-    k_unpack_bits<<<blocks_for(g.S), kThreads, 0, st>>>(g, bits, out);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_valid_vs_safe(const GridInfo& g, const uint8_t* valid, const uint8_t* safe, int safe_rank,
-                                 unsigned long long* count, cudaStream_t st) {
-    k_valid_vs_safe<<<blocks_for(g.S), kThreads, 0, st>>>(g, valid, safe, safe_rank, count);
+    k_unpack_bits<<<warp_blocks(g.rows), kPlaneThreads, 0, st>>>(g, bits, out);
     return cudaGetLastError();
 }
 
@@ -549,11 +620,11 @@ cudaError_t launch_x_classes(const GridInfo& g, const uint32_t* xt, bword* xcls,
 }
 
 cudaError_t launch_plane_reps(const GridInfo& g, const uint32_t* xt, const uint32_t* yt, const uint32_t* wt,
-                              uint8_t* xrep, cudaStream_t st) {
+                              uint8_t* xrep, uint32_t* max_reps, cudaStream_t st) {
     const uint64_t warps = static_cast<uint64_t>(g.slices) * g.mw;
     uint64_t b = (warps + kThreadsReps / 32 - 1) / (kThreadsReps / 32);
     if (b > 8192) b = 8192;
-    k_plane_reps<<<static_cast<unsigned int>(b), kThreadsReps, 0, st>>>(g, xt, yt, wt, xrep);
+    k_plane_reps<<<static_cast<unsigned int>(b), kThreadsReps, 0, st>>>(g, xt, yt, wt, xrep, max_reps);
     return cudaGetLastError();
 }
 
