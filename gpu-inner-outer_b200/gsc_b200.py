@@ -138,6 +138,7 @@ SIGNATURES = {
     "gsc_run_case": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ModelDesc), ctypes.POINTER(QueryDesc),
                                     ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(Result),
                                     ctypes.POINTER(Timings)]),
+    "gsc_problem_simulate": (ctypes.c_int, [_P, ctypes.c_uint32, _P, ctypes.c_uint32, ctypes.c_uint64, _P, _P, _P]),
     "gsc_batch_create": (ctypes.c_int, [_P, ctypes.c_uint32, ctypes.POINTER(ModelDesc), ctypes.POINTER(QueryDesc),
                                         ctypes.POINTER(BatchOptions), ctypes.POINTER(_P)]),
     "gsc_batch_solve": (ctypes.c_int, [_P, ctypes.c_uint32]),
@@ -333,6 +334,22 @@ class Problem:
 
     def read(self, iter_capacity=4096, masks=True, out=None) -> dict:
         return _read_result(lambda r: lib().gsc_problem_read(self._h, r), self.ctx, iter_capacity, masks, out)
+
+    def simulate(self, x0, steps, seed, trajectories=True) -> dict:
+        """Closed-loop trajectories under the solved controller from each row
+        of x0 ([n][4]): ``trajectories`` [n][steps+1][4] (when asked),
+        ``final_states`` [n][4] and ``steps_done`` [n]."""
+        x0 = np.ascontiguousarray(x0, dtype=np.float64).reshape(-1, 4)
+        n = x0.shape[0]
+        tr = np.zeros((n, steps + 1, 4)) if trajectories else None
+        fin = np.zeros((n, 4))
+        done = np.zeros(n, np.uint32)
+        self.ctx.check(lib().gsc_problem_simulate(self._h, n, _ptr(x0), int(steps), int(seed), _ptr(tr), _ptr(fin),
+                                                  _ptr(done)))
+        out = {"final_states": fin, "steps_done": done}
+        if trajectories:
+            out["trajectories"] = tr
+        return out
 
     def export_abstraction(self):
         probe = Result()

@@ -277,6 +277,23 @@ int gsc_fixpoint_noalloc(const uint32_t shape[4], uint32_t inputs, int32_t wrap_
                          const uint8_t* candidate_mask, uint32_t max_iterations, uint8_t* reachable_mask,
                          uint32_t* controller, uint32_t* reach_step, gsc_result* summary, void* cuda_stream);
 
+/* ---- Closed-loop simulation of the controller ----------------------------
+ * The consumer of the controller table, plots/postprocess_controller.py:66-224:
+ * trajectories of the continuous unicycle under the problem's controller
+ * (after gsc_problem_solve), one device thread per trajectory reading the
+ * device-resident table.  Each sample period maps the state to a cell as
+ * the script does (theta wrapped with atan2(sin, cos), round((x - lb) / eta)
+ * half to even, clamped; :66-101), stops at the invalid input (:103-130),
+ * and takes integration_substeps Euler substeps x + dt * (f(x, u) + w) with
+ * theta re-wrapped (:132-176).  w is uniform in [-dhw, dhw] per dimension
+ * and substep, drawn from Philox4x32-10 keyed by `seed` (counter: substep
+ * and trajectory), so a run is reproducible; the script draws from numpy's
+ * global generator instead.  x0: [count][4]; trajectories (optional):
+ * [count][steps + 1][4], rows after a stop left 0 as in the script;
+ * final_states (optional): [count][4]; steps_done (optional): [count]. */
+int gsc_problem_simulate(gsc_problem* problem, uint32_t count, const double* x0, uint32_t steps, uint64_t seed,
+                         double* trajectories, double* final_states, uint32_t* steps_done);
+
 /* ---- Batched instances --------------------------------------------------
  * No counterpart in the reference (which solves one case per call).  Many
  * independent instances -- each its own model and query, of any grid and

@@ -95,3 +95,30 @@ def test_spot_step_agrees_with_full_solve():
     assert np.array_equal(rn, b["reachable_mask"])
     assert np.array_equal(ct, b["controller"])
     assert np.array_equal(st, b["reach_step"])
+
+
+def test_simulation_oracle_matches_reference_fixtures():
+    """oracle/sim_oracle.py against trajectories made by the reference's own
+    get_control_input / update_state (tests/golden/make_sim_golden.py)."""
+    import json
+    import os
+
+    import sim_oracle as S
+
+    here = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    with open(os.path.join(here, "sim_index.json")) as f:
+        sims = json.load(f)
+    index = golden_index()
+    for name in sims:
+        case = index[name]["case"]
+        z = np.load(os.path.join(here, f"sim_{name}.npz"))
+        shape, ishape = C.grid_shape(case)
+        grid = {"state_lb": case["state_lb"], "state_eta": case["state_eta"], "shape": list(shape),
+                "input_lb": case["input_lb"], "input_eta": case["input_eta"], "input_shape": list(ishape),
+                "sample_time": case["sample_time"], "integration_substeps": case["integration_substeps"],
+                "disturbance_half_width": case["disturbance_half_width"]}
+        traj, done = S.simulate(golden_arrays(name)["controller"], grid, z["x0"], int(z["steps"]), int(z["seed"]))
+        assert np.array_equal(done, z["steps_done"]), name
+        assert np.array_equal(traj, z["trajectories"]), name
+        assert done.max() > 0 and done.min() == 0   # both stopped and running trajectories are covered
+
