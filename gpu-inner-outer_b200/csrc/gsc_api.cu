@@ -581,6 +581,8 @@ int problem_plan(gsc_problem* p) {
     if (fused_ok) {
         p->max_reps = pl.max_reps;
         p->dil = pl.dil;
+        // dilated-row offsets are 32-bit in the satisfaction kernel
+        if (static_cast<uint64_t>(pl.dil.nk) * pl.dil.nl * g.rows * g.W >= 0xFFFFFFFFull) fused_ok = false;
         if (fused_smem_bytes(g, class_words(g), p->need_valid, p->max_reps) > kFusedSmemMax) fused_ok = false;
     }
     uint32_t method = p->method;
@@ -651,7 +653,7 @@ int problem_stage2(gsc_problem* p) {
     GSC_TRY(palloc(p, &p->hit, words));
     GSC_TRY(palloc(p, &p->best, g.S));
     const uint64_t combos = static_cast<uint64_t>(p->dil.nk) * p->dil.nl;
-    GSC_TRY(palloc(p, &p->dzw, combos * words));
+    GSC_TRY(palloc(p, &p->dzw, 2 * combos * words));
     GSC_CU(ctx, launch_pack_bits(g, 0, p->valid, nullptr, p->validb, st));
     GSC_CU(ctx, launch_pack_bits(g, 0, p->cand, nullptr, p->candb, st));
     if (!p->safe) {
@@ -666,7 +668,7 @@ int problem_stage2(gsc_problem* p) {
     }
     if (p->need_valid) {
         GSC_TRY(palloc(p, &p->vzw, combos * words));
-        GSC_CU(ctx, launch_dilate(g, p->validb, p->vzw, p->dil, nullptr, st));
+        GSC_CU(ctx, launch_dilate(g, p->validb, p->vzw, 0, p->dil, nullptr, st));
     }
     return GSC_OK;
 }
@@ -722,6 +724,7 @@ FusedFixArgs fused_args(const gsc_problem* p, cudaGraphConditionalHandle cond, i
     a.cls_words = class_words(p->g);
     a.max_reps = p->max_reps;
     a.dzw = p->dzw;
+    a.dzw_half = static_cast<uint64_t>(p->dil.nk) * p->dil.nl * p->g.rows * p->g.W;
     a.vzw = p->vzw;
     a.kidx = p->kidx;
     a.lidx = p->lidx;

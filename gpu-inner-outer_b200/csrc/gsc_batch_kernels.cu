@@ -56,9 +56,10 @@ __global__ void __launch_bounds__(256) k_batch_dilate(const InstanceDesc* __rest
         const uint32_t k = find_task(wl.dil_off, wl.n, t);
         const InstanceDesc& d = descs[wl.slot[k]];
         if (d.a.fc->stop) continue;
+        bword* out = d.a.dzw + (d.a.fc->iter & 1) * d.a.dzw_half;
         const uint32_t b = (t - wl.dil_off[k]) * wl.chunk;
         const uint32_t end = min(b + wl.chunk, d.words);
-        for (uint32_t p = b + threadIdx.x; p < end; p += blockDim.x) dilate_position(d.g, d.a.dp, d.a.dzw, d.a.dil, p);
+        for (uint32_t p = b + threadIdx.x; p < end; p += blockDim.x) dilate_position(d.g, d.a.dp, out, d.a.dil, p);
     }
 }
 

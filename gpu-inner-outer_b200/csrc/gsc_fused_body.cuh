@@ -131,6 +131,8 @@ __device__ __forceinline__ void dilate_position(const GridInfo& g, const bword* 
 // WMAX: register words per row; EXACTW: g.W == WMAX (else g.W <= WMAX at run
 // time).  NVMODE: 0 / 1 = validity test off / on, 2 = a.need_valid decides.
 // Every early return is taken by the whole block.
+constexpr unsigned long long kIncrementalRows = 16;
+
 template <int WMAX, bool EXACTW, int NVMODE>
 __device__ __forceinline__ void sat_col_task(const GridInfo& g, const FusedFixArgs& a, uint32_t task,
                                              bword* smem, uint32_t* s_nrep) {
@@ -156,6 +158,7 @@ __device__ __forceinline__ void sat_col_task(const GridInfo& g, const FusedFixAr
     bword* cls = sat + mr * nw;                           // max_reps * cw
     uint32_t* yts = cls + mr * cw;                        // max_reps * n1
     uint32_t* reps = yts + mr * n1;                       // ma: acceleration of each representative slot
+    uint8_t* rowchg = reinterpret_cast<uint8_t*>(reps + ma);   // max_reps * n1: E row lost a bit
 
     const uint64_t pcol = (static_cast<uint64_t>(i2) * g.n[3] + i3) * g.M + static_cast<uint64_t>(ma) * jw;
     int any = 0;
@@ -164,6 +167,7 @@ __device__ __forceinline__ void sat_col_task(const GridInfo& g, const FusedFixAr
         act[e] = v;
         any |= (v != 0);
     }
+    for (uint32_t e = tid; e < (mr * n1 + 3) / 4; e += bd) reinterpret_cast<uint32_t*>(rowchg)[e] = 0;
     if (tid < 32) {
         // Representatives in increasing acceleration order (warp ballot).
         uint32_t n = 0;
@@ -179,23 +183,41 @@ __device__ __forceinline__ void sat_col_task(const GridInfo& g, const FusedFixAr
     any = __syncthreads_or(any);
     const uint32_t nrep = *s_nrep;
     if (!any || nrep == 0) return;
-    if (tid == 0) atomicAdd(a.stats + kStatsCols * (fc->iter + 1) + 3, static_cast<unsigned long long>(nrep));
 
     // B. dilated D' rows at each representative's (theta, v) box corner.
+    // After the first iteration, every active state failed every input in
+    // the previous one, and D' only loses cells, so a state can newly pass
+    // only where its box lost a D' cell: where the previous iteration's
+    // dilated row had a bit that this one has not.  When the previous
+    // iteration added few states (at most one per kIncrementalRows x-rows;
+    // a new state touches the items of about that many rows), a block with
+    // no such bit, and a (representative, row) item whose y range has none,
+    // is skipped: its states still fail.  With more new states nearly every
+    // item is touched, and the extra loads would cost more than they save.
     const uint32_t ze = a.zt[i2 * mw + jw];
     const uint32_t lz = lo16(ze), hz = hi16(ze);
     const uint32_t nz = (lz <= hz) ? hz - lz + 1 : n2 - lz + hz + 1;
     const uint32_t kslot = a.kidx[nz];
+    const uint32_t it = fc->iter;
+    const bool incremental = it > 0 && a.stats[kStatsCols * it] * kIncrementalRows <= g.rows;
+    const bword* cur = a.dzw + (it & 1) * a.dzw_half;
+    const bword* prv = a.dzw + ((it + 1) & 1) * a.dzw_half;
+    int lost = 0;
     for (uint32_t e = tid; e < nrep * nw; e += bd) {
         const uint32_t r = fdiv(e, g.magic_nw), rem = e - r * nw;
-        const uint32_t y = rem / W, wd = rem - y * W;
         const uint32_t we = a.wt[i3 * ma + reps[r]];
         const uint32_t lw = lo16(we), nwb = hi16(we) - lw + 1;
-        const uint64_t off = static_cast<uint64_t>(kslot * a.nl + a.lidx[nwb]) * pos +
-                             (y + n1 * (lz + n2 * lw)) * W + wd;
-        Eall[r * nw * nv + rem] = __ldg(a.dzw + off);
+        const uint32_t off = (kslot * a.nl + a.lidx[nwb]) * pos + n1 * (lz + n2 * lw) * W + rem;
+        const bword c = __ldg(cur + off);
+        Eall[r * nw * nv + rem] = c;
+        if (incremental && (__ldg(prv + off) & ~c)) {
+            rowchg[r * n1 + rem / W] = 1;
+            lost = 1;
+        }
         if (NV) Eall[r * nw * nv + nw + rem] = __ldg(a.vzw + off);
     }
+    if (incremental && !__syncthreads_or(lost)) return;
+    if (tid == 0) atomicAdd(a.stats + kStatsCols * (it + 1) + 3, static_cast<unsigned long long>(nrep));
     for (uint32_t r = tid >> 5; r < nrep; r += bd >> 5) {
         const uint64_t pl = pcol + reps[r];
         for (uint32_t e = lane; e < cw; e += 32) cls[r * cw + e] = __ldg(a.xcls + pl * cw + e);
@@ -216,6 +238,11 @@ __device__ __forceinline__ void sat_col_task(const GridInfo& g, const FusedFixAr
             anyc |= cm[w];
         }
         const uint32_t ye = yts[r * n1 + i1];
+        if (anyc && ye != kReject && incremental) {
+            uint32_t ch = 0;
+            for (uint32_t y = lo16(ye); y <= hi16(ye); ++y) ch |= rowchg[r * n1 + y];
+            if (!ch) anyc = 0;
+        }
         if (anyc && ye != kReject) {
 #pragma unroll
             for (int w = 0; w < WMAX; ++w) ntest += __popc(cm[w]);
