@@ -653,7 +653,9 @@ int problem_stage2(gsc_problem* p) {
     GSC_TRY(palloc(p, &p->hit, words));
     GSC_TRY(palloc(p, &p->best, g.S));
     const uint64_t combos = static_cast<uint64_t>(p->dil.nk) * p->dil.nl;
-    GSC_TRY(palloc(p, &p->dzw, 2 * combos * words));
+    GSC_TRY(palloc(p, &p->dzw, combos * words));
+    p->rl_words = static_cast<uint32_t>(g.rows / 32 + 2);
+    GSC_TRY(palloc(p, &p->rowlost, 2ull * p->rl_words));
     GSC_CU(ctx, launch_pack_bits(g, 0, p->valid, nullptr, p->validb, st));
     GSC_CU(ctx, launch_pack_bits(g, 0, p->cand, nullptr, p->candb, st));
     if (!p->safe) {
@@ -668,7 +670,7 @@ int problem_stage2(gsc_problem* p) {
     }
     if (p->need_valid) {
         GSC_TRY(palloc(p, &p->vzw, combos * words));
-        GSC_CU(ctx, launch_dilate(g, p->validb, p->vzw, 0, p->dil, nullptr, st));
+        GSC_CU(ctx, launch_dilate(g, p->validb, p->vzw, p->dil, nullptr, nullptr, 0, st));
     }
     return GSC_OK;
 }
@@ -724,7 +726,8 @@ FusedFixArgs fused_args(const gsc_problem* p, cudaGraphConditionalHandle cond, i
     a.cls_words = class_words(p->g);
     a.max_reps = p->max_reps;
     a.dzw = p->dzw;
-    a.dzw_half = static_cast<uint64_t>(p->dil.nk) * p->dil.nl * p->g.rows * p->g.W;
+    a.rowlost = p->rowlost;
+    a.rl_words = p->rl_words;
     a.vzw = p->vzw;
     a.kidx = p->kidx;
     a.lidx = p->lidx;

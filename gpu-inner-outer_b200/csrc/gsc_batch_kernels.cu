@@ -56,10 +56,17 @@ __global__ void __launch_bounds__(256) k_batch_dilate(const InstanceDesc* __rest
         const uint32_t k = find_task(wl.dil_off, wl.n, t);
         const InstanceDesc& d = descs[wl.slot[k]];
         if (d.a.fc->stop) continue;
-        bword* out = d.a.dzw + (d.a.fc->iter & 1) * d.a.dzw_half;
+        const uint32_t c = d.a.fc->iter;
+        const uint32_t* lost = c > 0 ? d.a.rowlost + (c & 1) * d.a.rl_words : nullptr;
+        uint32_t* next = d.a.rowlost + ((c + 1) & 1) * d.a.rl_words;
         const uint32_t b = (t - wl.dil_off[k]) * wl.chunk;
         const uint32_t end = min(b + wl.chunk, d.words);
-        for (uint32_t p = b + threadIdx.x; p < end; p += blockDim.x) dilate_position(d.g, d.a.dp, out, d.a.dil, p);
+        // The last task also clears row-bit words beyond the positions.
+        const uint32_t span = end == d.words ? max(end, d.a.rl_words) : end;
+        for (uint32_t p = b + threadIdx.x; p < span; p += blockDim.x) {
+            if (p < d.a.rl_words) next[p] = 0;
+            if (p < end) dilate_position(d.g, d.a.dp, d.a.dzw, d.a.dil, p, lost);
+        }
     }
 }
 

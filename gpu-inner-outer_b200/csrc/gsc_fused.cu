@@ -46,13 +46,18 @@ __global__ void k_fused_init(GridInfo g, FusedFixArgs a, const uint8_t* __restri
 
 // (theta, v)-dilated copies of a bit-sliced set, one thread per word
 // position (dilate_position).
-__global__ void k_dilate(GridInfo g, const bword* __restrict__ src, bword* __restrict__ dst, uint64_t half,
-                         DilateArgs d, const FixControl* fc) {
+__global__ void k_dilate(GridInfo g, const bword* __restrict__ src, bword* __restrict__ dst, DilateArgs d,
+                         const FixControl* fc, uint32_t* rowlost, uint32_t rl_words) {
     if (fc && fc->stop) return;
-    bword* out = dst + (fc ? (fc->iter & 1) * half : 0);
+    const uint32_t c = fc ? fc->iter : 0;
+    const uint32_t* lost = (rowlost && c > 0) ? rowlost + (c & 1) * rl_words : nullptr;
+    uint32_t* next = rowlost ? rowlost + ((c + 1) & 1) * rl_words : nullptr;
     const uint32_t pos = static_cast<uint32_t>(g.rows * g.W);
-    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < pos; p += gridDim.x * blockDim.x)
-        dilate_position(g, src, out, d, p);
+    const uint32_t span = next ? max(pos, rl_words) : pos;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < span; p += gridDim.x * blockDim.x) {
+        if (next && p < rl_words) next[p] = 0;
+        if (p < pos) dilate_position(g, src, dst, d, p, lost);
+    }
 }
 
 // The set-up plan (one block): which theta widths (wrapped lengths of the
@@ -202,9 +207,9 @@ size_t fused_smem_bytes(const GridInfo& g, uint32_t cls_words, int need_valid, u
     const size_t nw = static_cast<size_t>(g.n[1]) * g.W;
     const size_t nv = need_valid ? 2 : 1;
     const size_t mr = max_reps;
-    // act, E rows (D' and valid), sat, class records, y tables, representatives, changed-row bytes
+    // act, E rows (D' and valid), sat, class records, y tables, representatives, changed-row masks
     const size_t words = nw + mr * nw * nv + mr * nw + mr * cls_words + mr * g.n[1] + static_cast<size_t>(g.ma) +
-                         (mr * g.n[1] + 3) / 4;
+                         mr * ((g.n[1] + 31) / 32);
     return sizeof(bword) * words;
 }
 
@@ -216,12 +221,12 @@ cudaError_t launch_plan(const GridInfo& g, const uint32_t* zt, const uint32_t* w
     return cudaGetLastError();
 }
 
-cudaError_t launch_dilate(const GridInfo& g, const bword* src, bword* dst, uint64_t half, const DilateArgs& d,
-                          const FixControl* fc, cudaStream_t st) {
+cudaError_t launch_dilate(const GridInfo& g, const bword* src, bword* dst, const DilateArgs& d, const FixControl* fc,
+                          uint32_t* rowlost, uint32_t rl_words, cudaStream_t st) {
     const uint64_t pos = g.rows * g.W;
     uint64_t b = (pos + 255) / 256;
     if (b > 8192) b = 8192;
-    k_dilate<<<static_cast<unsigned int>(b ? b : 1), 256, 0, st>>>(g, src, dst, half, d, fc);
+    k_dilate<<<static_cast<unsigned int>(b ? b : 1), 256, 0, st>>>(g, src, dst, d, fc, rowlost, rl_words);
     return cudaGetLastError();
 }
 
@@ -233,7 +238,7 @@ cudaError_t launch_fused_init(const GridInfo& g, const FusedFixArgs& a, const ui
 cudaError_t launch_fused_iteration(const GridInfo& g, const FusedFixArgs& a, cudaStream_t st, uint32_t* launches,
                                    cudaEvent_t* ev) {
     if (ev) cudaEventRecord(ev[0], st);
-    cudaError_t derr = launch_dilate(g, a.dp, a.dzw, a.dzw_half, a.dil, a.fc, st);
+    cudaError_t derr = launch_dilate(g, a.dp, a.dzw, a.dil, a.fc, a.rowlost, a.rl_words, st);
     if (derr != cudaSuccess) return derr;
     if (ev) cudaEventRecord(ev[1], st);
     const size_t sm = fused_smem_bytes(g, a.cls_words, a.need_valid, a.max_reps);

@@ -80,8 +80,11 @@ __device__ __forceinline__ void init_control(FixControl* fc, uint32_t max_iterat
 // = OR of src over theta cells z .. z+k-1 (wrapped) and v cells v .. v+l-1
 // (entries whose v window leaves the grid are never read and are left 0).
 // The theta ORs are extended incrementally.
+// With `lost` (the rows that lost a D' cell since the last dilation) the
+// position is left as it is when no row of its widest window did.
 __device__ __forceinline__ void dilate_position(const GridInfo& g, const bword* __restrict__ src,
-                                                bword* __restrict__ dst, const DilateArgs& d, uint32_t p) {
+                                                bword* __restrict__ dst, const DilateArgs& d, uint32_t p,
+                                                const uint32_t* __restrict__ lost) {
     const uint32_t n1 = g.n[1], n2 = g.n[2], n3 = g.n[3], W = g.W;
     const uint32_t pos = static_cast<uint32_t>(g.rows * W);
     const uint32_t kmax = d.kval[d.nk - 1];
@@ -90,6 +93,17 @@ __device__ __forceinline__ void dilate_position(const GridInfo& g, const bword* 
     const uint32_t y = r % n1, q = r / n1;
     const uint32_t z = q % n2, v = q / n2;
     const uint32_t lfit = min(lmax, n3 - v);   // v windows that stay inside the grid
+    if (lost) {
+        uint32_t hit = 0, zz = z;
+        for (uint32_t i = 0; i < kmax && !hit; ++i) {
+            for (uint32_t j = 0; j < lfit; ++j) {
+                const uint32_t rr = y + n1 * (zz + n2 * (v + j));
+                hit |= (lost[rr >> 5] >> (rr & 31)) & 1u;
+            }
+            zz = (zz + 1 == n2) ? 0 : zz + 1;
+        }
+        if (!hit) return;
+    }
     bword zor[kMaxDilate];
 #pragma unroll
     for (uint32_t j = 0; j < kMaxDilate; ++j) zor[j] = 0;
@@ -158,7 +172,8 @@ __device__ __forceinline__ void sat_col_task(const GridInfo& g, const FusedFixAr
     bword* cls = sat + mr * nw;                           // max_reps * cw
     uint32_t* yts = cls + mr * cw;                        // max_reps * n1
     uint32_t* reps = yts + mr * n1;                       // ma: acceleration of each representative slot
-    uint8_t* rowchg = reinterpret_cast<uint8_t*>(reps + ma);   // max_reps * n1: E row lost a bit
+    uint32_t* rowchg = reps + ma;                         // max_reps * W1: y rows of a window that lost a cell
+    const uint32_t W1 = (n1 + 31) / 32;
 
     const uint64_t pcol = (static_cast<uint64_t>(i2) * g.n[3] + i3) * g.M + static_cast<uint64_t>(ma) * jw;
     int any = 0;
@@ -167,7 +182,6 @@ __device__ __forceinline__ void sat_col_task(const GridInfo& g, const FusedFixAr
         act[e] = v;
         any |= (v != 0);
     }
-    for (uint32_t e = tid; e < (mr * n1 + 3) / 4; e += bd) reinterpret_cast<uint32_t*>(rowchg)[e] = 0;
     if (tid < 32) {
         // Representatives in increasing acceleration order (warp ballot).
         uint32_t n = 0;
@@ -184,39 +198,50 @@ __device__ __forceinline__ void sat_col_task(const GridInfo& g, const FusedFixAr
     const uint32_t nrep = *s_nrep;
     if (!any || nrep == 0) return;
 
-    // B. dilated D' rows at each representative's (theta, v) box corner.
     // After the first iteration, every active state failed every input in
     // the previous one, and D' only loses cells, so a state can newly pass
-    // only where its box lost a D' cell: where the previous iteration's
-    // dilated row had a bit that this one has not.  When the previous
-    // iteration added few states (at most one per kIncrementalRows x-rows;
-    // a new state touches the items of about that many rows), a block with
-    // no such bit, and a (representative, row) item whose y range has none,
-    // is skipped: its states still fail.  With more new states nearly every
-    // item is touched, and the extra loads would cost more than they save.
+    // only if its box holds a cell that left D' in the previous iteration.
+    // When that iteration added few states (at most one per
+    // kIncrementalRows x-rows; a new state touches the items of about that
+    // many rows), the rows that lost a cell (rowlost, from the finalize
+    // kernel) are gathered per representative over its (theta, v) window,
+    // and a block with none, or a (representative, row) item whose y range
+    // has none, is skipped: its states still fail.
     const uint32_t ze = a.zt[i2 * mw + jw];
     const uint32_t lz = lo16(ze), hz = hi16(ze);
     const uint32_t nz = (lz <= hz) ? hz - lz + 1 : n2 - lz + hz + 1;
     const uint32_t kslot = a.kidx[nz];
     const uint32_t it = fc->iter;
     const bool incremental = it > 0 && a.stats[kStatsCols * it] * kIncrementalRows <= g.rows;
-    const bword* cur = a.dzw + (it & 1) * a.dzw_half;
-    const bword* prv = a.dzw + ((it + 1) & 1) * a.dzw_half;
-    int lost = 0;
+    if (incremental) {
+        const uint32_t* rl = a.rowlost + (it & 1) * a.rl_words;
+        int lost = 0;
+        for (uint32_t e = tid; e < nrep * W1; e += bd) {
+            const uint32_t r = e / W1, yw = e - r * W1;
+            const uint32_t we = a.wt[i3 * ma + reps[r]];
+            uint32_t m = 0, z = lz;
+            for (uint32_t i = 0; i < nz; ++i) {
+                for (uint32_t v = lo16(we); v <= hi16(we); ++v) {
+                    const uint32_t bit = n1 * (z + n2 * v) + yw * 32;
+                    m |= __funnelshift_r(rl[bit >> 5], rl[(bit >> 5) + 1], bit & 31);
+                }
+                z = (z + 1 == n2) ? 0 : z + 1;
+            }
+            if (yw == W1 - 1 && (n1 & 31)) m &= (1u << (n1 & 31)) - 1;
+            rowchg[r * W1 + yw] = m;
+            lost |= m != 0;
+        }
+        if (!__syncthreads_or(lost)) return;
+    }
+    // B. dilated D' rows at each representative's (theta, v) box corner.
     for (uint32_t e = tid; e < nrep * nw; e += bd) {
         const uint32_t r = fdiv(e, g.magic_nw), rem = e - r * nw;
         const uint32_t we = a.wt[i3 * ma + reps[r]];
         const uint32_t lw = lo16(we), nwb = hi16(we) - lw + 1;
         const uint32_t off = (kslot * a.nl + a.lidx[nwb]) * pos + n1 * (lz + n2 * lw) * W + rem;
-        const bword c = __ldg(cur + off);
-        Eall[r * nw * nv + rem] = c;
-        if (incremental && (__ldg(prv + off) & ~c)) {
-            rowchg[r * n1 + rem / W] = 1;
-            lost = 1;
-        }
+        Eall[r * nw * nv + rem] = __ldg(a.dzw + off);
         if (NV) Eall[r * nw * nv + nw + rem] = __ldg(a.vzw + off);
     }
-    if (incremental && !__syncthreads_or(lost)) return;
     if (tid == 0) atomicAdd(a.stats + kStatsCols * (it + 1) + 3, static_cast<unsigned long long>(nrep));
     for (uint32_t r = tid >> 5; r < nrep; r += bd >> 5) {
         const uint64_t pl = pcol + reps[r];
@@ -240,8 +265,8 @@ __device__ __forceinline__ void sat_col_task(const GridInfo& g, const FusedFixAr
         const uint32_t ye = yts[r * n1 + i1];
         if (anyc && ye != kReject && incremental) {
             uint32_t ch = 0;
-            for (uint32_t y = lo16(ye); y <= hi16(ye); ++y) ch |= rowchg[r * n1 + y];
-            if (!ch) anyc = 0;
+            for (uint32_t y = lo16(ye); y <= hi16(ye); ++y) ch |= rowchg[r * W1 + (y >> 5)] >> (y & 31);
+            if (!(ch & 1u)) anyc = 0;
         }
         if (anyc && ye != kReject) {
 #pragma unroll
@@ -344,7 +369,12 @@ __device__ __forceinline__ void finalize_word(const GridInfo& g, const FusedFixA
     const bword h = a.hit[e];
     const bword rn = rp | h;
     rnext[e] = rn;
-    a.dp[e] = (a.validb[e] & ~rn) | a.unsafeb[e];
+    const bword dn = (a.validb[e] & ~rn) | a.unsafeb[e];
+    if (a.dp[e] & ~dn) {   // the row lost a D' cell in iteration `it`
+        const uint32_t r = static_cast<uint32_t>(e / g.W);
+        atomicOr(a.rowlost + (it & 1) * a.rl_words + (r >> 5), 1u << (r & 31));
+    }
+    a.dp[e] = dn;
     if (h) {
         a.hit[e] = 0;
         a.active[e] &= ~h;

@@ -112,6 +112,8 @@ struct gsc_problem {
     uint8_t* xrep = nullptr;
     uint32_t max_reps = 0;
     gsc_b200::bword *dzw = nullptr, *vzw = nullptr;
+    uint32_t* rowlost = nullptr;
+    uint32_t rl_words = 0;
     uint8_t *kidx = nullptr, *lidx = nullptr;
     gsc_b200::DilateArgs dil{};
     int need_valid = 0;

@@ -141,9 +141,10 @@ struct FusedFixArgs {
     const uint8_t* xrep;       // per plane: the first acceleration of its omega column with identical boxes
     uint32_t cls_words;        // 32-bit words per class record
     uint32_t max_reps;         // max representative accelerations of one omega column
-    bword* dzw;                // (theta, v)-dilated D' [2][combo][rows * W]: half (iter & 1) is rebuilt
-                               // each iteration, the other half keeps the previous iteration's
-    uint64_t dzw_half;         // words of one half
+    bword* dzw;                // (theta, v)-dilated D' [combo][rows * W], brought up to date each iteration
+    uint32_t* rowlost;         // [2][rl_words] bit per x-row: the row lost a D' cell in the iteration
+                               // (iter & 1) just finalised
+    uint32_t rl_words;         // rows / 32 + 2
     const bword* vzw;          // (theta, v)-dilated valid set (when validity is more than safety)
     const uint8_t* kidx;       // [n2 + 1]: theta width -> its slot in dil.kval
     const uint8_t* lidx;       // [n3 + 1]: v width -> its slot in dil.lval
@@ -157,9 +158,12 @@ constexpr int kClassMax = 6;
 constexpr size_t kFusedSmemMax = 200 * 1024;
 // Dynamic shared memory of the fused satisfaction kernel.
 size_t fused_smem_bytes(const GridInfo& g, uint32_t cls_words, int need_valid, uint32_t max_reps);
-// Writes the dilated copies of src to dst + (fc ? (fc->iter & 1) * half : 0).
-cudaError_t launch_dilate(const GridInfo& g, const bword* src, bword* dst, uint64_t half, const DilateArgs& d,
-                          const FixControl* fc, cudaStream_t st);
+// Dilated copies of src into dst.  With fc and rowlost (during a fixpoint,
+// after its first iteration) only positions whose window holds a row that
+// lost a D' cell are recomputed; it also clears the row bits the next
+// finalize writes.
+cudaError_t launch_dilate(const GridInfo& g, const bword* src, bword* dst, const DilateArgs& d, const FixControl* fc,
+                          uint32_t* rowlost, uint32_t rl_words, cudaStream_t st);
 // Fills a PlanRecord from the counts, flags and (when xrep is set) the
 // theta / v tables and plane representatives; writes kidx / lidx.
 cudaError_t launch_plan(const GridInfo& g, const uint32_t* zt, const uint32_t* wt, const uint8_t* xrep,
