@@ -47,7 +47,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(C.PRESETS) + ["batched", "served"], default="demo_scale")
+    ap.add_argument("--workload", choices=sorted(C.PRESETS) + ["batched", "served", "simulate"], default="demo_scale")
     ap.add_argument("--method", choices=["auto", "stored", "fused"], default="auto")
     ap.add_argument("--cpu-sample-states", type=int, default=160000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -59,6 +59,8 @@ def parse():
     ap.add_argument("--rates", type=str, default="0.5,0.75,0.9",
                     help="Poisson arrival rates as fractions of the measured saturation throughput")
     ap.add_argument("--serve-budget-gb", type=float, default=24.0)
+    ap.add_argument("--trajectories", type=int, default=1 << 20)
+    ap.add_argument("--sim-steps", type=int, default=40)
     ap.add_argument("--plain-queries", type=int, default=0,
                     help="queries timed through the plain API for the sequential baseline (0 = all)")
     return ap.parse_args()
@@ -315,8 +317,7 @@ def bench_batched(args):
         t0 = time.perf_counter()
         bb = G.Batch(ctx, cases, autotune=True)
         bb.solve(graph=True)
-        for i in range(len(cases)):
-            bb.read(i, out=outs[i])
+        bb.read_all(outs)
         bb.close()
         if k:
             e2e.append((time.perf_counter() - t0) * 1e3)
@@ -354,7 +355,8 @@ def bench_batched(args):
                    "l2": "flushed before every step (256 MiB write)"},
         "e2e": {"value": n / (e2e_ms * 1e-3), "unit": "instances/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
-                "note": "gsc_batch_create (abstractions + set-up) + graph solve + reads into pinned memory"},
+                "note": "gsc_batch_create (abstractions + set-up) + graph solve + gsc_batch_read_all into pinned "
+                        "memory + destroy"},
         "plain_sequential": {
             "e2e_instances_per_s": n / (plain_total * 1e-3), "e2e_ms_total": plain_total,
             "device_solve_ms_total": sum(plain_dev), "p50_ms": percentile(plain_ms, 50),
@@ -511,13 +513,85 @@ def bench_served(args):
     ctx.close()
 
 
+def bench_simulate(args):
+    """Closed-loop simulation of the published demo's controller
+    (postprocess_controller.py's workload, scaled out): `--trajectories`
+    seeded start states, `--sim-steps` sample periods of 32 Euler substeps.
+    value = trajectories/s of gsc_problem_simulate returning final states and
+    stop steps (start states in, summaries out, inside the timed call); e2e =
+    the same returning every visited state; cpu_baseline = the numpy port on
+    a bounded sample."""
+    import numpy as np
+    import torch
+    import gsc_b200 as G
+
+    sys.path.insert(0, ORACLE)
+    import sim_oracle as S
+
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    case = C.hyperbolic_demo_case()
+    ctx = G.Context(0)
+    absn = G.Abstraction(ctx, case)
+    prob = G.Problem(ctx, absn, case, G.METHOD_FUSED)
+    prob.solve(graph=True)
+    n, steps, K = args.trajectories, args.sim_steps, int(case["integration_substeps"])
+    rng = np.random.default_rng(args.seed)
+    x0 = rng.uniform([-1.8, -1.8, -3.1, 0.1], [1.8, 1.8, 3.1, 1.9], (n, 4))
+    for _ in range(args.warmup):
+        prob.simulate(x0[: 1 << 14], steps, 1, trajectories=False)
+    times = []
+    with ClockSampler(gpu_uuid(torch, dev)) as clocks:
+        for k in range(args.steps):
+            t0 = time.perf_counter()
+            r = prob.simulate(x0, steps, 1000 + k, trajectories=False)
+            times.append(time.perf_counter() - t0)
+    t = statistics.median(times)
+    substeps = int(r["steps_done"].astype(np.int64).sum()) * K
+    m = min(n, 1 << 16)
+    e2e = []
+    for k in range(3):
+        t0 = time.perf_counter()
+        prob.simulate(x0[:m], steps, 2000 + k, trajectories=True)
+        e2e.append(time.perf_counter() - t0)
+    te = statistics.median(e2e)
+    ctl = prob.read()["controller"]
+    shape, ishape = C.grid_shape(case)
+    ms = 512
+    t0 = time.perf_counter()
+    S.simulate(ctl, S.grid_of(case, shape, ishape), x0[:ms], steps, 3)
+    tc = time.perf_counter() - t0
+    line = {
+        "metric": "controller simulation trajectories/s", "value": n / t, "unit": "trajectories/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"simulate_hyperbolic_demo_{n}_trajectories_{steps}_periods",
+                   "trajectories": n, "periods": steps, "substeps_per_period": K,
+                   "substeps_simulated": substeps, "substeps_per_s": substeps / t,
+                   "mean_periods_before_stop": float(r["steps_done"].mean())},
+        "e2e": {"value": m / te, "unit": "trajectories/s", "h2d_bytes_per_step": 32 * m,
+                "d2h_bytes_per_step": m * (steps + 1) * 32 + 36 * m, "ms_per_step": te * 1e3,
+                "note": f"{m} trajectories with every visited state returned"},
+        "cpu_baseline": {"value": ms / tc, "unit": "trajectories/s", "cores": 1, "kind": "port",
+                         "sample": f"{ms} of the same start states through oracle/sim_oracle.py (numpy, vectorised)"},
+        # one k_simulate launch per device chunk of (256 MB / 68 B) trajectories
+        "gpu_launches": args.steps * -(-n // min(n, (256 << 20) // 68)),
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line))
+    prob.close()
+    absn.close()
+    ctx.close()
+
+
 def main():
     args = parse()
-    if args.workload in ("batched", "served") and args.impl != "reference":
-        (bench_batched if args.workload == "batched" else bench_served)(args)
+    if args.workload in ("batched", "served", "simulate") and args.impl != "reference":
+        {"batched": bench_batched, "served": bench_served, "simulate": bench_simulate}[args.workload](args)
         return
-    if args.workload in ("batched", "served"):
-        print(json.dumps({"impl": "reference", "unavailable": "the reference has no batched or served mode"}))
+    if args.workload in ("batched", "served", "simulate"):
+        print(json.dumps({"impl": "reference", "unavailable": "the reference has no batched, served or "
+                                                              "device simulation mode"}))
         return
     case = C.checked(C.PRESETS[args.workload]())
     if args.impl == "reference":

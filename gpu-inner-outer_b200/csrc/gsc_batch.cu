@@ -90,9 +90,9 @@ uint32_t wmax_of(uint32_t w) { return w <= 1 ? 1 : w == 2 ? 2 : w <= 4 ? 4 : 8; 
 
 struct gsc_batch {
     gsc_context* ctx = nullptr;
-    // Declaration order is destruction order reversed: problems, then
-    // abstractions, release into the pool before the pool frees its regions.
-    std::unique_ptr<DevicePool> pool;
+    DevicePool* pool = nullptr;   // the context's caching pool
+    std::vector<std::pair<void*, uint64_t>> own;   // instance table and work list
+    uint64_t own_bytes = 0;
     std::vector<std::unique_ptr<gsc_abstraction>> abs;
     std::vector<std::unique_ptr<gsc_problem>> probs;
     PlanRecord* hplans = nullptr;   // pinned
@@ -116,6 +116,7 @@ struct gsc_batch {
         if (graph) cudaGraphDestroy(graph);
         probs.clear();
         abs.clear();
+        device_release_all(ctx, pool, own, own_bytes);
         if (hplans) cudaFreeHost(hplans);
         if (hrunning) cudaFreeHost(hrunning);
     }
@@ -255,7 +256,7 @@ int batch_create(gsc_batch* b, uint32_t count, const gsc_model_desc* models, con
                  const gsc_batch_options* opt) {
     gsc_context* ctx = b->ctx;
     cudaStream_t st = ctx->stream;
-    b->pool.reset(new DevicePool(ctx, 256ull << 20, 0));
+    b->pool = ctx->pool.get();
     GSC_CU(ctx, cudaMallocHost(&b->hplans, sizeof(PlanRecord) * count));
     GSC_CU(ctx, cudaMallocHost(&b->hrunning, sizeof(uint32_t)));
     std::vector<std::vector<std::pair<void*, uint64_t>>> tmp(count);
@@ -265,7 +266,7 @@ int batch_create(gsc_batch* b, uint32_t count, const gsc_model_desc* models, con
         if (!a) return GSC_ERR_OUT_OF_MEMORY;
         a->ctx = ctx;
         a->model = models[i];
-        a->pool = b->pool.get();
+        a->pool = b->pool;
         std::string err;
         const int s = grid_from_model(&models[i], &a->g, &err);
         if (s != GSC_OK) return fail(ctx, s, "instance " + std::to_string(i) + ": " + err);
@@ -280,7 +281,7 @@ int batch_create(gsc_batch* b, uint32_t count, const gsc_model_desc* models, con
         p->ctx = ctx;
         p->abs = b->abs[i].get();
         p->g = b->abs[i]->g;
-        p->pool = b->pool.get();
+        p->pool = b->pool;
         p->stream = st;
         p->method = GSC_METHOD_FUSED;
         p->hplan = b->hplans + i;
@@ -291,7 +292,7 @@ int batch_create(gsc_batch* b, uint32_t count, const gsc_model_desc* models, con
     GSC_CU(ctx, cudaStreamSynchronize(st));
     for (uint32_t i = 0; i < count; ++i) {
         uint64_t tb = 0;
-        device_release_all(ctx, b->pool.get(), tmp[i], tb);
+        device_release_all(ctx, b->pool, tmp[i], tb);
     }
     for (uint32_t i = 0; i < count; ++i) {
         gsc_problem* p = b->probs[i].get();
@@ -314,13 +315,11 @@ int batch_create(gsc_batch* b, uint32_t count, const gsc_model_desc* models, con
     b->smem = smem;
     if (smem > kFusedSmemMax) return fail(ctx, GSC_ERR_UNSUPPORTED, "batch: an instance needs too much shared memory");
     void* q = nullptr;
-    uint64_t own = 0;
-    std::vector<std::pair<void*, uint64_t>> bufs;
-    GSC_TRY(device_alloc(ctx, b->pool.get(), bufs, own, &q, sizeof(InstanceDesc) * count));
+    GSC_TRY(device_alloc(ctx, b->pool, b->own, b->own_bytes, &q, sizeof(InstanceDesc) * count));
     b->ddesc = static_cast<InstanceDesc*>(q);
-    GSC_TRY(device_alloc(ctx, b->pool.get(), bufs, own, &q, 4ull * (count + 4ull * (count + 1))));
+    GSC_TRY(device_alloc(ctx, b->pool, b->own, b->own_bytes, &q, 4ull * (count + 4ull * (count + 1))));
     b->dlist = static_cast<uint32_t*>(q);
-    GSC_TRY(device_alloc(ctx, b->pool.get(), bufs, own, &q, 4));
+    GSC_TRY(device_alloc(ctx, b->pool, b->own, b->own_bytes, &q, 4));
     b->drunning = static_cast<uint32_t*>(q);
     GSC_CU(ctx, cudaMemcpyAsync(b->ddesc, hd.data(), sizeof(InstanceDesc) * count, cudaMemcpyHostToDevice, st));
 
@@ -460,8 +459,72 @@ int gsc_batch_timings(gsc_batch* b, gsc_batch_report* out) {
     const int sms = sm_count(ctx);
     b->t.sat_blocks_per_sm = b->shape.sat_blocks / static_cast<uint32_t>(sms);
     b->t.chunk_words = b->shape.chunk;
-    b->t.device_bytes = b->pool ? b->pool->total : 0;
+    uint64_t held = b->own_bytes;
+    for (const auto& a : b->abs) held += a->bytes;
+    for (const auto& p : b->probs) held += p->bytes;
+    b->t.device_bytes = held;
     *out = b->t;
+    return GSC_OK;
+}
+
+int gsc_batch_read_all(gsc_batch* b, gsc_result* out) {
+    if (!b || !out) return GSC_ERR_INVALID_ARGUMENT;
+    gsc_context* ctx = b->ctx;
+    cudaGetLastError();
+    GSC_CU(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    const size_t n = b->probs.size();
+    // Control records first (the reachable set's buffer depends on the
+    // iteration count), then every copy, with one wait each.
+    std::vector<FixControl> fc(n);
+    for (size_t i = 0; i < n; ++i)
+        GSC_CU(ctx, cudaMemcpyAsync(&fc[i], b->probs[i]->fc, sizeof(FixControl), cudaMemcpyDeviceToHost, st));
+    GSC_CU(ctx, cudaStreamSynchronize(st));
+    std::vector<std::vector<unsigned long long>> hs(n);
+    for (size_t i = 0; i < n; ++i) {
+        gsc_problem* p = b->probs[i].get();
+        const GridInfo& g = p->g;
+        gsc_result* r = out + i;
+        if (r->valid_mask) GSC_CU(ctx, cudaMemcpyAsync(r->valid_mask, p->valid, g.S, cudaMemcpyDeviceToHost, st));
+        if (r->candidate_mask)
+            GSC_CU(ctx, cudaMemcpyAsync(r->candidate_mask, p->cand, g.S, cudaMemcpyDeviceToHost, st));
+        if (r->reachable_mask) {
+            GSC_CU(ctx, launch_unpack_bits(g, (fc[i].iter & 1) ? p->reach1 : p->reach0, p->reach8, st));
+            GSC_CU(ctx, cudaMemcpyAsync(r->reachable_mask, p->reach8, g.S, cudaMemcpyDeviceToHost, st));
+        }
+        if (r->controller)
+            GSC_CU(ctx, cudaMemcpyAsync(r->controller, p->controller, g.S * 4, cudaMemcpyDeviceToHost, st));
+        if (r->reach_step)
+            GSC_CU(ctx, cudaMemcpyAsync(r->reach_step, p->reach_step, g.S * 4, cudaMemcpyDeviceToHost, st));
+        const uint32_t rows = std::min<uint32_t>(fc[i].iter, r->iter_capacity);
+        if (rows && (r->iter_new_reachable || r->iter_new_certified)) {
+            hs[i].resize(static_cast<size_t>(kStatsCols) * (rows + 1));
+            GSC_CU(ctx, cudaMemcpyAsync(hs[i].data(), p->stats, hs[i].size() * 8, cudaMemcpyDeviceToHost, st));
+        }
+    }
+    GSC_CU(ctx, cudaStreamSynchronize(st));
+    for (size_t i = 0; i < n; ++i) {
+        const GridInfo& g = b->probs[i]->g;
+        gsc_result* r = out + i;
+        for (int d = 0; d < 4; ++d) r->shape[d] = g.n[d];
+        r->input_shape[0] = g.ma;
+        r->input_shape[1] = g.mw;
+        r->states = g.S;
+        r->inputs = g.M;
+        r->pairs = g.S * g.M;
+        r->iterations = fc[i].iter;
+        r->converged = static_cast<int32_t>(fc[i].converged);
+        r->message = static_cast<int32_t>(fc[i].message ? fc[i].message : GSC_MSG_MAX_ITERATIONS);
+        r->certified_candidates = fc[i].certified;
+        r->reachable_states = fc[i].reachable;
+        r->candidate_count = fc[i].candidate_count;
+        r->valid_count = fc[i].valid_count;
+        const uint32_t rows = hs[i].empty() ? 0 : static_cast<uint32_t>(hs[i].size() / kStatsCols - 1);
+        for (uint32_t k = 0; k < rows; ++k) {
+            if (r->iter_new_reachable) r->iter_new_reachable[k] = hs[i][kStatsCols * (k + 1)];
+            if (r->iter_new_certified) r->iter_new_certified[k] = hs[i][kStatsCols * (k + 1) + 1];
+        }
+    }
     return GSC_OK;
 }
 

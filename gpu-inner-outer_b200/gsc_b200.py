@@ -143,6 +143,7 @@ SIGNATURES = {
                                         ctypes.POINTER(BatchOptions), ctypes.POINTER(_P)]),
     "gsc_batch_solve": (ctypes.c_int, [_P, ctypes.c_uint32]),
     "gsc_batch_read": (ctypes.c_int, [_P, ctypes.c_uint32, ctypes.POINTER(Result)]),
+    "gsc_batch_read_all": (ctypes.c_int, [_P, ctypes.POINTER(Result)]),
     "gsc_batch_timings": (ctypes.c_int, [_P, ctypes.POINTER(BatchReport)]),
     "gsc_batch_destroy": (None, [_P]),
     "gsc_server_create": (ctypes.c_int, [_P, ctypes.POINTER(ServerOptions), ctypes.POINTER(_P)]),
@@ -319,6 +320,7 @@ class Problem:
         self.abs = abs_
         self._h = ctypes.c_void_p()
         self.query = _Query(case, **masks)
+        self.states = int(np.prod(grid_shape(case)[0], dtype=np.uint64))
         ctx.check(lib().gsc_problem_create(ctx._h, abs_._h, ctypes.byref(self.query.desc), int(method),
                                            ctypes.byref(self._h)))
         ctx._children.add(self)
@@ -333,7 +335,8 @@ class Problem:
         return {k: getattr(t, k) for k, _ in Timings._fields_}
 
     def read(self, iter_capacity=4096, masks=True, out=None) -> dict:
-        return _read_result(lambda r: lib().gsc_problem_read(self._h, r), self.ctx, iter_capacity, masks, out)
+        return _read_result(lambda r: lib().gsc_problem_read(self._h, r), self.ctx, iter_capacity, masks, out,
+                            self.states)
 
     def simulate(self, x0, steps, seed, trajectories=True) -> dict:
         """Closed-loop trajectories under the solved controller from each row
@@ -373,14 +376,16 @@ class Problem:
             pass
 
 
-def _read_result(call, ctx, iter_capacity=4096, masks=True, out=None) -> dict:
-    """Run a gsc_*_read call twice (shape probe, then the arrays) and return
-    the result as a dict of numpy arrays and scalars.  ``out`` may supply the
-    five arrays (e.g. views of pinned host memory)."""
+def _read_result(call, ctx, iter_capacity=4096, masks=True, out=None, states=None) -> dict:
+    """Run a gsc_*_read call (after a shape probe when the state count is not
+    given) and return the result as a dict of numpy arrays and scalars.
+    ``out`` may supply the five arrays (e.g. views of pinned host memory)."""
     r = Result()
-    probe = Result()
-    ctx.check(call(ctypes.byref(probe)))
-    S = int(probe.states)
+    if states is None:
+        probe = Result()
+        ctx.check(call(ctypes.byref(probe)))
+        states = int(probe.states)
+    S = int(states)
     if out is not None:
         out = dict(out)
         for k, v in out.items():
@@ -403,6 +408,10 @@ def _read_result(call, ctx, iter_capacity=4096, masks=True, out=None) -> dict:
     r.iter_new_certified = _ptr(nc)
     r.iter_capacity = iter_capacity
     ctx.check(call(ctypes.byref(r)))
+    return _result_dict(r, out, nr, nc, iter_capacity)
+
+
+def _result_dict(r, out, nr, nc, iter_capacity):
     it = int(r.iterations)
     out.update({
         "shape": tuple(r.shape), "input_shape": tuple(r.input_shape), "states": int(r.states),
@@ -432,6 +441,7 @@ class Batch:
         ctx.check(lib().gsc_batch_create(ctx._h, n, self.models, self.qdescs, ctypes.byref(opt),
                                          ctypes.byref(self._h)))
         self.count = n
+        self.states = [int(np.prod(grid_shape(c)[0], dtype=np.uint64)) for c in cases]
         ctx._children.add(self)
 
     def solve(self, graph=True):
@@ -439,7 +449,32 @@ class Batch:
 
     def read(self, index, iter_capacity=4096, masks=True, out=None) -> dict:
         return _read_result(lambda r: lib().gsc_batch_read(self._h, int(index), r), self.ctx, iter_capacity, masks,
-                            out)
+                            out, self.states[int(index)])
+
+    def read_all(self, outs=None, iter_capacity=4096) -> list:
+        """Every instance with one batched read (gsc_batch_read_all); ``outs``
+        may supply each instance's five arrays."""
+        n = self.count
+        rs = (Result * n)()
+        keep = []
+        for i in range(n):
+            S = self.states[i]
+            o = dict(outs[i]) if outs is not None else {
+                "valid_mask": np.zeros(S, np.uint8), "candidate_mask": np.zeros(S, np.uint8),
+                "reachable_mask": np.zeros(S, np.uint8), "controller": np.zeros(S, np.uint32),
+                "reach_step": np.zeros(S, np.uint32)}
+            for k, v in o.items():
+                if v.size != S or not v.flags["C_CONTIGUOUS"]:
+                    raise ValueError(f"outs[{i}][{k}] must be a contiguous array of {S} elements")
+                setattr(rs[i], k, _ptr(v))
+            nr = np.zeros(iter_capacity, np.uint64)
+            nc = np.zeros(iter_capacity, np.uint64)
+            rs[i].iter_new_reachable = _ptr(nr)
+            rs[i].iter_new_certified = _ptr(nc)
+            rs[i].iter_capacity = iter_capacity
+            keep.append((o, nr, nc))
+        self.ctx.check(lib().gsc_batch_read_all(self._h, rs))
+        return [_result_dict(rs[i], keep[i][0], keep[i][1], keep[i][2], iter_capacity) for i in range(n)]
 
     def report(self) -> dict:
         t = BatchReport()

@@ -1,13 +1,16 @@
-// main.cpp -- gsc_b200_cli: the reference CLI's --gpu mode (src/main.cpp:125-218)
-// over libgsc_b200.
+// main.cpp -- gsc_b200_cli: the reference CLI (src/main.cpp:125-218) over
+// libgsc_b200.
 //
-//   gsc_b200_cli <config.cfg> [--gpu] [--method auto|stored|fused] [--no-graph]
-//                [--output DIR] [--print-config]
+//   gsc_b200_cli <config.cfg> [--gpu|--compare] [--method auto|stored|fused]
+//                [--no-graph] [--output DIR] [--print-config]
 //
 // The summary lines keep the reference's labels (main.cpp:12-38).  --output
 // writes the result arrays as raw little-endian files plus summary.json (the
 // HDF5 layout of result_io.cpp needs libhdf5, which this build does not link).
-// There is no CPU method in the product: --cpu and --compare are refused.
+// There is no CPU method in the product, so --cpu is refused; --compare keeps
+// the reference's exit codes (0 = every output array equal, 3 = a difference,
+// 2 = no GPU run, main.cpp:189-211) but compares the two device methods: the
+// reference's own 16-corner count (stored) against the fused method.
 #include <sys/stat.h>
 
 #include <cstdio>
@@ -95,11 +98,11 @@ void write_results(const std::string& dir, const gsc::CaseConfig& cfg, const gsc
     js << "]}\n";
 }
 
-void print_summary(const gsc::GpuRunReport& g) {
+void print_summary(const gsc::GpuRunReport& g, const char* label = "gpu") {
     std::uint64_t candidates = 0;
     for (auto v : g.result.candidate_mask) candidates += (v != 0);
     const auto& r = g.result;
-    std::cout << "\n[gpu]\n";
+    std::cout << "\n[" << label << "]\n";
     std::cout << "states        : " << g.state_grid.total_size << '\n';
     std::cout << "inputs        : " << g.input_grid.total_size << '\n';
     std::cout << "pairs         : " << g.pair_count << '\n';
@@ -121,8 +124,8 @@ void print_summary(const gsc::GpuRunReport& g) {
 
 int main(int argc, char** argv) {
     if (argc < 2) {
-        std::cerr << "usage: gsc_b200_cli <config.cfg> [--gpu] [--method auto|stored|fused] [--no-graph] "
-                     "[--output DIR] [--print-config]\n";
+        std::cerr << "usage: gsc_b200_cli <config.cfg> [--gpu|--compare] [--method auto|stored|fused] "
+                     "[--no-graph] [--output DIR] [--print-config]\n";
         return 1;
     }
     try {
@@ -130,11 +133,16 @@ int main(int argc, char** argv) {
         gsc::RunOptions opt;
         std::string output;
         bool print_only = false;
+        bool compare = false;
         for (int i = 2; i < argc; ++i) {
             const std::string a = argv[i];
             if (a == "--gpu") continue;
-            if (a == "--cpu" || a == "--compare") {
-                std::cerr << "error: " << a << " needs the CPU method, which this library does not ship\n";
+            if (a == "--compare") {
+                compare = true;
+                continue;
+            }
+            if (a == "--cpu") {
+                std::cerr << "error: --cpu needs the CPU method, which this library does not ship\n";
                 return 2;
             }
             if (a == "--no-graph") {
@@ -154,6 +162,28 @@ int main(int argc, char** argv) {
         if (print_only) {
             print_config(cfg);
             return 0;
+        }
+        if (compare) {   // main.cpp:189-211, the two device methods
+            gsc::RunOptions so = opt, fo = opt;
+            so.method = GSC_METHOD_STORED;
+            fo.method = GSC_METHOD_FUSED;
+            const gsc::GpuRunReport s = gsc::run_case_cuda_u32(cfg, so);
+            const gsc::GpuRunReport f = s.executed ? gsc::run_case_cuda_u32(cfg, fo) : s;
+            if (!s.executed || !f.executed) {
+                std::cerr << "gpu compare unavailable: " << (s.executed ? f.message : s.message) << '\n';
+                return 2;
+            }
+            print_summary(s, "stored");
+            print_summary(f, "fused");
+            const auto& a = s.result;
+            const auto& b = f.result;
+            const bool same = a.valid_mask == b.valid_mask && a.candidate_mask == b.candidate_mask &&
+                              a.reachable_mask == b.reachable_mask && a.controller == b.controller &&
+                              a.reach_step == b.reach_step && a.iterations == b.iterations &&
+                              a.message == b.message;
+            if (!output.empty()) write_results(output, cfg, f);
+            std::cout << "exact_match   : " << (same ? "true" : "false") << '\n';
+            return same ? 0 : 3;
         }
         const gsc::GpuRunReport g = gsc::run_case_cuda_u32(cfg, opt);
         if (!g.executed) {   // main.cpp:168-171

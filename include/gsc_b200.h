@@ -301,8 +301,9 @@ int gsc_problem_simulate(gsc_problem* problem, uint32_t count, const double* x0,
  * together: every fixpoint iteration of every instance is one pass of four
  * kernels over all instances (persistent blocks walking a task list), and
  * with GSC_SOLVE_GRAPH the whole loop is one CUDA graph whose while-node
- * reads a device flag cleared when no instance is left running.  Each
- * instance's result is bit-identical to its own gsc_problem solve.  Fused
+ * reads a device flag cleared when no instance is left running.  Device
+ * memory comes from the context's caching pool.  Each instance's result is
+ * bit-identical to its own gsc_problem solve.  Fused
  * method only: an instance the fused method cannot take fails the create
  * with GSC_ERR_UNSUPPORTED and the instance index in gsc_last_error. */
 typedef struct gsc_batch gsc_batch;
@@ -337,6 +338,9 @@ int gsc_batch_create(gsc_context* ctx, uint32_t count, const gsc_model_desc* mod
 int gsc_batch_solve(gsc_batch* batch, uint32_t flags);
 /* Instance `index` of the last solve, as gsc_problem_read. */
 int gsc_batch_read(gsc_batch* batch, uint32_t index, gsc_result* out);
+/* Every instance at once (out: one gsc_result per instance, in creation
+ * order): all copies are queued, then one wait. */
+int gsc_batch_read_all(gsc_batch* batch, gsc_result* out);
 int gsc_batch_timings(gsc_batch* batch, gsc_batch_report* out);
 void gsc_batch_destroy(gsc_batch* batch);
 

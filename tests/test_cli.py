@@ -53,9 +53,17 @@ def test_parser_rejects_unknown_keys(tmp_path):
     assert r.returncode == 1 and "state_lb expects 4" in r.stderr
 
 
-def test_cpu_modes_are_refused():
-    r = subprocess.run([CLI, os.path.join(CFG, "hyperbolic_demo.cfg"), "--compare"], capture_output=True, text=True)
-    assert r.returncode == 2
+def test_cpu_mode_is_refused():
+    r = subprocess.run([CLI, os.path.join(CFG, "hyperbolic_demo.cfg"), "--cpu"], capture_output=True, text=True)
+    assert r.returncode == 2 and "CPU method" in r.stderr
+
+
+@pytest.mark.gpu
+def test_cli_compare_exit_code_contract():
+    """--compare: the reference's exit codes over the two device methods."""
+    r = subprocess.run([CLI, os.path.join(CFG, "unicycle_small.cfg"), "--compare"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    assert "exact_match   : true" in r.stdout and "[stored]" in r.stdout and "[fused]" in r.stdout
 
 
 def _read(d, name, dtype):

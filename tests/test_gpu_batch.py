@@ -44,12 +44,15 @@ def check_entry(got, name):
 @pytest.mark.parametrize("graph", [True, False], ids=["graph", "hostloop"])
 def test_batch_of_golden_cases(ctx, graph):
     """All golden cases (different grids, inputs, obstacles, wrap-around,
-    an empty candidate set, max_iterations 0) in one batch."""
+    an empty candidate set, max_iterations 0) in one batch, read one by one
+    and all at once."""
     names = sorted(INDEX)
     b = G.Batch(ctx, [INDEX[n]["case"] for n in names])
     b.solve(graph=graph)
     for i, n in enumerate(names):
         check_entry(b.read(i), n)
+    for n, got in zip(names, b.read_all()):
+        check_entry(got, n)
     rep = b.report()
     assert rep["instances"] == len(names)
     assert rep["max_iterations_run"] == max(INDEX[n]["iterations"] for n in names)
