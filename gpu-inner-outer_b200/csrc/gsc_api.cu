@@ -725,6 +725,7 @@ FusedFixArgs fused_args(const gsc_problem* p, cudaGraphConditionalHandle cond, i
     a.xrep = p->xrep;
     a.cls_words = class_words(p->g);
     a.max_reps = p->max_reps;
+    a.sat_threads = fused_sat_threads(p->g, p->max_reps);
     a.dzw = p->dzw;
     a.rowlost = p->rowlost;
     a.rl_words = p->rl_words;
@@ -831,6 +832,10 @@ int gsc_problem_create(gsc_context* ctx, const gsc_abstraction* abs, const gsc_q
     p->timings.abstraction_ms = abs->build_ms;
     p->timings.device_bytes = p->bytes;
     p->timings.method = p->method;
+    if (p->method == GSC_METHOD_FUSED) {
+        p->timings.max_reps = p->max_reps;
+        p->timings.sat_threads = fused_sat_threads(p->g, p->max_reps);
+    }
     *out = p.release();
     return GSC_OK;
 }

@@ -197,11 +197,16 @@ cudaError_t launch_sat_col_t(const GridInfo& g, const FusedFixArgs& a, size_t sm
         if (e != cudaSuccess) return e;
         if (dev >= 0 && dev < 64) configured[dev] = true;
     }
-    k_sat_col<W, NV><<<g.slices * g.mw, kFusedWarps * 32, sm, st>>>(g, a);
+    k_sat_col<W, NV><<<g.slices * g.mw, a.sat_threads, sm, st>>>(g, a);
     return cudaGetLastError();
 }
 
 }  // namespace
+
+uint32_t fused_sat_threads(const GridInfo& g, uint32_t max_reps) {
+    const uint64_t work = static_cast<uint64_t>(max_reps) * g.n[1] * g.W;
+    return work <= 1024 ? 64u : work <= 2304 ? 128u : 256u;
+}
 
 size_t fused_smem_bytes(const GridInfo& g, uint32_t cls_words, int need_valid, uint32_t max_reps) {
     const size_t nw = static_cast<size_t>(g.n[1]) * g.W;

@@ -141,6 +141,7 @@ struct FusedFixArgs {
     const uint8_t* xrep;       // per plane: the first acceleration of its omega column with identical boxes
     uint32_t cls_words;        // 32-bit words per class record
     uint32_t max_reps;         // max representative accelerations of one omega column
+    uint32_t sat_threads;      // threads per satisfaction block (64, 128 or 256)
     bword* dzw;                // (theta, v)-dilated D' [combo][rows * W], brought up to date each iteration
     uint32_t* rowlost;         // [2][rl_words] bit per x-row: the row lost a D' cell in the iteration
                                // (iter & 1) just finalised
@@ -153,11 +154,14 @@ struct FusedFixArgs {
     cudaGraphConditionalHandle cond;
     int use_cond;
 };
-constexpr int kFusedWarps = 4;
+constexpr int kFusedWarps = 8;   // most warps of a satisfaction block
 constexpr int kClassMax = 6;
 constexpr size_t kFusedSmemMax = 200 * 1024;
 // Dynamic shared memory of the fused satisfaction kernel.
 size_t fused_smem_bytes(const GridInfo& g, uint32_t cls_words, int need_valid, uint32_t max_reps);
+// Threads per satisfaction block for a problem: more when a block has more
+// representative rows to stage and test (max_reps * n1 * W words).
+uint32_t fused_sat_threads(const GridInfo& g, uint32_t max_reps);
 // Dilated copies of src into dst.  With fc and rowlost (during a fixpoint,
 // after its first iteration) only positions whose window holds a row that
 // lost a D' cell are recomputed; it also clears the row bits the next

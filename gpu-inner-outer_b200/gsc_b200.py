@@ -82,7 +82,7 @@ class Timings(ctypes.Structure):
         ("readback_ms", ctypes.c_double), ("device_bytes", ctypes.c_uint64), ("method", ctypes.c_uint32),
         ("kernel_launches", ctypes.c_uint32), ("iterations", ctypes.c_uint32), ("sat_launches", ctypes.c_uint32),
         ("sat_kernel_ms", ctypes.c_double), ("scan_kernel_ms", ctypes.c_double), ("pair_tests", ctypes.c_uint64),
-        ("aux_count", ctypes.c_uint64),
+        ("aux_count", ctypes.c_uint64), ("sat_threads", ctypes.c_uint32), ("max_reps", ctypes.c_uint32),
     ]
 
 

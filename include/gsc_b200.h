@@ -178,6 +178,9 @@ typedef struct {
     uint64_t aux_count;             /* stored: box counts evaluated; fused:
                                        (slice, representative input) planes
                                        staged, summed over iterations             */
+    uint32_t sat_threads;           /* fused: threads per satisfaction block      */
+    uint32_t max_reps;              /* fused: most representative accelerations
+                                       of one omega column                        */
 } gsc_timings;
 
 typedef struct gsc_context gsc_context;
