@@ -245,6 +245,24 @@ def gpu_uuid(torch, dev):
         return None
 
 
+def max_over_ranks(dist, values, device):
+    """Every rank's values replaced by their maximum over the ranks (one
+    all-reduce); unchanged without a process group."""
+    if not dist:
+        return [float(v) for v in values]
+    import torch
+
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
+def replica_value(world, units_per_rank, ms):
+    """Whole-job throughput of `world` replicas that each process
+    `units_per_rank` units in `ms` milliseconds (the slowest rank's time)."""
+    return world * units_per_rank / (ms * 1e-3)
+
+
 def pinned_outputs(torch, S):
     """The five result arrays of one problem as numpy views of pinned memory."""
     import numpy as np
@@ -655,13 +673,9 @@ def main():
     if dist:
         dist.barrier()
     step_ms = [a.elapsed_time(b) for a, b in evs]
-    total_ms = sum(step_ms)
-    if dist:
-        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(dist, [sum(step_ms)], dev)[0]
     ms_per_step = total_ms / args.steps
-    value = world * P * iters / (ms_per_step * 1e-3)
+    value = replica_value(world, P * iters, ms_per_step)
 
     # Dominant kernel: one profiled solve (events around each satisfaction launch).
     prob.solve(profile=True)
@@ -687,11 +701,7 @@ def main():
         torch.cuda.synchronize(dev)
         if k > 0:
             e2e_ms.append((time.perf_counter() - t0) * 1e3)
-    e2e_step = statistics.median(e2e_ms)
-    if dist:
-        t = torch.tensor([e2e_step], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_step = float(t.item())
+    e2e_step = max_over_ranks(dist, [statistics.median(e2e_ms)], dev)[0]
     K = case["integration_substeps"]
     h2d = 8 * (2 * shape[2] * ishape[1] * K + shape[3] * ishape[0] * K + shape[2] * ishape[1] +
                shape[3] * ishape[0]) + 64 * len(case.get("obstacles", []))
@@ -723,7 +733,7 @@ def main():
                      "kernel_ms_per_launch": per_launch_ms, "algorithmic_bytes_per_launch": alg,
                      "peak_kind": peak_kind},
         "cpu_baseline": cpu,
-        "e2e": {"value": world * P * r["iterations"] / (e2e_step * 1e-3), "unit": "pair-checks/s",
+        "e2e": {"value": replica_value(world, P * r["iterations"], e2e_step), "unit": "pair-checks/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_step},
         "gpu_launches": launches,
         "clocks": clocks.summary(),
