@@ -1,0 +1,105 @@
+"""Parity at the largest sizes, where the full CPU oracle is too slow:
+  * 128x128x72x48 states x 144 inputs (8.2 G pairs): after the GPU's
+    iteration k-1 (a solve capped at k-1 iterations), the oracle recomputes
+    iteration k for 10^5 seeded states plus every state the GPU changed in
+    iteration k (up to a cap), and must agree bit for bit with the GPU's
+    solve capped at k iterations;
+  * the fused method's widest rows (256 x-cells, 8 words) and the first width
+    it refuses (257 x-cells: the automatic method falls back to the stored
+    one), both against the full oracle."""
+import numpy as np
+import pytest
+
+import gsc_b200 as G
+import gsc_cases as C
+import oracle as O
+from helpers import assert_same_result
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = G.Context(0)
+    yield c
+    c.close()
+
+
+def capped(ctx, absn, case, k):
+    q = C.clone(case, max_iterations=k)
+    p = G.Problem(ctx, absn, q, G.METHOD_FUSED)
+    p.solve(graph=True)
+    r = p.read()
+    p.close()
+    return r
+
+
+@pytest.mark.timeout(600)
+def test_large_workload_spot_checked_per_iteration(ctx):
+    case = C.large_case()
+    absn = G.Abstraction(ctx, case)
+    full = capped(ctx, absn, case, case["max_iterations"])
+    assert full["iterations"] == 75 and full["message"] == "iteration stalled before candidate closure"
+    rng = np.random.default_rng(11)
+    S = full["states"]
+    for k in (1, 2, 20, 75):
+        a = capped(ctx, absn, case, k - 1)
+        b = capped(ctx, absn, case, k)
+        changed = np.flatnonzero((a["reachable_mask"] != b["reachable_mask"]) | (a["controller"] != b["controller"]))
+        states = np.unique(np.concatenate([rng.integers(0, S, 100_000, dtype=np.uint64),
+                                           changed[:50_000].astype(np.uint64)]))
+        rn, ct, st = O.spot_step(case, a["valid_mask"], a["candidate_mask"], a["reachable_mask"], a["controller"],
+                                 a["reach_step"], k, states)
+        assert np.array_equal(rn, b["reachable_mask"][states]), k
+        assert np.array_equal(ct, b["controller"][states]), k
+        assert np.array_equal(st, b["reach_step"][states]), k
+        if k < 75:
+            assert changed.size > 0, k
+    absn.close()
+
+
+def test_widest_fused_rows(ctx):
+    """256 x-cells: eight 32-bit words per row, the fused method's limit."""
+    case = C.unicycle_grid_case((256, 16, 8, 6), (3, 3), "wide_256", max_iterations=64)
+    want = O.solve(case)
+    absn = G.Abstraction(ctx, case)
+    p = G.Problem(ctx, absn, case, G.METHOD_AUTO)
+    p.solve(graph=True)
+    got = p.read()
+    assert p.timings()["method"] == G.METHOD_FUSED
+    p.close()
+    assert_same_result(got, want, "nx=256")
+    assert got["iterations"] == want["iterations"] and got["message"] == want["message"]
+    absn.close()
+
+
+def test_no_method_beyond_both_limits(ctx):
+    """257 x-cells: wider than the fused rows and than the stored method's
+    one-byte box bounds (255 cells per dimension)."""
+    case = C.unicycle_grid_case((257, 16, 8, 6), (3, 3), "wide_257")
+    absn = G.Abstraction(ctx, case)
+    with pytest.raises(G.GscError) as e:
+        G.Problem(ctx, absn, case, G.METHOD_AUTO)
+    assert e.value.status == 4
+    absn.close()
+
+
+def test_boxes_wider_than_a_word_fall_back_to_stored(ctx):
+    """x-boxes of more than 32 cells (a large x disturbance on 255 x-cells):
+    the fused method refuses them, the automatic choice is the stored
+    method, and the result is the oracle's."""
+    case = C.unicycle_grid_case((255, 8, 6, 4), (3, 3), "wide_boxes", max_iterations=64)
+    case["disturbance_half_width"] = [2.6, 0.01, 0.01, 0.01]
+    want = O.solve(case)
+    absn = G.Abstraction(ctx, case)
+    p = G.Problem(ctx, absn, case, G.METHOD_AUTO)
+    p.solve(graph=True)
+    got = p.read()
+    assert p.timings()["method"] == G.METHOD_STORED
+    p.close()
+    assert_same_result(got, want, "wide boxes")
+    assert got["iterations"] == want["iterations"] and got["message"] == want["message"]
+    with pytest.raises(G.GscError) as e:
+        G.Problem(ctx, absn, case, G.METHOD_FUSED)
+    assert e.value.status == 4
+    absn.close()
