@@ -12,6 +12,8 @@
 //   k_batch_status    one block: a copy of every instance's control record,
 //                     the number still running, and the CUDA-graph loop
 //                     condition.
+#include <atomic>
+
 #include "gsc_fused_body.cuh"
 
 namespace gsc_b200 {
@@ -153,15 +155,17 @@ inline unsigned int grid_of(uint32_t tasks, uint32_t cap) {
 template <int WMAX>
 cudaError_t launch_sat_t(const InstanceDesc* descs, const WorkList& wl, const WorkTotals& tot, const BatchShape& sh,
                          size_t smem, cudaStream_t st) {
-    static bool configured[64] = {};
+    // Launches may come from several host threads (a server's loop and the
+    // caller's); setting the attribute twice is harmless.
+    static std::atomic<bool> configured[64];
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= 64 || !configured[dev]) {
+    if (dev < 0 || dev >= 64 || !configured[dev].load()) {
         e = cudaFuncSetAttribute(k_batch_sat<WMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(kFusedSmemMax));
         if (e != cudaSuccess) return e;
-        if (dev >= 0 && dev < 64) configured[dev] = true;
+        if (dev >= 0 && dev < 64) configured[dev].store(true);
     }
     const uint32_t blocks = sh.sat_blocks ? grid_of(tot.sat, sh.sat_blocks) : grid_of(tot.sat, 0xFFFFFFFFu);
     k_batch_sat<WMAX><<<blocks, sh.sat_threads, smem, st>>>(descs, wl);

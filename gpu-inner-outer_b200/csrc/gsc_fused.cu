@@ -20,6 +20,8 @@
 //   k_fused_finalize applies the hits (reachable, active, controller,
 //                    reach_step, counters), builds D' for the next iteration,
 //                    and its last block applies the stop rules.
+#include <atomic>
+
 #include "gsc_fused_body.cuh"
 
 namespace gsc_b200 {
@@ -187,15 +189,17 @@ __global__ void __launch_bounds__(256) k_fused_finalize(GridInfo g, FusedFixArgs
 template <int W, bool NV>
 cudaError_t launch_sat_col_t(const GridInfo& g, const FusedFixArgs& a, size_t sm, cudaStream_t st) {
     // Opting in above 48 KB of shared memory is a per-device function attribute.
-    static bool configured[64] = {};
+    // Launches may come from several host threads (a server's loop and the
+    // caller's); setting the attribute twice is harmless.
+    static std::atomic<bool> configured[64];
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= 64 || !configured[dev]) {
+    if (dev < 0 || dev >= 64 || !configured[dev].load()) {
         e = cudaFuncSetAttribute(k_sat_col<W, NV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(kFusedSmemMax));
         if (e != cudaSuccess) return e;
-        if (dev >= 0 && dev < 64) configured[dev] = true;
+        if (dev >= 0 && dev < 64) configured[dev].store(true);
     }
     k_sat_col<W, NV><<<g.slices * g.mw, a.sat_threads, sm, st>>>(g, a);
     return cudaGetLastError();
