@@ -59,6 +59,8 @@ def parse():
     ap.add_argument("--rates", type=str, default="0.5,0.75,0.9",
                     help="Poisson arrival rates as fractions of the measured saturation throughput")
     ap.add_argument("--serve-budget-gb", type=float, default=24.0)
+    ap.add_argument("--host-loop", action="store_true",
+                    help="batched: iterate from the host instead of one CUDA graph (for per-kernel profiling)")
     ap.add_argument("--trajectories", type=int, default=1 << 20)
     ap.add_argument("--sim-steps", type=int, default=40)
     ap.add_argument("--plain-queries", type=int, default=0,
@@ -308,11 +310,12 @@ def bench_batched(args):
     ctx = G.Context(0, stream.cuda_stream)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
+    graph = not args.host_loop
     b = G.Batch(ctx, cases, autotune=True)     # tunes once; later batches of this class reuse the shapes
     rep0 = b.report()
     for _ in range(args.warmup):
         flush.fill_(1)
-        b.solve(graph=True)
+        b.solve(graph=graph)
     torch.cuda.synchronize(dev)
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     launches = 0
@@ -320,7 +323,7 @@ def bench_batched(args):
         for k in range(args.steps):
             flush.fill_(k & 0xFF)
             evs[k][0].record(stream)
-            b.solve(graph=True)
+            b.solve(graph=graph)
             evs[k][1].record(stream)
         torch.cuda.synchronize(dev)
     rep = b.report()
