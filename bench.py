@@ -37,6 +37,7 @@ sys.path.insert(0, PKG)
 import gsc_cases as C  # noqa: E402
 
 REF_BIN = os.path.join(ORACLE, "_ref", "gsc_ref")
+REF_GPU_BIN = os.path.join(ORACLE, "_ref", "gsc_ref_gpu")
 PUBLISHED_DEMO_SOLVE_MS = 214.936   # README.md:69, RTX 4090, 12 iterations
 PUBLISHED_DEMO_PAIRS = 401310000
 
@@ -100,6 +101,31 @@ def reference_sample(case, n_states, seed, threads):
     }
 
 
+def reference_gpu_runs(case, runs):
+    """The reference's own CUDA backend (cuda/kernels.cu, rebuilt for sm_100a
+    by oracle/Makefile) on this GPU: one record per run_case_cuda_u32 call."""
+    sys.path.insert(0, ORACLE)
+    import oracle as O
+
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "case.bin")
+        with open(path, "wb") as f:
+            f.write(bytes(O.to_struct(case)))
+        r = subprocess.run([REF_GPU_BIN, path, str(runs)], capture_output=True, text=True, timeout=900)
+    if r.returncode != 0:
+        return {"unavailable": (r.stderr.strip().splitlines() or ["exit %d" % r.returncode])[-1]}
+    recs = [json.loads(ln) for ln in r.stdout.splitlines() if ln.startswith("{")]
+    med = lambda k: statistics.median(x[k] for x in recs)
+    return {"runs": len(recs), "solve_ms": med("solve_ms"), "abstraction_ms": med("abstraction_ms"),
+            "total_ms": med("total_ms"), "pair_satisfaction_ms": med("pair_satisfaction_ms"),
+            "prefix_build_ms": med("prefix_build_ms"), "iterations": recs[0]["iterations"],
+            "reachable_states": recs[0]["reachable_states"],
+            "certified_candidates": recs[0]["certified_candidates"], "message": recs[0]["message"],
+            "device_bytes": recs[0]["device_bytes"],
+            "note": "the reference's cuda/kernels.cu built for sm_100a, run_case_cuda_u32 on the same GPU "
+                    "(solve_ms: its fixpoint loop; total_ms: with the abstraction and its copy to the host)"}
+
+
 def cpu_threads():
     try:
         return len(os.sched_getaffinity(0))
@@ -137,6 +163,11 @@ def run_reference_arm(args, case):
                          "sample": sample},
         "e2e": {"value": v, "unit": "pair-checks/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    # The reference's CUDA backend expresses the published demo (built-in
+    # hyperbolic constraint, rectangular candidate set) but not the quadric
+    # safe set of the other workloads.
+    if args.workload == "hyperbolic_demo" and os.path.exists(REF_GPU_BIN):
+        line["reference_gpu"] = reference_gpu_runs(case, 3)
     print(json.dumps(line))
 
 
