@@ -5,6 +5,7 @@
 // path is the tabulation of cos/sin along theta trajectories and of the
 // theta / v trajectories themselves (model.hpp:26-46), done with the C
 // library the reference calls, in its operation order.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -608,6 +609,9 @@ int problem_stage2(gsc_problem* p) {
     GSC_TRY(palloc(p, &p->fc, 1));
     GSC_TRY(palloc(p, &p->stats, static_cast<uint64_t>(kStatsCols) * p->stats_cap));
     GSC_TRY(palloc(p, &p->reach8, g.S));
+    // Pool memory is recycled: a read before the first solve sees a zero
+    // control record (no iterations), not a previous owner's bytes.
+    GSC_CU(ctx, cudaMemsetAsync(p->fc, 0, sizeof(FixControl), st));
 
     if (p->method == GSC_METHOD_STORED) {
         GSC_TRY(palloc(p, &p->pvalid, g.tsize));
@@ -971,7 +975,7 @@ int gsc_problem_read(gsc_problem* p, gsc_result* r) {
         GSC_CU(ctx, cudaMemcpyAsync(r->controller, p->controller, g.S * 4, cudaMemcpyDeviceToHost, st));
     if (r->reach_step)
         GSC_CU(ctx, cudaMemcpyAsync(r->reach_step, p->reach_step, g.S * 4, cudaMemcpyDeviceToHost, st));
-    const uint32_t n = std::min<uint32_t>(fc.iter, r->iter_capacity);
+    const uint32_t n = std::min<uint32_t>({fc.iter, r->iter_capacity, p->stats_cap - 1});
     if (n && (r->iter_new_reachable || r->iter_new_certified)) {
         std::vector<unsigned long long> hs(static_cast<size_t>(kStatsCols) * (n + 1));
         GSC_CU(ctx, cudaMemcpyAsync(hs.data(), p->stats, hs.size() * 8, cudaMemcpyDeviceToHost, st));

@@ -6,9 +6,11 @@
 // records) in the middle; all device memory comes from one growable pool.
 // The fixpoint is the batched kernels of gsc_batch_kernels.cu over every
 // instance, optionally as one CUDA graph: [init] -> while (any running)
-// { dilate, satisfaction, finalize, status }.  Launch shapes come from the
-// options, or from a small autotuner that times candidate shapes on the
-// batch itself and caches the winner per shape class.
+// { dilate, satisfaction, finalize, status }.  An instance that fills the
+// GPU on its own (is_big_instance) iterates with the one-problem kernels
+// inside the same step and shares only init and status.  Launch shapes come
+// from the options, or from a small autotuner that times candidate shapes
+// on the batch's small instances and caches the winner per shape class.
 #include <algorithm>
 #include <chrono>
 #include <cstring>
@@ -98,11 +100,15 @@ struct gsc_batch {
     PlanRecord* hplans = nullptr;   // pinned
     uint32_t* hrunning = nullptr;   // pinned
     InstanceDesc* ddesc = nullptr;
-    uint32_t* dlist = nullptr;
+    uint32_t* dlist = nullptr;       // the small instances' work list
+    uint32_t* dlist_all = nullptr;   // every instance: init and status
     uint32_t* drunning = nullptr;
-    std::vector<uint32_t> hlist;
-    WorkTotals tot{};
-    WorkList wl{};
+    std::vector<uint32_t> hlist, hlist_all;
+    std::vector<uint32_t> small;     // indices of the instances the batched kernels run
+    std::vector<BigInstance> big;    // the instances the one-problem kernels run
+    WorkTotals tot{}, tot_all{};
+    WorkList wl{}, wl_all{};
+    uint32_t step_launches = 0;      // kernel launches of one iteration step
     BatchShape shape{};
     uint32_t wmax = 1;
     size_t smem = 0;
@@ -139,26 +145,40 @@ uint32_t log2_ceil(uint64_t v) {
     return l;
 }
 
+// Work lists with `chunk` word positions per task: the small instances'
+// (the batched kernels) and every instance's (init and status).
 int upload_list(gsc_batch* b, uint32_t chunk) {
     std::vector<const gsc_problem*> probs;
     std::vector<uint32_t> slots;
-    for (uint32_t i = 0; i < b->probs.size(); ++i) {
+    for (uint32_t i : b->small) {
         probs.push_back(b->probs[i].get());
         slots.push_back(i);
     }
     build_work_list(probs, slots, chunk, b->hlist, b->tot);
+    probs.clear();
+    slots.clear();
+    for (uint32_t i = 0; i < b->probs.size(); ++i) {
+        probs.push_back(b->probs[i].get());
+        slots.push_back(i);
+    }
+    build_work_list(probs, slots, chunk, b->hlist_all, b->tot_all);
     GSC_CU(b->ctx, cudaMemcpyAsync(b->dlist, b->hlist.data(), b->hlist.size() * 4, cudaMemcpyHostToDevice,
                                    b->ctx->stream));
-    GSC_CU(b->ctx, cudaStreamSynchronize(b->ctx->stream));   // the host list is reused
-    b->wl = device_work_list(b->dlist, static_cast<uint32_t>(slots.size()), chunk, nullptr, b->drunning);
+    GSC_CU(b->ctx, cudaMemcpyAsync(b->dlist_all, b->hlist_all.data(), b->hlist_all.size() * 4,
+                                   cudaMemcpyHostToDevice, b->ctx->stream));
+    GSC_CU(b->ctx, cudaStreamSynchronize(b->ctx->stream));   // the host lists are reused
+    b->wl = device_work_list(b->dlist, static_cast<uint32_t>(b->small.size()), chunk, nullptr, b->drunning);
+    b->wl_all = device_work_list(b->dlist_all, static_cast<uint32_t>(b->probs.size()), chunk, nullptr, b->drunning);
     return GSC_OK;
 }
 
+cudaError_t enqueue_step(gsc_batch* b, cudaGraphConditionalHandle cond, int use_cond, uint32_t* launches) {
+    return launch_batch_step(b->ddesc, b->wl, b->tot, b->wl_all, b->big.data(), static_cast<uint32_t>(b->big.size()),
+                             b->shape, b->wmax, b->smem, sm_count(b->ctx), cond, use_cond, b->ctx->stream, launches);
+}
+
 int enqueue_iterations(gsc_batch* b, uint32_t count, uint32_t* launches) {
-    const int sms = sm_count(b->ctx);
-    for (uint32_t i = 0; i < count; ++i)
-        GSC_CU(b->ctx, launch_batch_iteration(b->ddesc, b->wl, b->tot, b->shape, b->wmax, b->smem, sms, 0, 0,
-                                              b->ctx->stream, launches));
+    for (uint32_t i = 0; i < count; ++i) GSC_CU(b->ctx, enqueue_step(b, 0, 0, launches));
     return GSC_OK;
 }
 
@@ -224,7 +244,7 @@ int build_batch_graph(gsc_batch* b) {
     GSC_CU(ctx, cudaGraphCreate(&g, 0));
     b->graph = g;
     GSC_CU(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-    cudaError_t e = launch_batch_init(b->ddesc, b->wl, b->tot, sms, st);
+    cudaError_t e = launch_batch_init(b->ddesc, b->wl_all, b->tot_all, sms, st);
     cudaError_t e2 = cudaStreamEndCapture(st, &ginit);
     GSC_CU(ctx, e);
     GSC_CU(ctx, e2);
@@ -242,7 +262,7 @@ int build_batch_graph(gsc_batch* b) {
     GSC_CU(ctx, cudaGraphAddNode(&cnode, g, &init_node, 1, &cp));
     cudaGraph_t body = cp.conditional.phGraph_out[0];
     GSC_CU(ctx, cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-    e = launch_batch_iteration(b->ddesc, b->wl, b->tot, b->shape, b->wmax, b->smem, sms, handle, 1, st, nullptr);
+    e = enqueue_step(b, handle, 1, nullptr);
     cudaGraph_t body_out = nullptr;
     e2 = cudaStreamEndCapture(st, &body_out);
     GSC_CU(ctx, e);
@@ -300,25 +320,35 @@ int batch_create(gsc_batch* b, uint32_t count, const gsc_model_desc* models, con
         if (s == GSC_OK) s = problem_stage2(p);
         if (s != GSC_OK) return fail(ctx, s, "instance " + std::to_string(i) + ": " + ctx->last_error);
     }
-    // Instance table, work list and launch shapes.
+    // Instance table, work lists and launch shapes; wmax and the shared
+    // memory of the batched satisfaction kernel come from the small instances.
     std::vector<InstanceDesc> hd(count);
     uint32_t wmax = 1, nv_any = 0;
     size_t smem = 0;
     for (uint32_t i = 0; i < count; ++i) {
         const gsc_problem* p = b->probs[i].get();
         hd[i] = make_instance(p);
+        if (instance_smem(p) > kFusedSmemMax)
+            return fail(ctx, GSC_ERR_UNSUPPORTED, "instance " + std::to_string(i) + ": needs too much shared memory");
+        if (is_big_instance(p->g)) {
+            b->big.push_back(BigInstance{p->g, hd[i].a});
+            continue;
+        }
+        b->small.push_back(i);
         wmax = std::max(wmax, p->g.W);
         smem = std::max(smem, instance_smem(p));
         nv_any |= p->need_valid ? 1u : 0u;
     }
     b->wmax = wmax_of(wmax);
     b->smem = smem;
-    if (smem > kFusedSmemMax) return fail(ctx, GSC_ERR_UNSUPPORTED, "batch: an instance needs too much shared memory");
+    b->step_launches = 3 * static_cast<uint32_t>(b->big.size()) + (b->small.empty() ? 0u : 3u) + 1u;
     void* q = nullptr;
     GSC_TRY(device_alloc(ctx, b->pool, b->own, b->own_bytes, &q, sizeof(InstanceDesc) * count));
     b->ddesc = static_cast<InstanceDesc*>(q);
     GSC_TRY(device_alloc(ctx, b->pool, b->own, b->own_bytes, &q, 4ull * (count + 4ull * (count + 1))));
     b->dlist = static_cast<uint32_t*>(q);
+    GSC_TRY(device_alloc(ctx, b->pool, b->own, b->own_bytes, &q, 4ull * (count + 4ull * (count + 1))));
+    b->dlist_all = static_cast<uint32_t*>(q);
     GSC_TRY(device_alloc(ctx, b->pool, b->own, b->own_bytes, &q, 4));
     b->drunning = static_cast<uint32_t*>(q);
     GSC_CU(ctx, cudaMemcpyAsync(b->ddesc, hd.data(), sizeof(InstanceDesc) * count, cudaMemcpyHostToDevice, st));
@@ -333,10 +363,11 @@ int batch_create(gsc_batch* b, uint32_t count, const gsc_model_desc* models, con
         return fail(ctx, GSC_ERR_INVALID_ARGUMENT, "chunk_words must be a positive multiple of 256");
     GSC_TRY(upload_list(b, b->shape.chunk));
     b->t.tuned = 0;
-    if (opt && opt->autotune) {
+    if (opt && opt->autotune && !b->small.empty()) {
         uint64_t words = 0;
-        for (const auto& d : hd) words += d.words;
-        const ShapeKey key{b->wmax, count, log2_ceil(b->tot.sat), log2_ceil(words), nv_any};
+        for (uint32_t i : b->small) words += hd[i].words;
+        const ShapeKey key{b->wmax, static_cast<uint32_t>(b->small.size()), log2_ceil(b->tot.sat), log2_ceil(words),
+                           nv_any};
         bool hit = false;
         {
             std::lock_guard<std::mutex> lk(g_tune_mu);
@@ -401,7 +432,7 @@ int gsc_batch_solve(gsc_batch* b, uint32_t flags) {
         GSC_CU(ctx, cudaGraphLaunch(b->exec, st));
         launches = 0;   // counted below from the iterations run
     } else {
-        GSC_CU(ctx, launch_batch_init(b->ddesc, b->wl, b->tot, sms, st));
+        GSC_CU(ctx, launch_batch_init(b->ddesc, b->wl_all, b->tot_all, sms, st));
         launches = 1;
         uint32_t cap = 0;
         for (const auto& p : b->probs) cap = std::max(cap, p->stats_cap);
@@ -443,18 +474,20 @@ int gsc_batch_timings(gsc_batch* b, gsc_batch_report* out) {
         FixControl fc;
         GSC_CU(ctx, cudaMemcpyAsync(&fc, p->fc, sizeof(fc), cudaMemcpyDeviceToHost, ctx->stream));
         GSC_CU(ctx, cudaStreamSynchronize(ctx->stream));
-        maxit = std::max(maxit, fc.iter);
-        if (fc.iter) {
-            std::vector<unsigned long long> hs(static_cast<size_t>(kStatsCols) * (fc.iter + 1));
+        const uint32_t iters = std::min<uint32_t>(fc.iter, p->stats_cap - 1);
+        maxit = std::max(maxit, iters);
+        if (iters) {
+            std::vector<unsigned long long> hs(static_cast<size_t>(kStatsCols) * (iters + 1));
             GSC_CU(ctx, cudaMemcpyAsync(hs.data(), p->stats, hs.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
             GSC_CU(ctx, cudaStreamSynchronize(ctx->stream));
-            for (uint32_t i = 1; i <= fc.iter; ++i) tests += hs[kStatsCols * i + 2];
+            for (uint32_t i = 1; i <= iters; ++i) tests += hs[kStatsCols * i + 2];
         }
     }
     b->t.max_iterations_run = maxit;
     b->t.pair_tests = tests;
     // Graph solves run the body once per iteration of the longest instance.
-    b->t.kernel_launches = b->last_launches == 0xFFFFFFFFu ? 1 + 4 * std::max<uint32_t>(maxit, 1) : b->last_launches;
+    b->t.kernel_launches =
+        b->last_launches == 0xFFFFFFFFu ? 1 + b->step_launches * std::max<uint32_t>(maxit, 1) : b->last_launches;
     b->t.sat_threads = b->shape.sat_threads;
     const int sms = sm_count(ctx);
     b->t.sat_blocks_per_sm = b->shape.sat_blocks / static_cast<uint32_t>(sms);
@@ -496,7 +529,7 @@ int gsc_batch_read_all(gsc_batch* b, gsc_result* out) {
             GSC_CU(ctx, cudaMemcpyAsync(r->controller, p->controller, g.S * 4, cudaMemcpyDeviceToHost, st));
         if (r->reach_step)
             GSC_CU(ctx, cudaMemcpyAsync(r->reach_step, p->reach_step, g.S * 4, cudaMemcpyDeviceToHost, st));
-        const uint32_t rows = std::min<uint32_t>(fc[i].iter, r->iter_capacity);
+        const uint32_t rows = std::min<uint32_t>({fc[i].iter, r->iter_capacity, p->stats_cap - 1});
         if (rows && (r->iter_new_reachable || r->iter_new_certified)) {
             hs[i].resize(static_cast<size_t>(kStatsCols) * (rows + 1));
             GSC_CU(ctx, cudaMemcpyAsync(hs[i].data(), p->stats, hs[i].size() * 8, cudaMemcpyDeviceToHost, st));

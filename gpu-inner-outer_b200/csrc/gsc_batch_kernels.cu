@@ -12,6 +12,8 @@
 //   k_batch_status    one block: a copy of every instance's control record,
 //                     the number still running, and the CUDA-graph loop
 //                     condition.
+// Instances big enough to fill the GPU alone run the one-problem kernels in
+// the same step (launch_batch_step) and share only init and status.
 #include <atomic>
 
 #include "gsc_fused_body.cuh"
@@ -183,41 +185,50 @@ cudaError_t launch_batch_init(const InstanceDesc* descs, const WorkList& wl, con
     return cudaGetLastError();
 }
 
-cudaError_t launch_batch_iteration(const InstanceDesc* descs, const WorkList& wl, const WorkTotals& tot,
-                                   const BatchShape& sh, uint32_t wmax, size_t smem, int sms,
-                                   cudaGraphConditionalHandle cond, int use_cond, cudaStream_t st,
-                                   uint32_t* launches) {
+cudaError_t launch_batch_step(const InstanceDesc* descs, const WorkList& small, const WorkTotals& tot_small,
+                              const WorkList& all, const BigInstance* big, uint32_t nbig, const BatchShape& sh,
+                              uint32_t wmax, size_t smem, int sms, cudaGraphConditionalHandle cond, int use_cond,
+                              cudaStream_t st, uint32_t* launches) {
     if (sh.sat_threads < 32 || sh.sat_threads > 256 || sh.sat_threads % 32 || smem > kFusedSmemMax)
         return cudaErrorInvalidValue;
     uint32_t n = 0;
     cudaError_t e = cudaSuccess;
-    if (tot.dil) {
-        k_batch_dilate<<<grid_of(tot.dil, 16u * sms), 256, 0, st>>>(descs, wl);
+    // A stopped big instance's kernels return at once (they read its stop flag).
+    for (uint32_t i = 0; e == cudaSuccess && i < nbig; ++i) e = launch_fused_iteration(big[i].g, big[i].a, st, &n);
+    if (e == cudaSuccess && tot_small.dil) {
+        k_batch_dilate<<<grid_of(tot_small.dil, 16u * sms), 256, 0, st>>>(descs, small);
         e = cudaGetLastError();
         ++n;
     }
-    if (e == cudaSuccess && tot.sat) {
+    if (e == cudaSuccess && tot_small.sat) {
         switch (wmax) {
-            case 1: e = launch_sat_t<1>(descs, wl, tot, sh, smem, st); break;
-            case 2: e = launch_sat_t<2>(descs, wl, tot, sh, smem, st); break;
+            case 1: e = launch_sat_t<1>(descs, small, tot_small, sh, smem, st); break;
+            case 2: e = launch_sat_t<2>(descs, small, tot_small, sh, smem, st); break;
             case 3:
-            case 4: e = launch_sat_t<4>(descs, wl, tot, sh, smem, st); break;
-            default: e = launch_sat_t<8>(descs, wl, tot, sh, smem, st); break;
+            case 4: e = launch_sat_t<4>(descs, small, tot_small, sh, smem, st); break;
+            default: e = launch_sat_t<8>(descs, small, tot_small, sh, smem, st); break;
         }
         ++n;
     }
-    if (e == cudaSuccess && tot.fin) {
-        k_batch_finalize<<<grid_of(tot.fin, 16u * sms), 256, 0, st>>>(descs, wl);
+    if (e == cudaSuccess && tot_small.fin) {
+        k_batch_finalize<<<grid_of(tot_small.fin, 16u * sms), 256, 0, st>>>(descs, small);
         e = cudaGetLastError();
         ++n;
     }
     if (e == cudaSuccess) {
-        k_batch_status<<<1, 256, 0, st>>>(descs, wl, cond, use_cond);
+        k_batch_status<<<1, 256, 0, st>>>(descs, all, cond, use_cond);
         e = cudaGetLastError();
         ++n;
     }
     if (launches) *launches += n;
     return e;
+}
+
+cudaError_t launch_batch_iteration(const InstanceDesc* descs, const WorkList& wl, const WorkTotals& tot,
+                                   const BatchShape& sh, uint32_t wmax, size_t smem, int sms,
+                                   cudaGraphConditionalHandle cond, int use_cond, cudaStream_t st,
+                                   uint32_t* launches) {
+    return launch_batch_step(descs, wl, tot, wl, nullptr, 0, sh, wmax, smem, sms, cond, use_cond, st, launches);
 }
 
 }  // namespace gsc_b200

@@ -214,6 +214,21 @@ struct WorkTotals {
     uint32_t sat, dil, fin, ini;
 };
 
+// An instance of a batch that keeps the GPU busy on its own (at least
+// kBigPairs state-input pairs per iteration) iterates with the one-problem
+// kernels, whose row width is a compile-time constant and whose arguments
+// stay in the constant bank.  Smaller instances gain more from sharing the
+// batched kernels' launches than they lose to their run-time row width.
+constexpr uint64_t kBigPairs = 1ull << 28;
+inline bool is_big_instance(const GridInfo& g) { return g.S * g.M >= kBigPairs; }
+
+// A big instance of a batch: its grid and its fixpoint arguments (without a
+// graph condition; the batch's status kernel sets that).
+struct BigInstance {
+    GridInfo g;
+    FusedFixArgs a;
+};
+
 cudaError_t launch_batch_init(const InstanceDesc* descs, const WorkList& wl, const WorkTotals& tot, int sms,
                               cudaStream_t st);
 // One fixpoint iteration of every listed instance: dilate, satisfaction,
@@ -222,6 +237,14 @@ cudaError_t launch_batch_iteration(const InstanceDesc* descs, const WorkList& wl
                                    const BatchShape& sh, uint32_t wmax, size_t smem, int sms,
                                    cudaGraphConditionalHandle cond, int use_cond, cudaStream_t st,
                                    uint32_t* launches);
+// One fixpoint iteration of a mixed batch: each of the nbig big instances
+// with the one-problem kernels, the instances of `small` with the batched
+// kernels (wmax and smem are theirs), then the status kernel over `all`
+// (every instance, big and small, in the order its status records use).
+cudaError_t launch_batch_step(const InstanceDesc* descs, const WorkList& small, const WorkTotals& tot_small,
+                              const WorkList& all, const BigInstance* big, uint32_t nbig, const BatchShape& sh,
+                              uint32_t wmax, size_t smem, int sms, cudaGraphConditionalHandle cond, int use_cond,
+                              cudaStream_t st, uint32_t* launches);
 size_t batch_sat_static_smem();
 
 // Class record words per plane: a 16-byte header + kClassMax * W masks.

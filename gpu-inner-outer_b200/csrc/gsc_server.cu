@@ -3,7 +3,9 @@
 // No counterpart in the reference.  One loop thread owns three streams:
 //   prep   set-up of admitted queries (problem stage 1, plan, stage 2, init);
 //   main   batched fixpoint steps over every running query (the kernels of
-//          gsc_batch_kernels.cu on a task list of the running slots);
+//          gsc_batch_kernels.cu on a task list of the running slots; a
+//          query that fills the GPU alone runs the one-problem kernels in
+//          the same step);
 //   copy   results of stopped queries to the callers' buffers.
 // A query moves QUEUED -> PREP1 -> PREP2 -> RUN -> COPY -> DONE.  Admission
 // is in arrival order while a slot is free and the query's buffers fit the
@@ -63,12 +65,13 @@ struct gsc_server {
     cudaEvent_t ev_step = nullptr;
     // device
     InstanceDesc* ddesc = nullptr;
-    uint32_t* dlist = nullptr;
+    uint32_t* dlist = nullptr;         // every running query: status
+    uint32_t* dlist_small = nullptr;   // the running queries the batched kernels run
     FixControl* dstatus = nullptr;
     void* dmem = nullptr;
     // pinned host
     InstanceDesc* hdesc = nullptr;
-    uint32_t* hlist = nullptr;
+    uint32_t* hlist = nullptr;   // both lists, the small one after the other
     FixControl* hstatus = nullptr;
     PlanRecord* hplans = nullptr;
     unsigned long long* hstats = nullptr;   // [slot][kStatsRows][kStatsCols]
@@ -333,10 +336,11 @@ void loop(gsc_server* s) {
     cudaSetDevice(s->ctx->device);
     const int sms = sm_count(s->ctx);
     bool list_dirty = true;
-    std::vector<const gsc_problem*> probs;
-    std::vector<uint32_t> slots, hl;
-    WorkTotals tot{};
-    WorkList wl{};
+    std::vector<const gsc_problem*> probs, sprobs;
+    std::vector<uint32_t> slots, sslots, hl, hls;
+    std::vector<BigInstance> big;
+    WorkTotals tot{}, tot_small{};
+    WorkList wl{}, wl_small{};
     uint32_t wmax = 1;
     size_t smem = 0;
     const uint32_t K = s->opt.iterations_per_step;
@@ -355,27 +359,44 @@ void loop(gsc_server* s) {
             continue;
         }
         if (list_dirty) {
+            // Queries that fill the GPU alone run the one-problem kernels;
+            // the status list covers every running query, in running order.
             probs.clear();
             slots.clear();
+            sprobs.clear();
+            sslots.clear();
+            big.clear();
             uint32_t w = 1;
             smem = 0;
             for (Req* r : s->running) {
                 probs.push_back(r->p.get());
                 slots.push_back(r->slot);
+                if (is_big_instance(r->p->g)) {
+                    big.push_back(BigInstance{r->p->g, s->hdesc[r->slot].a});
+                    continue;
+                }
+                sprobs.push_back(r->p.get());
+                sslots.push_back(r->slot);
                 w = std::max(w, r->p->g.W);
                 smem = std::max(smem, instance_smem(r->p.get()));
             }
             wmax = wmax_of(w);
             build_work_list(probs, slots, s->shape.chunk, hl, tot);
+            build_work_list(sprobs, sslots, s->shape.chunk, hls, tot_small);
             std::memcpy(s->hlist, hl.data(), hl.size() * 4);
+            std::memcpy(s->hlist + hl.size(), hls.data(), hls.size() * 4);
             cudaMemcpyAsync(s->dlist, s->hlist, hl.size() * 4, cudaMemcpyHostToDevice, s->s_main);
+            cudaMemcpyAsync(s->dlist_small, s->hlist + hl.size(), hls.size() * 4, cudaMemcpyHostToDevice, s->s_main);
             wl = device_work_list(s->dlist, static_cast<uint32_t>(slots.size()), s->shape.chunk, s->dstatus, nullptr);
+            wl_small = device_work_list(s->dlist_small, static_cast<uint32_t>(sslots.size()), s->shape.chunk, nullptr,
+                                        nullptr);
             list_dirty = false;
         }
         const uint32_t n = static_cast<uint32_t>(s->running.size());
         cudaError_t e = cudaSuccess;
         for (uint32_t i = 0; e == cudaSuccess && i < K; ++i)
-            e = launch_batch_iteration(s->ddesc, wl, tot, s->shape, wmax, smem, sms, 0, 0, s->s_main, nullptr);
+            e = launch_batch_step(s->ddesc, wl_small, tot_small, wl, big.data(), static_cast<uint32_t>(big.size()),
+                                  s->shape, wmax, smem, sms, 0, 0, s->s_main, nullptr);
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(s->hstatus, s->dstatus, sizeof(FixControl) * n, cudaMemcpyDeviceToHost, s->s_main);
         if (e == cudaSuccess) e = cudaEventRecord(s->ev_step, s->s_main);
@@ -490,7 +511,7 @@ int gsc_server_create(gsc_context* ctx, const gsc_server_options* options, gsc_s
     GSC_CU(ctx, cudaEventCreateWithFlags(&s->ev_step, cudaEventDisableTiming));
     const uint32_t n = o.max_slots;
     const size_t list_words = n + 4ull * (n + 1);
-    const size_t dbytes = sizeof(InstanceDesc) * n + sizeof(FixControl) * n + 4 * list_words + 256 * 3;
+    const size_t dbytes = sizeof(InstanceDesc) * n + sizeof(FixControl) * n + 2 * 4 * list_words + 256 * 4;
     GSC_CU(ctx, cudaMalloc(&s->dmem, dbytes));
     char* d = static_cast<char*>(s->dmem);
     auto carve = [&](size_t bytes) {
@@ -501,8 +522,9 @@ int gsc_server_create(gsc_context* ctx, const gsc_server_options* options, gsc_s
     s->ddesc = reinterpret_cast<InstanceDesc*>(carve(sizeof(InstanceDesc) * n));
     s->dstatus = reinterpret_cast<FixControl*>(carve(sizeof(FixControl) * n));
     s->dlist = reinterpret_cast<uint32_t*>(carve(4 * list_words));
+    s->dlist_small = reinterpret_cast<uint32_t*>(carve(4 * list_words));
     GSC_CU(ctx, cudaMallocHost(&s->hdesc, sizeof(InstanceDesc) * n));
-    GSC_CU(ctx, cudaMallocHost(&s->hlist, 4 * list_words));
+    GSC_CU(ctx, cudaMallocHost(&s->hlist, 2 * 4 * list_words));
     GSC_CU(ctx, cudaMallocHost(&s->hstatus, sizeof(FixControl) * n));
     GSC_CU(ctx, cudaMallocHost(&s->hplans, sizeof(PlanRecord) * n));
     GSC_CU(ctx, cudaMallocHost(&s->hstats, sizeof(unsigned long long) * kStatsCols * kStatsRows * n));

@@ -114,3 +114,25 @@ def test_batch_rejects_bad_options(ctx):
     with pytest.raises(G.GscError) as e:
         G.Batch(ctx, [INDEX["small"]["case"]], sat_threads=96)
     assert e.value.status == 1
+
+
+def test_batch_with_instances_that_fill_the_gpu(ctx):
+    """Instances of 65x65x38x25 states x 100 inputs (4 x 10^8 pairs) iterate
+    with the one-problem kernels inside the batch, the small ones with the
+    batched kernels; every result is its solo solve's, in the graph (launch
+    shapes autotuned) and the host loop.  Without autotuning (which iterates
+    the small instances to time them), a report before the first solve reads
+    no iterations from the recycled pool memory."""
+    demo = C.demo_scale_case()
+    cases = [demo, INDEX["small_obstacles"]["case"], C.clone(demo, max_iterations=5), INDEX["hyperbolic_mid_a"]["case"]]
+    want = [solo(ctx, c) for c in cases]
+    for graph in (True, False):
+        b = G.Batch(ctx, cases, autotune=graph)
+        if not graph:
+            assert b.report()["max_iterations_run"] == 0
+        b.solve(graph=graph)
+        for i, got in enumerate(b.read_all()):
+            assert_same_result(got, want[i], f"graph={graph} instance {i}")
+            assert got["iterations"] == want[i]["iterations"] and got["message"] == want[i]["message"]
+        assert b.report()["max_iterations_run"] == max(w["iterations"] for w in want)
+        b.close()

@@ -134,3 +134,31 @@ def test_wait_timeout_and_unknown_ticket(ctx, models):
             assert time.time() < deadline
             time.sleep(0.001)
     srv.close()
+
+
+def test_served_queries_that_fill_the_gpu_match_alone(ctx, models):
+    """Queries on a 65x65x38x25 x 100 grid (4 x 10^8 pairs) iterate with the
+    one-problem kernels next to small queries on the batched kernels; each
+    result is the same query's solved alone."""
+    cases, absn = models
+    demo = C.demo_scale_case()
+    a_demo = G.Abstraction(ctx, demo)
+    srv = G.Server(ctx, memory_budget=6 << 30, iterations_per_step=1)
+    queries = []
+    for i in range(12):
+        k = ("demo", "small", "mid")[i % 3]
+        queries.append((k, C.random_query(demo if k == "demo" else cases[k], 23, i)))
+    abs_of = {"demo": a_demo, "small": absn["small"], "mid": absn["mid"]}
+    tickets = [srv.submit(abs_of[k], q) for k, q in queries]
+    results = [srv.wait(t) for t in tickets]
+    st = srv.stats()
+    srv.close()
+    assert st["completed"] == len(queries) and st["failed"] == 0
+    assert st["max_running"] > 1
+    for (k, q), got in zip(queries, results):
+        assert got["status"] == 0
+        want = alone(ctx, abs_of[k], q)
+        assert_same_result(got, want, q["name"])
+        for f in ("iterations", "message", "converged", "reachable_states", "certified_candidates"):
+            assert got[f] == want[f], (q["name"], f)
+    a_demo.close()
