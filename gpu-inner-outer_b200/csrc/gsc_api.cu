@@ -660,6 +660,9 @@ int problem_stage2(gsc_problem* p) {
     GSC_TRY(palloc(p, &p->dzw, combos * words));
     p->rl_words = static_cast<uint32_t>(g.rows / 32 + 2);
     GSC_TRY(palloc(p, &p->rowlost, 2ull * p->rl_words));
+    GSC_TRY(palloc(p, &p->offz, static_cast<uint64_t>(g.n[2]) * g.mw));
+    GSC_TRY(palloc(p, &p->offv, static_cast<uint64_t>(g.n[3]) * g.ma));
+    GSC_CU(ctx, launch_sat_offsets(g, p->zt, p->wt, p->kidx, p->lidx, p->dil.nl, p->offz, p->offv, st));
     GSC_CU(ctx, launch_pack_bits(g, 0, p->valid, nullptr, p->validb, st));
     GSC_CU(ctx, launch_pack_bits(g, 0, p->cand, nullptr, p->candb, st));
     if (!p->safe) {
@@ -738,6 +741,8 @@ FusedFixArgs fused_args(const gsc_problem* p, cudaGraphConditionalHandle cond, i
     a.lidx = p->lidx;
     a.nl = p->dil.nl;
     a.dil = p->dil;
+    a.offz = p->offz;
+    a.offv = p->offv;
     a.cond = cond;
     a.use_cond = use_cond;
     return a;

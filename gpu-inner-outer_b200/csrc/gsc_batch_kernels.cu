@@ -80,7 +80,7 @@ template <int WMAX>
 __global__ void __launch_bounds__(256) k_batch_sat(const InstanceDesc* __restrict__ descs, WorkList wl) {
     extern __shared__ __align__(16) bword smem[];
     __shared__ __align__(16) InstanceDesc sd;
-    __shared__ uint32_t s_nrep;
+    __shared__ uint32_t s_meta[4];
     const uint32_t total = wl.sat_off[wl.n];
     uint32_t cur = 0xFFFFFFFFu;
     for (uint32_t t = blockIdx.x; t < total; t += gridDim.x) {
@@ -93,7 +93,7 @@ __global__ void __launch_bounds__(256) k_batch_sat(const InstanceDesc* __restric
             __syncthreads();
             cur = slot;
         }
-        sat_col_task<WMAX, false, 2>(sd.g, sd.a, t - wl.sat_off[k], smem, &s_nrep);
+        sat_col_task<WMAX, false, 2>(sd.g, sd.a, t - wl.sat_off[k], smem, s_meta);
         __syncthreads();
     }
 }

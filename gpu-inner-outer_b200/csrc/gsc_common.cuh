@@ -196,7 +196,7 @@ struct FixControl {
     uint32_t max_iterations;
     uint32_t stats_cap;       // stats entries (iteration index 1..stats_cap-1)
     uint32_t ticket;          // blocks of the finalize kernel done this iteration
-    uint32_t pad;
+    uint32_t last_new;        // states the last iteration added (saturated at 2^32 - 1)
     unsigned long long candidate_count;
     unsigned long long certified;
     unsigned long long reachable;

@@ -228,6 +228,7 @@ __global__ void k_fix_init(FixControl* fc, uint32_t max_iterations, uint32_t sta
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         fc->iter = 0;
         fc->ticket = 0;
+        fc->last_new = 0;
         fc->max_iterations = max_iterations;
         fc->stats_cap = stats_cap;
         fc->valid_count = counts[0];

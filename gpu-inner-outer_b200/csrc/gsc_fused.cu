@@ -143,12 +143,41 @@ __global__ void __launch_bounds__(256) k_plan(GridInfo g, const uint32_t* __rest
     }
 }
 
+// The two parts of the word offset in dzw of a representative's dilated D'
+// row 0 (sat_col_task, phase B), (kslot * nl + lslot) * rows * W +
+// n1 * (lz + n2 * lw) * W in 32-bit arithmetic: per omega column and theta
+// cell the kslot and lz terms, per acceleration and v cell the lslot and lw
+// terms (0 for a rejected v box, which is never a representative).
+__global__ void k_sat_offsets(GridInfo g, const uint32_t* __restrict__ zt, const uint32_t* __restrict__ wt,
+                              const uint8_t* __restrict__ kidx, const uint8_t* __restrict__ lidx, uint32_t nl,
+                              uint32_t* __restrict__ offz, uint32_t* __restrict__ offv) {
+    const uint32_t n1 = g.n[1], n2 = g.n[2], W = g.W;
+    const uint32_t pos = static_cast<uint32_t>(g.rows * W);
+    const uint32_t nzt = n2 * g.mw, nwt = g.n[3] * g.ma;
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < nzt + nwt; e += gridDim.x * blockDim.x) {
+        if (e < nzt) {
+            const uint32_t ze = zt[e];
+            const uint32_t lz = lo16(ze), hz = hi16(ze);
+            const uint32_t nz = (lz <= hz) ? hz - lz + 1 : n2 - lz + hz + 1;
+            offz[e] = kidx[nz] * nl * pos + n1 * lz * W;
+        } else {
+            const uint32_t we = wt[e - nzt];
+            uint32_t o = 0;
+            if (we != kReject && hi16(we) >= lo16(we)) {
+                const uint32_t lw = lo16(we), nwb = hi16(we) - lw + 1;
+                o = lidx[nwb] * pos + n1 * n2 * lw * W;
+            }
+            offv[e - nzt] = o;
+        }
+    }
+}
+
 // One block per (theta, v) slice x omega column (sat_col_task).
 template <int W, bool NV>
 __global__ void __launch_bounds__(kFusedWarps * 32) k_sat_col(GridInfo g, FusedFixArgs a) {
     extern __shared__ __align__(16) bword smem[];
-    __shared__ uint32_t s_nrep;
-    sat_col_task<W, true, NV ? 1 : 0>(g, a, blockIdx.x, smem, &s_nrep);
+    __shared__ uint32_t s_meta[4];
+    sat_col_task<W, true, NV ? 1 : 0>(g, a, blockIdx.x, smem, s_meta);
 }
 
 // Apply the iteration's hits, build next iteration's D', count, and let the
@@ -216,8 +245,9 @@ size_t fused_smem_bytes(const GridInfo& g, uint32_t cls_words, int need_valid, u
     const size_t nw = static_cast<size_t>(g.n[1]) * g.W;
     const size_t nv = need_valid ? 2 : 1;
     const size_t mr = max_reps;
-    // act, E rows (D' and valid), sat, class records, y tables, representatives, changed-row masks
-    const size_t words = nw + mr * nw * nv + mr * nw + mr * cls_words + mr * g.n[1] + static_cast<size_t>(g.ma) +
+    // act, E rows (D' and valid), sat, class records, y tables, representatives (acceleration, v window,
+    // offset part), changed-row masks
+    const size_t words = nw + mr * nw * nv + mr * nw + mr * cls_words + mr * g.n[1] + 3 * static_cast<size_t>(g.ma) +
                          mr * ((g.n[1] + 31) / 32);
     return sizeof(bword) * words;
 }
@@ -236,6 +266,13 @@ cudaError_t launch_dilate(const GridInfo& g, const bword* src, bword* dst, const
     uint64_t b = (pos + 255) / 256;
     if (b > 8192) b = 8192;
     k_dilate<<<static_cast<unsigned int>(b ? b : 1), 256, 0, st>>>(g, src, dst, d, fc, rowlost, rl_words);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sat_offsets(const GridInfo& g, const uint32_t* zt, const uint32_t* wt, const uint8_t* kidx,
+                               const uint8_t* lidx, uint32_t nl, uint32_t* offz, uint32_t* offv, cudaStream_t st) {
+    const uint64_t n = static_cast<uint64_t>(g.n[2]) * g.mw + static_cast<uint64_t>(g.n[3]) * g.ma;
+    k_sat_offsets<<<blocks_for(n, 256), 256, 0, st>>>(g, zt, wt, kidx, lidx, nl, offz, offv);
     return cudaGetLastError();
 }
 

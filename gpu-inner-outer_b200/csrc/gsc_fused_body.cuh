@@ -64,6 +64,7 @@ __device__ __forceinline__ void init_control(FixControl* fc, uint32_t max_iterat
                                              const unsigned long long* counts) {
     fc->iter = 0;
     fc->ticket = 0;
+    fc->last_new = 0;
     fc->max_iterations = max_iterations;
     fc->stats_cap = stats_cap;
     fc->valid_count = counts[0];
@@ -129,6 +130,15 @@ __device__ __forceinline__ void dilate_position(const GridInfo& g, const bword* 
     }
 }
 
+// 4-byte asynchronous copy global -> shared (cp.async), complete after
+// cp_async_wait_all and the block's next barrier.
+__device__ __forceinline__ void cp_async4(void* smem_dst, const void* gmem_src) {
+    const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(smem_dst));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(gmem_src) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 // One (theta, v) slice x omega column jw (task = slice * mw + jw) of the
 // satisfaction test, by the whole block:
 //  B. per representative acceleration (the lowest of each group of inputs
@@ -149,9 +159,8 @@ constexpr unsigned long long kIncrementalRows = 16;
 
 template <int WMAX, bool EXACTW, int NVMODE>
 __device__ __forceinline__ void sat_col_task(const GridInfo& g, const FusedFixArgs& a, uint32_t task,
-                                             bword* smem, uint32_t* s_nrep) {
+                                             bword* smem, uint32_t* s_meta) {
     const FixControl* fc = a.fc;
-    if (fc->stop) return;
     const uint32_t W = EXACTW ? static_cast<uint32_t>(WMAX) : g.W;
     const bool NV = NVMODE == 2 ? (a.need_valid != 0) : (NVMODE == 1);
     const uint32_t n0 = g.n[0], n1 = g.n[1], n2 = g.n[2], ma = g.ma, mw = g.mw;
@@ -164,7 +173,6 @@ __device__ __forceinline__ void sat_col_task(const GridInfo& g, const FusedFixAr
     const uint32_t nv = NV ? 2u : 1u;
     const uint32_t cw = a.cls_words;
     const uint32_t mr = a.max_reps;
-    const uint32_t pos = static_cast<uint32_t>(g.rows * W);
 
     bword* act = smem;
     bword* Eall = act + nw;                               // max_reps * nw * nv
@@ -172,53 +180,96 @@ __device__ __forceinline__ void sat_col_task(const GridInfo& g, const FusedFixAr
     bword* cls = sat + mr * nw;                           // max_reps * cw
     uint32_t* yts = cls + mr * cw;                        // max_reps * n1
     uint32_t* reps = yts + mr * n1;                       // ma: acceleration of each representative slot
-    uint32_t* rowchg = reps + ma;                         // max_reps * W1: y rows of a window that lost a cell
+    uint32_t* repw = reps + ma;                           // ma: its v window
+    uint32_t* repo = repw + ma;                           // ma: its part of the dilated rows' offset
+    uint32_t* rowchg = repo + ma;                         // max_reps * W1: y rows of a window that lost a cell
     const uint32_t W1 = (n1 + 31) / 32;
 
     const uint64_t pcol = (static_cast<uint64_t>(i2) * g.n[3] + i3) * g.M + static_cast<uint64_t>(ma) * jw;
+    // A. One round of loads that depend on the task alone: the active rows
+    // (two per thread before either is stored), the representatives in
+    // increasing acceleration order (warp ballot) with their v windows and
+    // offset parts, the omega column's theta window and offset part, and
+    // the control record (s_meta: [0] representatives, [1] theta window,
+    // [2] offset part, [3] iteration | incremental << 31, or all ones once
+    // stopped).
     int any = 0;
-    for (uint32_t e = tid; e < nw; e += bd) {
-        const bword v = a.active[wbase + e];
-        act[e] = v;
-        any |= (v != 0);
+    for (uint32_t e0 = tid; e0 < nw; e0 += 2 * bd) {
+        const uint32_t e1 = e0 + bd;
+        const bword v0 = a.active[wbase + e0];
+        const bword v1 = e1 < nw ? a.active[wbase + e1] : 0u;
+        act[e0] = v0;
+        if (e1 < nw) act[e1] = v1;
+        any |= (v0 | v1) != 0;
     }
     if (tid < 32) {
-        // Representatives in increasing acceleration order (warp ballot).
         uint32_t n = 0;
         for (uint32_t base = 0; base < ma; base += 32) {
             const uint32_t ja = base + lane;
-            const bool is_rep = ja < ma && a.xrep[pcol + ja] == ja && a.wt[i3 * ma + ja] != kReject;
+            uint32_t we = kReject, ov = 0;
+            bool is_rep = false;
+            if (ja < ma) {
+                we = a.wt[i3 * ma + ja];
+                ov = a.offv[i3 * ma + ja];
+                is_rep = a.xrep[pcol + ja] == ja && we != kReject;
+            }
             const uint32_t m = __ballot_sync(0xFFFFFFFFu, is_rep);
-            if (is_rep) reps[n + __popc(m & ((1u << lane) - 1))] = ja;
+            if (is_rep) {
+                const uint32_t k = n + __popc(m & ((1u << lane) - 1));
+                reps[k] = ja;
+                repw[k] = we;
+                repo[k] = ov;
+            }
             n += __popc(m);
         }
-        if (lane == 0) *s_nrep = n;
+        if (lane == 0) s_meta[0] = n;
+    }
+    if (tid == (bd > 32 ? 32u : 0u)) {
+        // After the first iteration, every active state failed every input
+        // in the previous one, and D' only loses cells, so a state can newly
+        // pass only if its box holds a cell that left D' in the previous
+        // iteration.  When that iteration added few states (at most one per
+        // kIncrementalRows x-rows; a new state touches the items of about
+        // that many rows), the iteration runs incrementally (phase B).
+        const uint32_t stop = fc->stop, it = fc->iter, last = fc->last_new;
+        const bool inc = it > 0 && static_cast<unsigned long long>(last) * kIncrementalRows <= g.rows;
+        s_meta[1] = a.zt[i2 * mw + jw];
+        s_meta[2] = a.offz[i2 * mw + jw];
+        s_meta[3] = stop ? 0xFFFFFFFFu : (it | (inc ? 0x80000000u : 0u));
     }
     any = __syncthreads_or(any);
-    const uint32_t nrep = *s_nrep;
-    if (!any || nrep == 0) return;
-
-    // After the first iteration, every active state failed every input in
-    // the previous one, and D' only loses cells, so a state can newly pass
-    // only if its box holds a cell that left D' in the previous iteration.
-    // When that iteration added few states (at most one per
-    // kIncrementalRows x-rows; a new state touches the items of about that
-    // many rows), the rows that lost a cell (rowlost, from the finalize
-    // kernel) are gathered per representative over its (theta, v) window,
-    // and a block with none, or a (representative, row) item whose y range
-    // has none, is skipped: its states still fail.
-    const uint32_t ze = a.zt[i2 * mw + jw];
+    const uint32_t nrep = s_meta[0], ctl = s_meta[3];
+    if (ctl == 0xFFFFFFFFu || !any || nrep == 0) return;
+    const uint32_t it = ctl & 0x7FFFFFFFu;
+    const bool incremental = (ctl >> 31) != 0;
+    const uint32_t ze = s_meta[1], offz = s_meta[2];
     const uint32_t lz = lo16(ze), hz = hi16(ze);
     const uint32_t nz = (lz <= hz) ? hz - lz + 1 : n2 - lz + hz + 1;
-    const uint32_t kslot = a.kidx[nz];
-    const uint32_t it = fc->iter;
-    const bool incremental = it > 0 && a.stats[kStatsCols * it] * kIncrementalRows <= g.rows;
+
+    // B. A second round, all in flight together: the dilated D' (and valid)
+    // rows at each representative's (theta, v) box corner, its class records
+    // and y tables, copied asynchronously into shared memory; and, in an
+    // incremental iteration, the rows of each representative's (theta, v)
+    // window that lost a cell (rowlost, from the finalize kernel).  A block
+    // with none, or a (representative, row) item whose y range has none, is
+    // skipped: its states still fail.
+    for (uint32_t e = tid; e < nrep * nw; e += bd) {
+        const uint32_t r = fdiv(e, g.magic_nw), rem = e - r * nw;
+        const uint32_t off = offz + repo[r] + rem;
+        cp_async4(Eall + r * nw * nv + rem, a.dzw + off);
+        if (NV) cp_async4(Eall + r * nw * nv + nw + rem, a.vzw + off);
+    }
+    for (uint32_t r = tid >> 5; r < nrep; r += bd >> 5) {
+        const uint64_t pl = pcol + reps[r];
+        for (uint32_t e = lane; e < cw; e += 32) cp_async4(cls + r * cw + e, a.xcls + pl * cw + e);
+        for (uint32_t e = lane; e < n1; e += 32) cp_async4(yts + r * n1 + e, a.yt + pl * n1 + e);
+    }
+    int lost = 0;
     if (incremental) {
         const uint32_t* rl = a.rowlost + (it & 1) * a.rl_words;
-        int lost = 0;
         for (uint32_t e = tid; e < nrep * W1; e += bd) {
             const uint32_t r = e / W1, yw = e - r * W1;
-            const uint32_t we = a.wt[i3 * ma + reps[r]];
+            const uint32_t we = repw[r];
             uint32_t m = 0, z = lz;
             for (uint32_t i = 0; i < nz; ++i) {
                 for (uint32_t v = lo16(we); v <= hi16(we); ++v) {
@@ -231,24 +282,14 @@ __device__ __forceinline__ void sat_col_task(const GridInfo& g, const FusedFixAr
             rowchg[r * W1 + yw] = m;
             lost |= m != 0;
         }
-        if (!__syncthreads_or(lost)) return;
     }
-    // B. dilated D' rows at each representative's (theta, v) box corner.
-    for (uint32_t e = tid; e < nrep * nw; e += bd) {
-        const uint32_t r = fdiv(e, g.magic_nw), rem = e - r * nw;
-        const uint32_t we = a.wt[i3 * ma + reps[r]];
-        const uint32_t lw = lo16(we), nwb = hi16(we) - lw + 1;
-        const uint32_t off = (kslot * a.nl + a.lidx[nwb]) * pos + n1 * (lz + n2 * lw) * W + rem;
-        Eall[r * nw * nv + rem] = __ldg(a.dzw + off);
-        if (NV) Eall[r * nw * nv + nw + rem] = __ldg(a.vzw + off);
+    cp_async_wait_all();
+    if (incremental) {
+        if (!__syncthreads_or(lost)) return;
+    } else {
+        __syncthreads();
     }
     if (tid == 0) atomicAdd(a.stats + kStatsCols * (it + 1) + 3, static_cast<unsigned long long>(nrep));
-    for (uint32_t r = tid >> 5; r < nrep; r += bd >> 5) {
-        const uint64_t pl = pcol + reps[r];
-        for (uint32_t e = lane; e < cw; e += 32) cls[r * cw + e] = __ldg(a.xcls + pl * cw + e);
-        for (uint32_t e = lane; e < n1; e += 32) yts[r * n1 + e] = __ldg(a.yt + pl * n1 + e);
-    }
-    __syncthreads();
     // C. the (representative, row) items.
     unsigned long long ntest = 0;
     for (uint32_t e = tid; e < nrep * n1; e += bd) {
@@ -357,7 +398,7 @@ __device__ __forceinline__ void sat_col_task(const GridInfo& g, const FusedFixAr
         if (got) atomicOr(a.hit + wbase + e, got);
     }
     for (int off = 16; off > 0; off >>= 1) ntest += __shfl_down_sync(0xFFFFFFFFu, ntest, off);
-    if ((tid & 31) == 0 && ntest) atomicAdd(a.stats + kStatsCols * (fc->iter + 1) + 2, ntest);
+    if ((tid & 31) == 0 && ntest) atomicAdd(a.stats + kStatsCols * (it + 1) + 2, ntest);
 }
 
 // Apply the iteration's hits to word e and build next iteration's D';
@@ -415,6 +456,7 @@ __device__ __forceinline__ void control_step(FixControl* fc, unsigned long long*
     fc->certified += tnc;
     fc->reachable += tnr;
     fc->iter = it;
+    fc->last_new = tnr > 0xFFFFFFFFull ? 0xFFFFFFFFu : static_cast<uint32_t>(tnr);
     if (fc->certified == fc->candidate_count) {
         fc->converged = 1;
         fc->message = 1;

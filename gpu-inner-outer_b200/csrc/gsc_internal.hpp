@@ -114,6 +114,8 @@ struct gsc_problem {
     gsc_b200::bword *dzw = nullptr, *vzw = nullptr;
     uint32_t* rowlost = nullptr;
     uint32_t rl_words = 0;
+    uint32_t* offz = nullptr;   // per omega column and theta cell: part of a dilated row's offset
+    uint32_t* offv = nullptr;   // per acceleration and v cell: the other part
     uint8_t *kidx = nullptr, *lidx = nullptr;
     gsc_b200::DilateArgs dil{};
     int need_valid = 0;

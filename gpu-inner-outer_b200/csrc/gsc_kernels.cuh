@@ -151,6 +151,11 @@ struct FusedFixArgs {
     const uint8_t* lidx;       // [n3 + 1]: v width -> its slot in dil.lval
     uint32_t nl;
     DilateArgs dil;
+    // Word offset of a representative's dilated D' row 0 in dzw, split into
+    // a part per omega column and theta cell and a part per acceleration and
+    // v cell (sums modulo 2^32, as dzw offsets are 32-bit):
+    const uint32_t* offz;      // [n2 * mw]: kslot * nl * rows * W + n1 * lz * W
+    const uint32_t* offv;      // [n3 * ma]: lslot * rows * W + n1 * n2 * lw * W
     cudaGraphConditionalHandle cond;
     int use_cond;
 };
@@ -261,6 +266,9 @@ cudaError_t launch_x_classes(const GridInfo& g, const uint32_t* xt, bword* xcls,
 cudaError_t launch_plane_reps(const GridInfo& g, const uint32_t* xt, const uint32_t* yt, const uint32_t* wt,
                               uint8_t* xrep, uint32_t* max_reps, cudaStream_t st);
 cudaError_t launch_fused_init(const GridInfo& g, const FusedFixArgs& a, const uint8_t* cand, cudaStream_t st);
+// The offz / offv tables of a problem (after its plan: kidx, lidx, nl).
+cudaError_t launch_sat_offsets(const GridInfo& g, const uint32_t* zt, const uint32_t* wt, const uint8_t* kidx,
+                               const uint8_t* lidx, uint32_t nl, uint32_t* offz, uint32_t* offv, cudaStream_t st);
 cudaError_t launch_fused_iteration(const GridInfo& g, const FusedFixArgs& a, cudaStream_t st, uint32_t* launches,
                                    cudaEvent_t* ev = nullptr);
 
