@@ -95,11 +95,17 @@ __device__ __forceinline__ void dilate_position(const GridInfo& g, const bword* 
     const uint32_t z = q % n2, v = q / n2;
     const uint32_t lfit = min(lmax, n3 - v);   // v windows that stay inside the grid
     if (lost) {
+        // Every bit of the window is read (no early exit), so the loads of
+        // several theta cells are in flight together.
         uint32_t hit = 0, zz = z;
-        for (uint32_t i = 0; i < kmax && !hit; ++i) {
-            for (uint32_t j = 0; j < lfit; ++j) {
-                const uint32_t rr = y + n1 * (zz + n2 * (v + j));
-                hit |= (lost[rr >> 5] >> (rr & 31)) & 1u;
+#pragma unroll 4
+        for (uint32_t i = 0; i < kmax; ++i) {
+#pragma unroll
+            for (uint32_t j = 0; j < kMaxDilate; ++j) {
+                if (j < lfit) {
+                    const uint32_t rr = y + n1 * (zz + n2 * (v + j));
+                    hit |= (lost[rr >> 5] >> (rr & 31)) & 1u;
+                }
             }
             zz = (zz + 1 == n2) ? 0 : zz + 1;
         }
@@ -109,6 +115,7 @@ __device__ __forceinline__ void dilate_position(const GridInfo& g, const bword* 
 #pragma unroll
     for (uint32_t j = 0; j < kMaxDilate; ++j) zor[j] = 0;
     uint32_t ki = 0, zz = z;
+#pragma unroll 2
     for (uint32_t i = 0; i < kmax; ++i) {
 #pragma unroll
         for (uint32_t j = 0; j < kMaxDilate; ++j)
@@ -426,12 +433,23 @@ __device__ __forceinline__ void finalize_word(const GridInfo& g, const FusedFixA
         const uint64_t sbase = r * g.n[0] + (e - r * g.W) * kBits;
         bword m = h;
         while (m) {
-            const uint32_t b = __ffs(m) - 1;
-            m &= m - 1;
-            const uint64_t s = sbase + b;
-            a.controller[s] = a.best[s];
-            a.best[s] = kInvalid32;
-            if (!((c >> b) & 1u)) a.reach_step[s] = it;
+            // Four states at a time: their best[] loads in flight together.
+            uint32_t b[4], j[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                b[k] = m ? static_cast<uint32_t>(__ffs(m) - 1) : kBits;
+                m &= m - 1;
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k) j[k] = b[k] < kBits ? a.best[sbase + b[k]] : kInvalid32;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                if (b[k] >= kBits) continue;
+                const uint64_t s = sbase + b[k];
+                a.controller[s] = j[k];
+                a.best[s] = kInvalid32;
+                if (!((c >> b[k]) & 1u)) a.reach_step[s] = it;
+            }
         }
     }
 }
@@ -450,21 +468,28 @@ __device__ __forceinline__ void add_counters(unsigned long long* row, unsigned l
 
 // The stop rules after iteration `it` (reachability.hpp:133-144), by one
 // thread once every counter of the iteration is in.
+// Its loads are one round, from L2 (where the other blocks' counter atomics
+// were performed).
 __device__ __forceinline__ void control_step(FixControl* fc, unsigned long long* row, uint32_t it) {
-    const unsigned long long tnr = atomicAdd(row, 0ull);
-    const unsigned long long tnc = atomicAdd(row + 1, 0ull);
-    fc->certified += tnc;
-    fc->reachable += tnr;
+    const unsigned long long tnr = __ldcg(row);
+    const unsigned long long tnc = __ldcg(row + 1);
+    const unsigned long long certified = __ldcg(&fc->certified) + tnc;
+    const unsigned long long reachable = __ldcg(&fc->reachable) + tnr;
+    const unsigned long long candidates = __ldcg(&fc->candidate_count);
+    const uint32_t max_iterations = __ldcg(&fc->max_iterations);
+    const uint32_t stats_cap = __ldcg(&fc->stats_cap);
+    fc->certified = certified;
+    fc->reachable = reachable;
     fc->iter = it;
     fc->last_new = tnr > 0xFFFFFFFFull ? 0xFFFFFFFFu : static_cast<uint32_t>(tnr);
-    if (fc->certified == fc->candidate_count) {
+    if (certified == candidates) {
         fc->converged = 1;
         fc->message = 1;
         fc->stop = 1;
     } else if (tnr == 0 && tnc == 0) {
         fc->message = 2;
         fc->stop = 1;
-    } else if (it >= fc->max_iterations || it + 1 >= fc->stats_cap) {
+    } else if (it >= max_iterations || it + 1 >= stats_cap) {
         fc->message = 3;
         fc->stop = 1;
     }
