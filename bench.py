@@ -60,6 +60,8 @@ def parse():
     ap.add_argument("--rates", type=str, default="0.5,0.75,0.9",
                     help="Poisson arrival rates as fractions of the measured saturation throughput")
     ap.add_argument("--serve-budget-gb", type=float, default=24.0)
+    ap.add_argument("--sat-warp-tasks", type=int, default=0, choices=[0, 1],
+                    help="served: one satisfaction task per warp in the serving loop's batched steps")
     ap.add_argument("--host-loop", action="store_true",
                     help="batched: iterate from the host instead of one CUDA graph (for per-kernel profiling)")
     ap.add_argument("--trajectories", type=int, default=1 << 20)
@@ -496,7 +498,8 @@ def bench_served(args):
         lat = [(submit_t[i] - arrivals[i]) * 1e3 + server_lat[i] for i in range(n)]
         return total, lat
 
-    srv = G.Server(ctx, memory_budget=int(args.serve_budget_gb * (1 << 30)), max_slots=256)
+    srv = G.Server(ctx, memory_budget=int(args.serve_budget_gb * (1 << 30)), max_slots=256,
+                   sat_warp_tasks=bool(args.sat_warp_tasks))
     # warm-up: a few queries of each model
     warm = [srv.submit(absn[k], C.random_query(models[k], args.seed + 1, i)) for i, k in enumerate(names * 4)]
     for t in warm:
@@ -545,7 +548,8 @@ def bench_served(args):
         "vs_baseline": None, "dtype": "u32 bit-sliced sets / int32 counts (f64 boxes)", "data": "synthetic",
         "config": {"workload": f"served_{n}_queries_3_models_seed{args.seed}",
                    "models": {k: models[k]["name"] for k in names}, "queries": n,
-                   "budget_gb": args.serve_budget_gb, "result_buffers_in_flight": depth},
+                   "budget_gb": args.serve_budget_gb, "result_buffers_in_flight": depth,
+                   "sat_warp_tasks": args.sat_warp_tasks},
         "saturation": {"throughput_qps": X, "p50_ms": percentile(sat_lat, 50), "p99_ms": percentile(sat_lat, 99)},
         "rates": rates,
         "e2e": {"value": X, "unit": "queries/s", "h2d_bytes_per_step": 0,

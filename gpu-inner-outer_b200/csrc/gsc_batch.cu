@@ -183,11 +183,17 @@ int enqueue_iterations(gsc_batch* b, uint32_t count, uint32_t* launches) {
 }
 
 // Time `reps` iterations from a fresh start under each candidate shape;
-// keep the fastest.
+// keep the fastest.  Candidates: one task per block (64 / 128 / 256
+// threads) and one task per warp (4 or 8 warps a block), each with one
+// block per task or a persistent grid, and two chunk sizes; a warp shape
+// whose staging does not fit a block's shared memory is left out.
 int autotune(gsc_batch* b) {
     gsc_context* ctx = b->ctx;
     const int sms = sm_count(ctx);
-    const uint32_t threads[] = {64, 128, 256};
+    struct Trial {
+        uint32_t threads, warp;
+    };
+    const Trial trials[] = {{64, 0}, {128, 0}, {256, 0}, {128, 1}, {256, 1}};
     const uint32_t per_sm[] = {0, 4, 8, 16};
     const uint32_t chunks[] = {1024, 4096};
     const uint32_t reps = 4;
@@ -200,9 +206,11 @@ int autotune(gsc_batch* b) {
     for (uint32_t ch : chunks) {
         status = upload_list(b, ch);
         if (status != GSC_OK) break;
-        for (uint32_t th : threads) {
+        for (const Trial& tr : trials) {
             for (uint32_t ps : per_sm) {
-                b->shape = BatchShape{th, ps * static_cast<uint32_t>(sms), ch};
+                const BatchShape cand{tr.threads, ps * static_cast<uint32_t>(sms), ch, tr.warp};
+                if (batch_sat_smem(cand, b->smem) > kFusedSmemMax) continue;
+                b->shape = cand;
                 cudaError_t e = launch_batch_init(b->ddesc, b->wl, b->tot, sms, ctx->stream);
                 if (e == cudaSuccess) e = cudaEventRecord(e0, ctx->stream);
                 for (uint32_t r = 0; e == cudaSuccess && r < reps; ++r)
@@ -357,10 +365,13 @@ int batch_create(gsc_batch* b, uint32_t count, const gsc_model_desc* models, con
     b->shape.sat_threads = (opt && opt->sat_threads) ? opt->sat_threads : 128;
     b->shape.sat_blocks = (opt ? opt->sat_blocks_per_sm : 0) * static_cast<uint32_t>(sms);
     b->shape.chunk = (opt && opt->chunk_words) ? opt->chunk_words : 2048;
+    b->shape.warp = (opt && opt->sat_warp_tasks) ? 1u : 0u;
     if (b->shape.sat_threads != 64 && b->shape.sat_threads != 128 && b->shape.sat_threads != 256)
         return fail(ctx, GSC_ERR_INVALID_ARGUMENT, "sat_threads must be 64, 128 or 256");
     if (b->shape.chunk < 256 || b->shape.chunk % 256)
         return fail(ctx, GSC_ERR_INVALID_ARGUMENT, "chunk_words must be a positive multiple of 256");
+    if (batch_sat_smem(b->shape, smem) > kFusedSmemMax)
+        return fail(ctx, GSC_ERR_UNSUPPORTED, "batch: one task per warp needs more shared memory than a block has");
     GSC_TRY(upload_list(b, b->shape.chunk));
     b->t.tuned = 0;
     if (opt && opt->autotune && !b->small.empty()) {
@@ -492,6 +503,7 @@ int gsc_batch_timings(gsc_batch* b, gsc_batch_report* out) {
     const int sms = sm_count(ctx);
     b->t.sat_blocks_per_sm = b->shape.sat_blocks / static_cast<uint32_t>(sms);
     b->t.chunk_words = b->shape.chunk;
+    b->t.sat_warp_tasks = b->shape.warp;
     uint64_t held = b->own_bytes;
     for (const auto& a : b->abs) held += a->bytes;
     for (const auto& p : b->probs) held += p->bytes;

@@ -75,26 +75,41 @@ __global__ void __launch_bounds__(256) k_batch_dilate(const InstanceDesc* __rest
 }
 
 // The instance of the current task is copied to shared memory when it
-// changes; the dynamic shared memory holds the largest instance's staging.
-template <int WMAX>
-__global__ void __launch_bounds__(256) k_batch_sat(const InstanceDesc* __restrict__ descs, WorkList wl) {
+// changes; the dynamic shared memory holds the largest instance's staging,
+// once per task group.  WARP: every warp of the block walks the task list
+// as its own group (tasks blockIdx.x * warps + warp, step gridDim.x *
+// warps), else the block is one group.
+template <int WMAX, bool WARP>
+__global__ void __launch_bounds__(256) k_batch_sat(const InstanceDesc* __restrict__ descs, WorkList wl,
+                                                   uint32_t task_words) {
     extern __shared__ __align__(16) bword smem[];
-    __shared__ __align__(16) InstanceDesc sd;
-    __shared__ uint32_t s_meta[4];
+    constexpr uint32_t kGroups = WARP ? 8u : 1u;
+    __shared__ __align__(16) InstanceDesc sd[kGroups];
+    __shared__ uint32_t s_meta[kGroups][4];
     const uint32_t total = wl.sat_off[wl.n];
+    const uint32_t grp = WARP ? (threadIdx.x >> 5) : 0u;
+    const uint32_t ngrp = WARP ? (blockDim.x >> 5) : 1u;
+    const uint32_t rank = WARP ? (threadIdx.x & 31u) : threadIdx.x;
+    const uint32_t gsize = WARP ? 32u : blockDim.x;
+    bword* gsm = smem + grp * task_words;
     uint32_t cur = 0xFFFFFFFFu;
-    for (uint32_t t = blockIdx.x; t < total; t += gridDim.x) {
+    bool stopped = false;
+    for (uint32_t t = blockIdx.x * ngrp + grp; t < total; t += gridDim.x * ngrp) {
         const uint32_t k = find_task(wl.sat_off, wl.n, t);
         const uint32_t slot = wl.slot[k];
         if (slot != cur) {
             const uint32_t* src = reinterpret_cast<const uint32_t*>(descs + slot);
-            uint32_t* dst = reinterpret_cast<uint32_t*>(&sd);
-            for (uint32_t i = threadIdx.x; i < sizeof(InstanceDesc) / 4; i += blockDim.x) dst[i] = src[i];
-            __syncthreads();
+            uint32_t* dst = reinterpret_cast<uint32_t*>(&sd[grp]);
+            for (uint32_t i = rank; i < sizeof(InstanceDesc) / 4; i += gsize) dst[i] = src[i];
+            group_sync<WARP>();
             cur = slot;
+            // An instance's stop flag changes only in the finalize kernel, so
+            // the tasks of a stopped instance are skipped without a look.
+            stopped = __ldcg(&sd[grp].a.fc->stop) != 0;
         }
-        sat_col_task<WMAX, false, 2>(sd.g, sd.a, t - wl.sat_off[k], smem, s_meta);
-        __syncthreads();
+        if (stopped) continue;
+        sat_col_task<WMAX, false, 2, WARP>(sd[grp].g, sd[grp].a, t - wl.sat_off[k], gsm, s_meta[grp]);
+        group_sync<WARP>();
     }
 }
 
@@ -154,7 +169,7 @@ inline unsigned int grid_of(uint32_t tasks, uint32_t cap) {
     return b ? b : 1u;
 }
 
-template <int WMAX>
+template <int WMAX, bool WARP>
 cudaError_t launch_sat_t(const InstanceDesc* descs, const WorkList& wl, const WorkTotals& tot, const BatchShape& sh,
                          size_t smem, cudaStream_t st) {
     // Launches may come from several host threads (a server's loop and the
@@ -164,19 +179,27 @@ cudaError_t launch_sat_t(const InstanceDesc* descs, const WorkList& wl, const Wo
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= 64 || !configured[dev].load()) {
-        e = cudaFuncSetAttribute(k_batch_sat<WMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        e = cudaFuncSetAttribute(k_batch_sat<WMAX, WARP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(kFusedSmemMax));
         if (e != cudaSuccess) return e;
         if (dev >= 0 && dev < 64) configured[dev].store(true);
     }
-    const uint32_t blocks = sh.sat_blocks ? grid_of(tot.sat, sh.sat_blocks) : grid_of(tot.sat, 0xFFFFFFFFu);
-    k_batch_sat<WMAX><<<blocks, sh.sat_threads, smem, st>>>(descs, wl);
+    const uint32_t per_block = WARP ? sh.sat_threads / 32 : 1u;
+    const uint32_t tasks = (tot.sat + per_block - 1) / per_block;
+    const uint32_t blocks = sh.sat_blocks ? grid_of(tasks, sh.sat_blocks) : grid_of(tasks, 0xFFFFFFFFu);
+    k_batch_sat<WMAX, WARP><<<blocks, sh.sat_threads, batch_sat_smem(sh, smem), st>>>(
+        descs, wl, static_cast<uint32_t>(smem / sizeof(bword)));
     return cudaGetLastError();
 }
 
-}  // namespace
+template <int WMAX>
+cudaError_t launch_sat_w(const InstanceDesc* descs, const WorkList& wl, const WorkTotals& tot, const BatchShape& sh,
+                         size_t smem, cudaStream_t st) {
+    return sh.warp ? launch_sat_t<WMAX, true>(descs, wl, tot, sh, smem, st)
+                   : launch_sat_t<WMAX, false>(descs, wl, tot, sh, smem, st);
+}
 
-size_t batch_sat_static_smem() { return sizeof(InstanceDesc) + 16; }
+}  // namespace
 
 cudaError_t launch_batch_init(const InstanceDesc* descs, const WorkList& wl, const WorkTotals& tot, int sms,
                               cudaStream_t st) {
@@ -189,7 +212,7 @@ cudaError_t launch_batch_step(const InstanceDesc* descs, const WorkList& small, 
                               const WorkList& all, const BigInstance* big, uint32_t nbig, const BatchShape& sh,
                               uint32_t wmax, size_t smem, int sms, cudaGraphConditionalHandle cond, int use_cond,
                               cudaStream_t st, uint32_t* launches) {
-    if (sh.sat_threads < 32 || sh.sat_threads > 256 || sh.sat_threads % 32 || smem > kFusedSmemMax)
+    if (sh.sat_threads < 32 || sh.sat_threads > 256 || sh.sat_threads % 32 || batch_sat_smem(sh, smem) > kFusedSmemMax)
         return cudaErrorInvalidValue;
     uint32_t n = 0;
     cudaError_t e = cudaSuccess;
@@ -202,11 +225,11 @@ cudaError_t launch_batch_step(const InstanceDesc* descs, const WorkList& small, 
     }
     if (e == cudaSuccess && tot_small.sat) {
         switch (wmax) {
-            case 1: e = launch_sat_t<1>(descs, small, tot_small, sh, smem, st); break;
-            case 2: e = launch_sat_t<2>(descs, small, tot_small, sh, smem, st); break;
+            case 1: e = launch_sat_w<1>(descs, small, tot_small, sh, smem, st); break;
+            case 2: e = launch_sat_w<2>(descs, small, tot_small, sh, smem, st); break;
             case 3:
-            case 4: e = launch_sat_t<4>(descs, small, tot_small, sh, smem, st); break;
-            default: e = launch_sat_t<8>(descs, small, tot_small, sh, smem, st); break;
+            case 4: e = launch_sat_w<4>(descs, small, tot_small, sh, smem, st); break;
+            default: e = launch_sat_w<8>(descs, small, tot_small, sh, smem, st); break;
         }
         ++n;
     }

@@ -146,6 +146,25 @@ __device__ __forceinline__ void cp_async4(void* smem_dst, const void* gmem_src) 
 
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
+// The group that runs one satisfaction task: the whole block, or one warp
+// (WARP), with its barrier and its barrier-with-OR.
+template <bool WARP>
+__device__ __forceinline__ void group_sync() {
+    if (WARP)
+        __syncwarp();
+    else
+        __syncthreads();
+}
+
+template <bool WARP>
+__device__ __forceinline__ int group_sync_or(int p) {
+    if (WARP) {
+        __syncwarp();
+        return __any_sync(0xFFFFFFFFu, p);
+    }
+    return __syncthreads_or(p);
+}
+
 // One (theta, v) slice x omega column jw (task = slice * mw + jw) of the
 // satisfaction test, by the whole block:
 //  B. per representative acceleration (the lowest of each group of inputs
@@ -161,10 +180,15 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 //     (atomicMin, so the lowest over all columns wins) and the hit bit is set.
 // WMAX: register words per row; EXACTW: g.W == WMAX (else g.W <= WMAX at run
 // time).  NVMODE: 0 / 1 = validity test off / on, 2 = a.need_valid decides.
-// Every early return is taken by the whole block.
+// WARP: the task is one warp's (its own smem and s_meta), else the block's.
+// Every early return is taken by the whole group.
 constexpr unsigned long long kIncrementalRows = 16;
+// An incremental iteration after one that added at most one state per
+// kSparseRows x-rows: most blocks find no lost row, so a block tests its
+// windows before it stages anything.
+constexpr unsigned long long kSparseRows = 128;
 
-template <int WMAX, bool EXACTW, int NVMODE>
+template <int WMAX, bool EXACTW, int NVMODE, bool WARP = false>
 __device__ __forceinline__ void sat_col_task(const GridInfo& g, const FusedFixArgs& a, uint32_t task,
                                              bword* smem, uint32_t* s_meta) {
     const FixControl* fc = a.fc;
@@ -175,7 +199,8 @@ __device__ __forceinline__ void sat_col_task(const GridInfo& g, const FusedFixAr
     const uint32_t slice = task / mw, jw = task - slice * mw;
     const uint32_t i2 = slice % n2, i3 = slice / n2;
     const uint64_t wbase = static_cast<uint64_t>(slice) * nw;
-    const uint32_t tid = threadIdx.x, bd = blockDim.x;
+    const uint32_t tid = WARP ? (threadIdx.x & 31u) : threadIdx.x;
+    const uint32_t bd = WARP ? 32u : blockDim.x;
     const uint32_t lane = tid & 31;
     const uint32_t nv = NV ? 2u : 1u;
     const uint32_t cw = a.cls_words;
@@ -198,8 +223,8 @@ __device__ __forceinline__ void sat_col_task(const GridInfo& g, const FusedFixAr
     // increasing acceleration order (warp ballot) with their v windows and
     // offset parts, the omega column's theta window and offset part, and
     // the control record (s_meta: [0] representatives, [1] theta window,
-    // [2] offset part, [3] iteration | incremental << 31, or all ones once
-    // stopped).
+    // [2] offset part, [3] iteration | incremental << 31 | sparse << 30, or
+    // all ones once stopped).
     int any = 0;
     for (uint32_t e0 = tid; e0 < nw; e0 += 2 * bd) {
         const uint32_t e1 = e0 + bd;
@@ -240,15 +265,17 @@ __device__ __forceinline__ void sat_col_task(const GridInfo& g, const FusedFixAr
         // that many rows), the iteration runs incrementally (phase B).
         const uint32_t stop = fc->stop, it = fc->iter, last = fc->last_new;
         const bool inc = it > 0 && static_cast<unsigned long long>(last) * kIncrementalRows <= g.rows;
+        const bool sparse = inc && static_cast<unsigned long long>(last) * kSparseRows <= g.rows;
         s_meta[1] = a.zt[i2 * mw + jw];
         s_meta[2] = a.offz[i2 * mw + jw];
-        s_meta[3] = stop ? 0xFFFFFFFFu : (it | (inc ? 0x80000000u : 0u));
+        s_meta[3] = stop ? 0xFFFFFFFFu : (it | (inc ? 0x80000000u : 0u) | (sparse ? 0x40000000u : 0u));
     }
-    any = __syncthreads_or(any);
+    any = group_sync_or<WARP>(any);
     const uint32_t nrep = s_meta[0], ctl = s_meta[3];
     if (ctl == 0xFFFFFFFFu || !any || nrep == 0) return;
-    const uint32_t it = ctl & 0x7FFFFFFFu;
+    const uint32_t it = ctl & 0x3FFFFFFFu;
     const bool incremental = (ctl >> 31) != 0;
+    const bool sparse = ((ctl >> 30) & 1u) != 0;
     const uint32_t ze = s_meta[1], offz = s_meta[2];
     const uint32_t lz = lo16(ze), hz = hi16(ze);
     const uint32_t nz = (lz <= hz) ? hz - lz + 1 : n2 - lz + hz + 1;
@@ -259,18 +286,22 @@ __device__ __forceinline__ void sat_col_task(const GridInfo& g, const FusedFixAr
     // incremental iteration, the rows of each representative's (theta, v)
     // window that lost a cell (rowlost, from the finalize kernel).  A block
     // with none, or a (representative, row) item whose y range has none, is
-    // skipped: its states still fail.
-    for (uint32_t e = tid; e < nrep * nw; e += bd) {
-        const uint32_t r = fdiv(e, g.magic_nw), rem = e - r * nw;
-        const uint32_t off = offz + repo[r] + rem;
-        cp_async4(Eall + r * nw * nv + rem, a.dzw + off);
-        if (NV) cp_async4(Eall + r * nw * nv + nw + rem, a.vzw + off);
-    }
-    for (uint32_t r = tid >> 5; r < nrep; r += bd >> 5) {
-        const uint64_t pl = pcol + reps[r];
-        for (uint32_t e = lane; e < cw; e += 32) cp_async4(cls + r * cw + e, a.xcls + pl * cw + e);
-        for (uint32_t e = lane; e < n1; e += 32) cp_async4(yts + r * n1 + e, a.yt + pl * n1 + e);
-    }
+    // skipped: its states still fail.  In a sparse iteration the windows are
+    // tested first and only a block with a lost row stages its rows.
+    auto stage = [&]() {
+        for (uint32_t e = tid; e < nrep * nw; e += bd) {
+            const uint32_t r = fdiv(e, g.magic_nw), rem = e - r * nw;
+            const uint32_t off = offz + repo[r] + rem;
+            cp_async4(Eall + r * nw * nv + rem, a.dzw + off);
+            if (NV) cp_async4(Eall + r * nw * nv + nw + rem, a.vzw + off);
+        }
+        for (uint32_t r = tid >> 5; r < nrep; r += bd >> 5) {
+            const uint64_t pl = pcol + reps[r];
+            for (uint32_t e = lane; e < cw; e += 32) cp_async4(cls + r * cw + e, a.xcls + pl * cw + e);
+            for (uint32_t e = lane; e < n1; e += 32) cp_async4(yts + r * n1 + e, a.yt + pl * n1 + e);
+        }
+    };
+    if (!sparse) stage();
     int lost = 0;
     if (incremental) {
         const uint32_t* rl = a.rowlost + (it & 1) * a.rl_words;
@@ -290,11 +321,18 @@ __device__ __forceinline__ void sat_col_task(const GridInfo& g, const FusedFixAr
             lost |= m != 0;
         }
     }
-    cp_async_wait_all();
-    if (incremental) {
-        if (!__syncthreads_or(lost)) return;
+    if (sparse) {
+        if (!group_sync_or<WARP>(lost)) return;
+        stage();
+        cp_async_wait_all();
+        group_sync<WARP>();
     } else {
-        __syncthreads();
+        cp_async_wait_all();
+        if (incremental) {
+            if (!group_sync_or<WARP>(lost)) return;
+        } else {
+            group_sync<WARP>();
+        }
     }
     if (tid == 0) atomicAdd(a.stats + kStatsCols * (it + 1) + 3, static_cast<unsigned long long>(nrep));
     // C. the (representative, row) items.
@@ -380,7 +418,7 @@ __device__ __forceinline__ void sat_col_task(const GridInfo& g, const FusedFixAr
         for (int w = 0; w < WMAX; ++w)
             if (EXACTW || static_cast<uint32_t>(w) < W) sat[r * nw + i1 * W + w] = sw[w];
     }
-    __syncthreads();
+    group_sync<WARP>();
     // D. lowest satisfied input of the column per state -> best[] and hit
     // bits.  Representatives are in increasing order and each is the lowest
     // input of its group, so the first representative that satisfies a state

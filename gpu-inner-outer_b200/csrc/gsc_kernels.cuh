@@ -212,6 +212,7 @@ struct BatchShape {
     uint32_t sat_threads;   // threads per satisfaction block
     uint32_t sat_blocks;    // persistent satisfaction blocks (0 = one per task)
     uint32_t chunk;         // word positions per dilate / finalize task
+    uint32_t warp;          // 1: one satisfaction task per warp (smem per task, sat_threads / 32 of them)
 };
 
 // Host-side task counts of one list (matching WorkList's offsets).
@@ -250,7 +251,9 @@ cudaError_t launch_batch_step(const InstanceDesc* descs, const WorkList& small, 
                               const WorkList& all, const BigInstance* big, uint32_t nbig, const BatchShape& sh,
                               uint32_t wmax, size_t smem, int sms, cudaGraphConditionalHandle cond, int use_cond,
                               cudaStream_t st, uint32_t* launches);
-size_t batch_sat_static_smem();
+// Dynamic shared memory of one satisfaction block for a shape, given one
+// task's staging (smem).
+inline size_t batch_sat_smem(const BatchShape& sh, size_t smem) { return sh.warp ? (sh.sat_threads / 32) * smem : smem; }
 
 // Class record words per plane: a 16-byte header + kClassMax * W masks.
 inline uint32_t class_words(const GridInfo& g) { return 4 + kClassMax * g.W; }

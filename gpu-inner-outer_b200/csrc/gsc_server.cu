@@ -394,9 +394,11 @@ void loop(gsc_server* s) {
         }
         const uint32_t n = static_cast<uint32_t>(s->running.size());
         cudaError_t e = cudaSuccess;
+        BatchShape shape = s->shape;
+        if (batch_sat_smem(shape, smem) > kFusedSmemMax) shape.warp = 0;
         for (uint32_t i = 0; e == cudaSuccess && i < K; ++i)
             e = launch_batch_step(s->ddesc, wl_small, tot_small, wl, big.data(), static_cast<uint32_t>(big.size()),
-                                  s->shape, wmax, smem, sms, 0, 0, s->s_main, nullptr);
+                                  shape, wmax, smem, sms, 0, 0, s->s_main, nullptr);
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(s->hstatus, s->dstatus, sizeof(FixControl) * n, cudaMemcpyDeviceToHost, s->s_main);
         if (e == cudaSuccess) e = cudaEventRecord(s->ev_step, s->s_main);
@@ -489,6 +491,7 @@ int gsc_server_create(gsc_context* ctx, const gsc_server_options* options, gsc_s
     s->shape.sat_threads = o.sat_threads ? o.sat_threads : 64;
     s->shape.sat_blocks = (o.sat_blocks_per_sm ? o.sat_blocks_per_sm : 16) * static_cast<uint32_t>(sm_count(ctx));
     s->shape.chunk = o.chunk_words ? o.chunk_words : 1024;
+    s->shape.warp = o.sat_warp_tasks ? 1u : 0u;
     if (s->shape.sat_threads != 64 && s->shape.sat_threads != 128 && s->shape.sat_threads != 256)
         return fail(ctx, GSC_ERR_INVALID_ARGUMENT, "sat_threads must be 64, 128 or 256");
     if (s->shape.chunk < 256 || s->shape.chunk % 256)

@@ -88,7 +88,8 @@ class Timings(ctypes.Structure):
 
 class BatchOptions(ctypes.Structure):
     _fields_ = [("autotune", ctypes.c_uint32), ("sat_threads", ctypes.c_uint32),
-                ("sat_blocks_per_sm", ctypes.c_uint32), ("chunk_words", ctypes.c_uint32)]
+                ("sat_blocks_per_sm", ctypes.c_uint32), ("chunk_words", ctypes.c_uint32),
+                ("sat_warp_tasks", ctypes.c_uint32)]
 
 
 class BatchReport(ctypes.Structure):
@@ -97,14 +98,15 @@ class BatchReport(ctypes.Structure):
         ("device_bytes", ctypes.c_uint64), ("instances", ctypes.c_uint32), ("max_iterations_run", ctypes.c_uint32),
         ("kernel_launches", ctypes.c_uint32), ("sat_threads", ctypes.c_uint32),
         ("sat_blocks_per_sm", ctypes.c_uint32), ("chunk_words", ctypes.c_uint32), ("tuned", ctypes.c_uint32),
-        ("pair_tests", ctypes.c_uint64),
+        ("sat_warp_tasks", ctypes.c_uint32), ("pair_tests", ctypes.c_uint64),
     ]
 
 
 class ServerOptions(ctypes.Structure):
     _fields_ = [("memory_budget", ctypes.c_uint64), ("max_slots", ctypes.c_uint32),
                 ("iterations_per_step", ctypes.c_uint32), ("sat_threads", ctypes.c_uint32),
-                ("sat_blocks_per_sm", ctypes.c_uint32), ("chunk_words", ctypes.c_uint32)]
+                ("sat_blocks_per_sm", ctypes.c_uint32), ("chunk_words", ctypes.c_uint32),
+                ("sat_warp_tasks", ctypes.c_uint32)]
 
 
 class ServerReport(ctypes.Structure):
@@ -430,14 +432,15 @@ class Batch:
     instance, the keyword masks a Problem takes."""
 
     def __init__(self, ctx: Context, cases, autotune=False, sat_threads=0, sat_blocks_per_sm=0, chunk_words=0,
-                 masks=None):
+                 masks=None, sat_warp_tasks=False):
         self.ctx = ctx
         self._h = ctypes.c_void_p()
         n = len(cases)
         self.queries = [_Query(c, **((masks or [{}] * n)[i] or {})) for i, c in enumerate(cases)]
         self.models = (ModelDesc * n)(*[model_desc(c) for c in cases])
         self.qdescs = (QueryDesc * n)(*[q.desc for q in self.queries])
-        opt = BatchOptions(int(bool(autotune)), int(sat_threads), int(sat_blocks_per_sm), int(chunk_words))
+        opt = BatchOptions(int(bool(autotune)), int(sat_threads), int(sat_blocks_per_sm), int(chunk_words),
+                           int(bool(sat_warp_tasks)))
         ctx.check(lib().gsc_batch_create(ctx._h, n, self.models, self.qdescs, ctypes.byref(opt),
                                          ctypes.byref(self._h)))
         self.count = n
@@ -504,11 +507,11 @@ class Server:
     allocates itself."""
 
     def __init__(self, ctx: Context, memory_budget=0, max_slots=0, iterations_per_step=0, sat_threads=0,
-                 sat_blocks_per_sm=0, chunk_words=0):
+                 sat_blocks_per_sm=0, chunk_words=0, sat_warp_tasks=False):
         self.ctx = ctx
         self._h = ctypes.c_void_p()
         opt = ServerOptions(int(memory_budget), int(max_slots), int(iterations_per_step), int(sat_threads),
-                            int(sat_blocks_per_sm), int(chunk_words))
+                            int(sat_blocks_per_sm), int(chunk_words), int(bool(sat_warp_tasks)))
         ctx.check(lib().gsc_server_create(ctx._h, ctypes.byref(opt), ctypes.byref(self._h)))
         self._pending = {}
         ctx._children.add(self)

@@ -318,6 +318,9 @@ typedef struct {
     uint32_t sat_blocks_per_sm;   /* persistent satisfaction blocks per SM (0 = one block
                                      per task)                                             */
     uint32_t chunk_words;         /* word positions per dilate / finalize task (0 = 2048)  */
+    uint32_t sat_warp_tasks;      /* 1: each warp of a satisfaction block runs its own task
+                                     (sat_threads / 32 tasks per block, no block barriers);
+                                     0: the whole block runs one task                       */
 } gsc_batch_options;
 
 typedef struct {
@@ -332,6 +335,7 @@ typedef struct {
     uint32_t sat_blocks_per_sm;
     uint32_t chunk_words;
     uint32_t tuned;               /* 1 = shapes from trials, 2 = from the process cache    */
+    uint32_t sat_warp_tasks;      /* as gsc_batch_options                                  */
     uint64_t pair_tests;          /* (state, input) tests of the last solve, all instances */
 } gsc_batch_report;
 
@@ -369,6 +373,8 @@ typedef struct {
     uint32_t sat_threads;           /* as gsc_batch_options (0 = 64)                                  */
     uint32_t sat_blocks_per_sm;     /* (0 = 16)                                                       */
     uint32_t chunk_words;           /* (0 = 1024)                                                     */
+    uint32_t sat_warp_tasks;        /* as gsc_batch_options (a step whose staging would not fit runs
+                                       one task per block)                                            */
 } gsc_server_options;
 
 typedef struct {

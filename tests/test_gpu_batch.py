@@ -90,10 +90,15 @@ def test_batch_mixed_sizes_autotuned_match_solo(ctx):
     b.close()
 
 
-@pytest.mark.parametrize("shape", [(64, 0, 1024), (256, 4, 4096), (128, 16, 256)])
+@pytest.mark.parametrize("shape", [(64, 0, 1024, 0), (256, 4, 4096, 0), (128, 16, 256, 0), (128, 0, 1024, 1),
+                                   (256, 8, 2048, 1)])
 def test_batch_launch_shapes_agree(ctx, shape):
+    """Block- and warp-per-task satisfaction launches, one block per task or
+    persistent, give the golden results."""
     cases = [INDEX[n]["case"] for n in ("small_obstacles", "hyperbolic_mid_a", "wraparound", "mini_instance_2")]
-    b = G.Batch(ctx, cases, sat_threads=shape[0], sat_blocks_per_sm=shape[1], chunk_words=shape[2])
+    b = G.Batch(ctx, cases, sat_threads=shape[0], sat_blocks_per_sm=shape[1], chunk_words=shape[2],
+                sat_warp_tasks=bool(shape[3]))
+    assert b.report()["sat_warp_tasks"] == shape[3]
     b.solve(graph=bool(shape[1] % 8))
     for i, n in enumerate(("small_obstacles", "hyperbolic_mid_a", "wraparound", "mini_instance_2")):
         check_entry(b.read(i), n)

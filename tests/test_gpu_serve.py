@@ -40,9 +40,10 @@ def alone(ctx, abs_, q):
     return out
 
 
-def test_served_mix_matches_alone(ctx, models):
+@pytest.mark.parametrize("warp", [False, True], ids=["block_tasks", "warp_tasks"])
+def test_served_mix_matches_alone(ctx, models, warp):
     cases, absn = models
-    srv = G.Server(ctx, memory_budget=2 << 30, iterations_per_step=1)
+    srv = G.Server(ctx, memory_budget=2 << 30, iterations_per_step=1, sat_warp_tasks=warp)
     queries = []
     for i in range(36):
         k = ("small", "mid", "tiny")[i % 3]
