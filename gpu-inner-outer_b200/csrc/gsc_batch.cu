@@ -99,6 +99,9 @@ struct gsc_batch {
     std::vector<std::unique_ptr<gsc_problem>> probs;
     PlanRecord* hplans = nullptr;   // pinned
     uint32_t* hrunning = nullptr;   // pinned
+    FixControl* hfc = nullptr;      // pinned: every instance's control record, for reads
+    unsigned long long* hstats = nullptr;   // pinned: every instance's per-iteration counters
+    std::vector<uint64_t> stats_off;        // instance -> its first entry in hstats
     InstanceDesc* ddesc = nullptr;
     uint32_t* dlist = nullptr;       // the small instances' work list
     uint32_t* dlist_all = nullptr;   // every instance: init and status
@@ -125,6 +128,8 @@ struct gsc_batch {
         device_release_all(ctx, pool, own, own_bytes);
         if (hplans) cudaFreeHost(hplans);
         if (hrunning) cudaFreeHost(hrunning);
+        if (hfc) cudaFreeHost(hfc);
+        if (hstats) cudaFreeHost(hstats);
     }
 };
 
@@ -280,13 +285,63 @@ int build_batch_graph(gsc_batch* b) {
     return GSC_OK;
 }
 
+// Streams for the set-up of a batch's instances (instance i on stream
+// i % kSetupStreams), so that the small set-up kernels of different
+// instances run side by side.  Every exit drains and destroys them.
+struct SetupStreams {
+    static constexpr int kSetupStreams = 8;
+    cudaStream_t s[kSetupStreams] = {};
+    cudaEvent_t ev[kSetupStreams + 1] = {};
+    ~SetupStreams() {
+        for (auto x : s)
+            if (x) {
+                cudaStreamSynchronize(x);
+                cudaStreamDestroy(x);
+            }
+        for (auto e : ev)
+            if (e) cudaEventDestroy(e);
+    }
+    cudaError_t create(cudaStream_t after) {
+        for (auto& e : ev) {
+            const cudaError_t r = cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+            if (r != cudaSuccess) return r;
+        }
+        cudaError_t r = cudaEventRecord(ev[kSetupStreams], after);
+        for (auto& x : s) {
+            if (r == cudaSuccess) r = cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking);
+            if (r == cudaSuccess) r = cudaStreamWaitEvent(x, ev[kSetupStreams], 0);
+        }
+        return r;
+    }
+    cudaStream_t of(uint32_t i) const { return s[i % kSetupStreams]; }
+    cudaError_t sync() {
+        for (auto x : s) {
+            const cudaError_t r = cudaStreamSynchronize(x);
+            if (r != cudaSuccess) return r;
+        }
+        return cudaSuccess;
+    }
+    // `st` waits for everything enqueued on the set-up streams.
+    cudaError_t join(cudaStream_t st) {
+        for (int k = 0; k < kSetupStreams; ++k) {
+            cudaError_t r = cudaEventRecord(ev[k], s[k]);
+            if (r == cudaSuccess) r = cudaStreamWaitEvent(st, ev[k], 0);
+            if (r != cudaSuccess) return r;
+        }
+        return cudaSuccess;
+    }
+};
+
 int batch_create(gsc_batch* b, uint32_t count, const gsc_model_desc* models, const gsc_query_desc* queries,
                  const gsc_batch_options* opt) {
     gsc_context* ctx = b->ctx;
     cudaStream_t st = ctx->stream;
     b->pool = ctx->pool.get();
+    SetupStreams ss;
+    GSC_CU(ctx, ss.create(st));
     GSC_CU(ctx, cudaMallocHost(&b->hplans, sizeof(PlanRecord) * count));
     GSC_CU(ctx, cudaMallocHost(&b->hrunning, sizeof(uint32_t)));
+    GSC_CU(ctx, cudaMallocHost(&b->hfc, sizeof(FixControl) * count));
     std::vector<std::vector<std::pair<void*, uint64_t>>> tmp(count);
     // Stage 1 of every instance, then one wait for all plan records.
     for (uint32_t i = 0; i < count; ++i) {
@@ -300,7 +355,7 @@ int batch_create(gsc_batch* b, uint32_t count, const gsc_model_desc* models, con
         if (s != GSC_OK) return fail(ctx, s, "instance " + std::to_string(i) + ": " + err);
         if (a->g.rows * a->g.W >= 0xFFFFFFFFull)
             return fail(ctx, GSC_ERR_UNSUPPORTED, "instance " + std::to_string(i) + ": grid too large for a batch");
-        GSC_TRY(abstraction_enqueue(a.get(), st, tmp[i]));
+        GSC_TRY(abstraction_enqueue(a.get(), ss.of(i), tmp[i]));
         b->abs.push_back(std::move(a));
     }
     for (uint32_t i = 0; i < count; ++i) {
@@ -310,14 +365,14 @@ int batch_create(gsc_batch* b, uint32_t count, const gsc_model_desc* models, con
         p->abs = b->abs[i].get();
         p->g = b->abs[i]->g;
         p->pool = b->pool;
-        p->stream = st;
+        p->stream = ss.of(i);
         p->method = GSC_METHOD_FUSED;
         p->hplan = b->hplans + i;
         const int s = problem_stage1(p.get(), &queries[i]);
         if (s != GSC_OK) return fail(ctx, s, "instance " + std::to_string(i) + ": " + ctx->last_error);
         b->probs.push_back(std::move(p));
     }
-    GSC_CU(ctx, cudaStreamSynchronize(st));
+    GSC_CU(ctx, ss.sync());
     for (uint32_t i = 0; i < count; ++i) {
         uint64_t tb = 0;
         device_release_all(ctx, b->pool, tmp[i], tb);
@@ -328,6 +383,16 @@ int batch_create(gsc_batch* b, uint32_t count, const gsc_model_desc* models, con
         if (s == GSC_OK) s = problem_stage2(p);
         if (s != GSC_OK) return fail(ctx, s, "instance " + std::to_string(i) + ": " + ctx->last_error);
     }
+    // Later work on the context stream (init, solves, reads) follows the set-up.
+    GSC_CU(ctx, ss.join(st));
+    for (auto& p : b->probs) p->stream = st;
+    // Pinned staging of the per-iteration counters for reads.
+    uint64_t stats_words = 0;
+    for (uint32_t i = 0; i < count; ++i) {
+        b->stats_off.push_back(stats_words);
+        stats_words += static_cast<uint64_t>(kStatsCols) * b->probs[i]->stats_cap;
+    }
+    GSC_CU(ctx, cudaMallocHost(&b->hstats, sizeof(unsigned long long) * stats_words));
     // Instance table, work lists and launch shapes; wmax and the shared
     // memory of the batched satisfaction kernel come from the small instances.
     std::vector<InstanceDesc> hd(count);
@@ -519,13 +584,19 @@ int gsc_batch_read_all(gsc_batch* b, gsc_result* out) {
     GSC_CU(ctx, cudaSetDevice(ctx->device));
     cudaStream_t st = ctx->stream;
     const size_t n = b->probs.size();
-    // Control records first (the reachable set's buffer depends on the
-    // iteration count), then every copy, with one wait each.
-    std::vector<FixControl> fc(n);
+    // Control records first, into pinned memory (the reachable set's buffer
+    // depends on the iteration count); then every unpack kernel, then every
+    // copy, so the copies run back to back; one wait each.
     for (size_t i = 0; i < n; ++i)
-        GSC_CU(ctx, cudaMemcpyAsync(&fc[i], b->probs[i]->fc, sizeof(FixControl), cudaMemcpyDeviceToHost, st));
+        GSC_CU(ctx, cudaMemcpyAsync(b->hfc + i, b->probs[i]->fc, sizeof(FixControl), cudaMemcpyDeviceToHost, st));
     GSC_CU(ctx, cudaStreamSynchronize(st));
-    std::vector<std::vector<unsigned long long>> hs(n);
+    const FixControl* fc = b->hfc;
+    for (size_t i = 0; i < n; ++i) {
+        gsc_problem* p = b->probs[i].get();
+        if (out[i].reachable_mask)
+            GSC_CU(ctx, launch_unpack_bits(p->g, (fc[i].iter & 1) ? p->reach1 : p->reach0, p->reach8, st));
+    }
+    std::vector<uint32_t> rows(n, 0);
     for (size_t i = 0; i < n; ++i) {
         gsc_problem* p = b->probs[i].get();
         const GridInfo& g = p->g;
@@ -533,19 +604,19 @@ int gsc_batch_read_all(gsc_batch* b, gsc_result* out) {
         if (r->valid_mask) GSC_CU(ctx, cudaMemcpyAsync(r->valid_mask, p->valid, g.S, cudaMemcpyDeviceToHost, st));
         if (r->candidate_mask)
             GSC_CU(ctx, cudaMemcpyAsync(r->candidate_mask, p->cand, g.S, cudaMemcpyDeviceToHost, st));
-        if (r->reachable_mask) {
-            GSC_CU(ctx, launch_unpack_bits(g, (fc[i].iter & 1) ? p->reach1 : p->reach0, p->reach8, st));
+        if (r->reachable_mask)
             GSC_CU(ctx, cudaMemcpyAsync(r->reachable_mask, p->reach8, g.S, cudaMemcpyDeviceToHost, st));
-        }
         if (r->controller)
             GSC_CU(ctx, cudaMemcpyAsync(r->controller, p->controller, g.S * 4, cudaMemcpyDeviceToHost, st));
         if (r->reach_step)
             GSC_CU(ctx, cudaMemcpyAsync(r->reach_step, p->reach_step, g.S * 4, cudaMemcpyDeviceToHost, st));
-        const uint32_t rows = std::min<uint32_t>({fc[i].iter, r->iter_capacity, p->stats_cap - 1});
-        if (rows && (r->iter_new_reachable || r->iter_new_certified)) {
-            hs[i].resize(static_cast<size_t>(kStatsCols) * (rows + 1));
-            GSC_CU(ctx, cudaMemcpyAsync(hs[i].data(), p->stats, hs[i].size() * 8, cudaMemcpyDeviceToHost, st));
-        }
+        rows[i] = std::min<uint32_t>({fc[i].iter, r->iter_capacity, p->stats_cap - 1});
+        if (rows[i] && (r->iter_new_reachable || r->iter_new_certified))
+            GSC_CU(ctx, cudaMemcpyAsync(b->hstats + b->stats_off[i], p->stats,
+                                        sizeof(unsigned long long) * kStatsCols * (rows[i] + 1),
+                                        cudaMemcpyDeviceToHost, st));
+        else
+            rows[i] = 0;
     }
     GSC_CU(ctx, cudaStreamSynchronize(st));
     for (size_t i = 0; i < n; ++i) {
@@ -564,10 +635,10 @@ int gsc_batch_read_all(gsc_batch* b, gsc_result* out) {
         r->reachable_states = fc[i].reachable;
         r->candidate_count = fc[i].candidate_count;
         r->valid_count = fc[i].valid_count;
-        const uint32_t rows = hs[i].empty() ? 0 : static_cast<uint32_t>(hs[i].size() / kStatsCols - 1);
-        for (uint32_t k = 0; k < rows; ++k) {
-            if (r->iter_new_reachable) r->iter_new_reachable[k] = hs[i][kStatsCols * (k + 1)];
-            if (r->iter_new_certified) r->iter_new_certified[k] = hs[i][kStatsCols * (k + 1) + 1];
+        const unsigned long long* hs = b->hstats + b->stats_off[i];
+        for (uint32_t k = 0; k < rows[i]; ++k) {
+            if (r->iter_new_reachable) r->iter_new_reachable[k] = hs[kStatsCols * (k + 1)];
+            if (r->iter_new_certified) r->iter_new_certified[k] = hs[kStatsCols * (k + 1) + 1];
         }
     }
     return GSC_OK;
