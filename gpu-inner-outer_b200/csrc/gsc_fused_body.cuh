@@ -350,9 +350,14 @@ __device__ __forceinline__ void sat_col_task(const GridInfo& g, const FusedFixAr
         }
         const uint32_t ye = yts[r * n1 + i1];
         if (anyc && ye != kReject && incremental) {
-            uint32_t ch = 0;
-            for (uint32_t y = lo16(ye); y <= hi16(ye); ++y) ch |= rowchg[r * W1 + (y >> 5)] >> (y & 31);
-            if (!(ch & 1u)) anyc = 0;
+            // Bits [lo, hi] of the representative's changed-row mask (fused
+            // boxes span at most 32 rows): one funnel shift.
+            const uint32_t lo = lo16(ye), hi = hi16(ye);
+            const uint32_t* rc = rowchg + r * W1;
+            const uint32_t wl = lo >> 5, wh = hi >> 5;
+            const uint32_t bits = __funnelshift_r(rc[wl], wh != wl ? rc[wh] : 0u, lo & 31);
+            const uint32_t len = hi - lo + 1;
+            if (!(len >= 32 ? bits : (bits & ((1u << len) - 1)))) anyc = 0;
         }
         if (anyc && ye != kReject) {
 #pragma unroll
