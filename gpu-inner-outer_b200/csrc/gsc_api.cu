@@ -397,6 +397,13 @@ void gsc_context_destroy(gsc_context* ctx) {
     cudaSetDevice(ctx->device);
     if (ctx->ev[0]) cudaEventDestroy(ctx->ev[0]);
     if (ctx->ev[1]) cudaEventDestroy(ctx->ev[1]);
+    for (auto s : ctx->setup)
+        if (s) {
+            cudaStreamSynchronize(s);
+            cudaStreamDestroy(s);
+        }
+    for (auto e : ctx->setup_ev)
+        if (e) cudaEventDestroy(e);
     ctx->pool.reset();
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -562,7 +569,11 @@ int problem_stage1(gsc_problem* p, const gsc_query_desc* qd) {
     GSC_CU(ctx, launch_plan(g, p->zt, p->wt, p->fused_candidate ? p->xrep : nullptr, p->counts, p->flags, p->kidx,
                             p->lidx, p->dplan, st));
     if (!p->hplan) p->hplan = &p->hplan_own;
-    GSC_CU(ctx, cudaMemcpyAsync(p->hplan, p->dplan, sizeof(PlanRecord), cudaMemcpyDeviceToHost, st));
+    if (p->hplan_dev)
+        GSC_CU(ctx, launch_store_words(reinterpret_cast<const uint32_t*>(p->dplan),
+                                       reinterpret_cast<uint32_t*>(p->hplan_dev), sizeof(PlanRecord) / 4, st));
+    else
+        GSC_CU(ctx, cudaMemcpyAsync(p->hplan, p->dplan, sizeof(PlanRecord), cudaMemcpyDeviceToHost, st));
     return GSC_OK;
 }
 

@@ -99,7 +99,10 @@ struct gsc_batch {
     std::vector<std::unique_ptr<gsc_problem>> probs;
     PlanRecord* hplans = nullptr;   // pinned
     uint32_t* hrunning = nullptr;   // pinned
-    FixControl* hfc = nullptr;      // pinned: every instance's control record, for reads
+    FixControl* hfc = nullptr;      // pinned: every instance's control record, for reads (written by
+                                    // the status kernel after every iteration)
+    FixControl* hfc_dev = nullptr;  // its device address
+    PlanRecord* hplans_dev = nullptr;
     unsigned long long* hstats = nullptr;   // pinned: every instance's per-iteration counters
     std::vector<uint64_t> stats_off;        // instance -> its first entry in hstats
     InstanceDesc* ddesc = nullptr;
@@ -107,6 +110,13 @@ struct gsc_batch {
     uint32_t* dlist_all = nullptr;   // every instance: init and status
     uint32_t* drunning = nullptr;
     std::vector<uint32_t> hlist, hlist_all;
+    // Pinned staging of the instance table and the two work lists, so their
+    // uploads do not wait for the set-up queued before them.
+    InstanceDesc* hdesc_pin = nullptr;
+    uint32_t* hlist_pin = nullptr;   // [2][count + 4 * (count + 1)]
+    bool lists_uploaded = false;
+    void* pin_early = nullptr;   // hplans, hrunning, hfc
+    void* pin_late = nullptr;    // hstats, hdesc_pin, hlist_pin
     std::vector<uint32_t> small;     // indices of the instances the batched kernels run
     std::vector<BigInstance> big;    // the instances the one-problem kernels run
     WorkTotals tot{}, tot_all{};
@@ -126,10 +136,8 @@ struct gsc_batch {
         probs.clear();
         abs.clear();
         device_release_all(ctx, pool, own, own_bytes);
-        if (hplans) cudaFreeHost(hplans);
-        if (hrunning) cudaFreeHost(hrunning);
-        if (hfc) cudaFreeHost(hfc);
-        if (hstats) cudaFreeHost(hstats);
+        if (pin_early) cudaFreeHost(pin_early);
+        if (pin_late) cudaFreeHost(pin_late);
     }
 };
 
@@ -167,13 +175,20 @@ int upload_list(gsc_batch* b, uint32_t chunk) {
         slots.push_back(i);
     }
     build_work_list(probs, slots, chunk, b->hlist_all, b->tot_all);
-    GSC_CU(b->ctx, cudaMemcpyAsync(b->dlist, b->hlist.data(), b->hlist.size() * 4, cudaMemcpyHostToDevice,
+    // A new upload (autotuning) waits until the previous one has read the
+    // pinned lists; the first does not wait.
+    if (b->lists_uploaded) GSC_CU(b->ctx, cudaStreamSynchronize(b->ctx->stream));
+    const size_t words = b->probs.size() + 4 * (b->probs.size() + 1);
+    uint32_t* pin_small = b->hlist_pin;
+    uint32_t* pin_all = b->hlist_pin + words;
+    std::memcpy(pin_small, b->hlist.data(), b->hlist.size() * 4);
+    std::memcpy(pin_all, b->hlist_all.data(), b->hlist_all.size() * 4);
+    GSC_CU(b->ctx, cudaMemcpyAsync(b->dlist, pin_small, b->hlist.size() * 4, cudaMemcpyHostToDevice, b->ctx->stream));
+    GSC_CU(b->ctx, cudaMemcpyAsync(b->dlist_all, pin_all, b->hlist_all.size() * 4, cudaMemcpyHostToDevice,
                                    b->ctx->stream));
-    GSC_CU(b->ctx, cudaMemcpyAsync(b->dlist_all, b->hlist_all.data(), b->hlist_all.size() * 4,
-                                   cudaMemcpyHostToDevice, b->ctx->stream));
-    GSC_CU(b->ctx, cudaStreamSynchronize(b->ctx->stream));   // the host lists are reused
+    b->lists_uploaded = true;
     b->wl = device_work_list(b->dlist, static_cast<uint32_t>(b->small.size()), chunk, nullptr, b->drunning);
-    b->wl_all = device_work_list(b->dlist_all, static_cast<uint32_t>(b->probs.size()), chunk, nullptr, b->drunning);
+    b->wl_all = device_work_list(b->dlist_all, static_cast<uint32_t>(b->probs.size()), chunk, b->hfc_dev, b->drunning);
     return GSC_OK;
 }
 
@@ -285,37 +300,42 @@ int build_batch_graph(gsc_batch* b) {
     return GSC_OK;
 }
 
-// Streams for the set-up of a batch's instances (instance i on stream
+// The context's set-up streams for one batch (instance i on stream
 // i % kSetupStreams), so that the small set-up kernels of different
-// instances run side by side.  Every exit drains and destroys them.
+// instances run side by side.  They have the device's highest stream
+// priority: in a pipelined run their blocks go ahead of a solve that fills
+// the GPU.  They are created once per context; a batch that fails drains
+// them before its memory is released, a batch that succeeds only joins
+// them into the context stream (no host wait).
 struct SetupStreams {
-    static constexpr int kSetupStreams = 8;
-    cudaStream_t s[kSetupStreams] = {};
-    cudaEvent_t ev[kSetupStreams + 1] = {};
+    static constexpr int kSetupStreams = gsc_context::kSetupStreams;
+    gsc_context* ctx = nullptr;
+    bool ok = false;
     ~SetupStreams() {
-        for (auto x : s)
-            if (x) {
-                cudaStreamSynchronize(x);
-                cudaStreamDestroy(x);
-            }
-        for (auto e : ev)
-            if (e) cudaEventDestroy(e);
+        if (ok || !ctx) return;
+        for (auto x : ctx->setup)
+            if (x) cudaStreamSynchronize(x);
     }
-    cudaError_t create(cudaStream_t after) {
-        for (auto& e : ev) {
-            const cudaError_t r = cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+    cudaError_t create(gsc_context* c, cudaStream_t after) {
+        ctx = c;
+        cudaError_t r = cudaSuccess;
+        if (!ctx->setup[0]) {
+            int least = 0, greatest = 0;
+            r = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+            for (auto& x : ctx->setup)
+                if (r == cudaSuccess) r = cudaStreamCreateWithPriority(&x, cudaStreamNonBlocking, greatest);
+            for (auto& e : ctx->setup_ev)
+                if (r == cudaSuccess) r = cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
             if (r != cudaSuccess) return r;
         }
-        cudaError_t r = cudaEventRecord(ev[kSetupStreams], after);
-        for (auto& x : s) {
-            if (r == cudaSuccess) r = cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking);
-            if (r == cudaSuccess) r = cudaStreamWaitEvent(x, ev[kSetupStreams], 0);
-        }
+        r = cudaEventRecord(ctx->setup_ev[kSetupStreams], after);
+        for (auto x : ctx->setup)
+            if (r == cudaSuccess) r = cudaStreamWaitEvent(x, ctx->setup_ev[kSetupStreams], 0);
         return r;
     }
-    cudaStream_t of(uint32_t i) const { return s[i % kSetupStreams]; }
+    cudaStream_t of(uint32_t i) const { return ctx->setup[i % kSetupStreams]; }
     cudaError_t sync() {
-        for (auto x : s) {
+        for (auto x : ctx->setup) {
             const cudaError_t r = cudaStreamSynchronize(x);
             if (r != cudaSuccess) return r;
         }
@@ -324,8 +344,8 @@ struct SetupStreams {
     // `st` waits for everything enqueued on the set-up streams.
     cudaError_t join(cudaStream_t st) {
         for (int k = 0; k < kSetupStreams; ++k) {
-            cudaError_t r = cudaEventRecord(ev[k], s[k]);
-            if (r == cudaSuccess) r = cudaStreamWaitEvent(st, ev[k], 0);
+            cudaError_t r = cudaEventRecord(ctx->setup_ev[k], ctx->setup[k]);
+            if (r == cudaSuccess) r = cudaStreamWaitEvent(st, ctx->setup_ev[k], 0);
             if (r != cudaSuccess) return r;
         }
         return cudaSuccess;
@@ -338,10 +358,29 @@ int batch_create(gsc_batch* b, uint32_t count, const gsc_model_desc* models, con
     cudaStream_t st = ctx->stream;
     b->pool = ctx->pool.get();
     SetupStreams ss;
-    GSC_CU(ctx, ss.create(st));
-    GSC_CU(ctx, cudaMallocHost(&b->hplans, sizeof(PlanRecord) * count));
-    GSC_CU(ctx, cudaMallocHost(&b->hrunning, sizeof(uint32_t)));
-    GSC_CU(ctx, cudaMallocHost(&b->hfc, sizeof(FixControl) * count));
+    GSC_CU(ctx, ss.create(ctx, st));
+    // Pinned host memory in two carved allocations (pinning is slow per call).
+    auto carve16 = [](char*& p, size_t bytes) {
+        char* r = p;
+        p += (bytes + 15) & ~size_t(15);
+        return r;
+    };
+    {
+        const size_t bytes = ((sizeof(PlanRecord) * count + 15) & ~size_t(15)) + 16 +
+                             ((sizeof(FixControl) * count + 15) & ~size_t(15));
+        GSC_CU(ctx, cudaMallocHost(&b->pin_early, bytes));
+        char* q = static_cast<char*>(b->pin_early);
+        b->hplans = reinterpret_cast<PlanRecord*>(carve16(q, sizeof(PlanRecord) * count));
+        b->hrunning = reinterpret_cast<uint32_t*>(carve16(q, sizeof(uint32_t)));
+        b->hfc = reinterpret_cast<FixControl*>(carve16(q, sizeof(FixControl) * count));
+        std::memset(b->pin_early, 0, bytes);
+        char* dq = nullptr;
+        GSC_CU(ctx, cudaHostGetDevicePointer(reinterpret_cast<void**>(&dq), b->pin_early, 0));
+        b->hplans_dev = reinterpret_cast<PlanRecord*>(dq + (reinterpret_cast<char*>(b->hplans) -
+                                                             static_cast<char*>(b->pin_early)));
+        b->hfc_dev = reinterpret_cast<FixControl*>(dq + (reinterpret_cast<char*>(b->hfc) -
+                                                          static_cast<char*>(b->pin_early)));
+    }
     std::vector<std::vector<std::pair<void*, uint64_t>>> tmp(count);
     // Stage 1 of every instance, then one wait for all plan records.
     for (uint32_t i = 0; i < count; ++i) {
@@ -368,6 +407,7 @@ int batch_create(gsc_batch* b, uint32_t count, const gsc_model_desc* models, con
         p->stream = ss.of(i);
         p->method = GSC_METHOD_FUSED;
         p->hplan = b->hplans + i;
+        p->hplan_dev = b->hplans_dev + i;
         const int s = problem_stage1(p.get(), &queries[i]);
         if (s != GSC_OK) return fail(ctx, s, "instance " + std::to_string(i) + ": " + ctx->last_error);
         b->probs.push_back(std::move(p));
@@ -385,6 +425,7 @@ int batch_create(gsc_batch* b, uint32_t count, const gsc_model_desc* models, con
     }
     // Later work on the context stream (init, solves, reads) follows the set-up.
     GSC_CU(ctx, ss.join(st));
+    ss.ok = true;
     for (auto& p : b->probs) p->stream = st;
     // Pinned staging of the per-iteration counters for reads.
     uint64_t stats_words = 0;
@@ -392,7 +433,16 @@ int batch_create(gsc_batch* b, uint32_t count, const gsc_model_desc* models, con
         b->stats_off.push_back(stats_words);
         stats_words += static_cast<uint64_t>(kStatsCols) * b->probs[i]->stats_cap;
     }
-    GSC_CU(ctx, cudaMallocHost(&b->hstats, sizeof(unsigned long long) * stats_words));
+    const size_t list_bytes = 2 * 4ull * (count + 4ull * (count + 1));
+    {
+        const size_t bytes = ((sizeof(unsigned long long) * stats_words + 15) & ~size_t(15)) +
+                             ((sizeof(InstanceDesc) * count + 15) & ~size_t(15)) + ((list_bytes + 15) & ~size_t(15));
+        GSC_CU(ctx, cudaMallocHost(&b->pin_late, bytes));
+        char* q = static_cast<char*>(b->pin_late);
+        b->hstats = reinterpret_cast<unsigned long long*>(carve16(q, sizeof(unsigned long long) * stats_words));
+        b->hdesc_pin = reinterpret_cast<InstanceDesc*>(carve16(q, sizeof(InstanceDesc) * count));
+        b->hlist_pin = reinterpret_cast<uint32_t*>(carve16(q, list_bytes));
+    }
     // Instance table, work lists and launch shapes; wmax and the shared
     // memory of the batched satisfaction kernel come from the small instances.
     std::vector<InstanceDesc> hd(count);
@@ -424,7 +474,8 @@ int batch_create(gsc_batch* b, uint32_t count, const gsc_model_desc* models, con
     b->dlist_all = static_cast<uint32_t*>(q);
     GSC_TRY(device_alloc(ctx, b->pool, b->own, b->own_bytes, &q, 4));
     b->drunning = static_cast<uint32_t*>(q);
-    GSC_CU(ctx, cudaMemcpyAsync(b->ddesc, hd.data(), sizeof(InstanceDesc) * count, cudaMemcpyHostToDevice, st));
+    std::memcpy(b->hdesc_pin, hd.data(), sizeof(InstanceDesc) * count);
+    GSC_CU(ctx, cudaMemcpyAsync(b->ddesc, b->hdesc_pin, sizeof(InstanceDesc) * count, cudaMemcpyHostToDevice, st));
 
     const int sms = sm_count(ctx);
     b->shape.sat_threads = (opt && opt->sat_threads) ? opt->sat_threads : 128;
@@ -467,6 +518,75 @@ int batch_create(gsc_batch* b, uint32_t count, const gsc_model_desc* models, con
     }
     b->t.instances = count;
     return GSC_OK;
+}
+
+// The reads of every instance of a solved batch: one host wait for `ctl`
+// (which follows the solve), after which the control records are in pinned
+// memory (the status kernel stores them there after every iteration; the
+// reachable set's buffer depends on the iteration count); the result fields
+// they give; then every unpack kernel and every copy on `st` (the copies back
+// to back), not waited for.
+// rows[i]: per-iteration counter rows staged for instance i.
+// unpacked: the reachable sets were unpacked already (launch_unpack_reach).
+int read_begin(gsc_batch* b, gsc_result* out, cudaStream_t ctl, cudaStream_t st, std::vector<uint32_t>& rows,
+               bool unpacked = false) {
+    gsc_context* ctx = b->ctx;
+    const size_t n = b->probs.size();
+    GSC_CU(ctx, cudaStreamSynchronize(ctl));
+    const FixControl* fc = b->hfc;
+    for (size_t i = 0; i < n && !unpacked; ++i) {
+        gsc_problem* p = b->probs[i].get();
+        if (out[i].reachable_mask)
+            GSC_CU(ctx, launch_unpack_bits(p->g, (fc[i].iter & 1) ? p->reach1 : p->reach0, p->reach8, st));
+    }
+    rows.assign(n, 0);
+    for (size_t i = 0; i < n; ++i) {
+        gsc_problem* p = b->probs[i].get();
+        const GridInfo& g = p->g;
+        gsc_result* r = out + i;
+        if (r->valid_mask) GSC_CU(ctx, cudaMemcpyAsync(r->valid_mask, p->valid, g.S, cudaMemcpyDeviceToHost, st));
+        if (r->candidate_mask)
+            GSC_CU(ctx, cudaMemcpyAsync(r->candidate_mask, p->cand, g.S, cudaMemcpyDeviceToHost, st));
+        if (r->reachable_mask)
+            GSC_CU(ctx, cudaMemcpyAsync(r->reachable_mask, p->reach8, g.S, cudaMemcpyDeviceToHost, st));
+        if (r->controller)
+            GSC_CU(ctx, cudaMemcpyAsync(r->controller, p->controller, g.S * 4, cudaMemcpyDeviceToHost, st));
+        if (r->reach_step)
+            GSC_CU(ctx, cudaMemcpyAsync(r->reach_step, p->reach_step, g.S * 4, cudaMemcpyDeviceToHost, st));
+        rows[i] = std::min<uint32_t>({fc[i].iter, r->iter_capacity, p->stats_cap - 1});
+        if (rows[i] && (r->iter_new_reachable || r->iter_new_certified))
+            GSC_CU(ctx, cudaMemcpyAsync(b->hstats + b->stats_off[i], p->stats,
+                                        sizeof(unsigned long long) * kStatsCols * (rows[i] + 1),
+                                        cudaMemcpyDeviceToHost, st));
+        else
+            rows[i] = 0;
+        for (int d = 0; d < 4; ++d) r->shape[d] = g.n[d];
+        r->input_shape[0] = g.ma;
+        r->input_shape[1] = g.mw;
+        r->states = g.S;
+        r->inputs = g.M;
+        r->pairs = g.S * g.M;
+        r->iterations = fc[i].iter;
+        r->converged = static_cast<int32_t>(fc[i].converged);
+        r->message = static_cast<int32_t>(fc[i].message ? fc[i].message : GSC_MSG_MAX_ITERATIONS);
+        r->certified_candidates = fc[i].certified;
+        r->reachable_states = fc[i].reachable;
+        r->candidate_count = fc[i].candidate_count;
+        r->valid_count = fc[i].valid_count;
+    }
+    return GSC_OK;
+}
+
+// After the stream of read_begin finished: the per-iteration counters.
+void read_finish(gsc_batch* b, gsc_result* out, const std::vector<uint32_t>& rows) {
+    for (size_t i = 0; i < rows.size(); ++i) {
+        gsc_result* r = out + i;
+        const unsigned long long* hs = b->hstats + b->stats_off[i];
+        for (uint32_t k = 0; k < rows[i]; ++k) {
+            if (r->iter_new_reachable) r->iter_new_reachable[k] = hs[kStatsCols * (k + 1)];
+            if (r->iter_new_certified) r->iter_new_certified[k] = hs[kStatsCols * (k + 1) + 1];
+        }
+    }
 }
 
 }  // namespace
@@ -577,70 +697,103 @@ int gsc_batch_timings(gsc_batch* b, gsc_batch_report* out) {
     return GSC_OK;
 }
 
+// Streams of a pipelined run; every exit drains them before the parts'
+// memory is released.
+struct RunStreams {
+    cudaStream_t solve = nullptr, copy = nullptr, ctl = nullptr;
+    cudaEvent_t ready = nullptr;
+    std::vector<cudaEvent_t> solved;
+    ~RunStreams() {
+        for (auto s : {solve, copy, ctl})
+            if (s) {
+                cudaStreamSynchronize(s);
+                cudaStreamDestroy(s);
+            }
+        if (ready) cudaEventDestroy(ready);
+        for (auto e : solved) cudaEventDestroy(e);
+    }
+};
+
+int gsc_batch_run(gsc_context* ctx, uint32_t count, const gsc_model_desc* models, const gsc_query_desc* queries,
+                  const gsc_batch_options* options, uint32_t part_instances, gsc_result* results) {
+    if (!ctx || !models || !queries || !results || count == 0) return GSC_ERR_INVALID_ARGUMENT;
+    cudaGetLastError();
+    GSC_CU(ctx, cudaSetDevice(ctx->device));
+    const uint32_t part = part_instances ? part_instances : std::max<uint32_t>(1, (count + 7) / 8);
+    const int sms = sm_count(ctx);
+    std::vector<std::unique_ptr<gsc_batch>> parts;   // destroyed after `rs` drained the streams
+    std::vector<uint32_t> first;
+    std::vector<std::vector<uint32_t>> rows;
+    RunStreams rs;
+    GSC_CU(ctx, cudaStreamCreateWithFlags(&rs.solve, cudaStreamNonBlocking));
+    GSC_CU(ctx, cudaStreamCreateWithFlags(&rs.copy, cudaStreamNonBlocking));
+    GSC_CU(ctx, cudaStreamCreateWithFlags(&rs.ctl, cudaStreamNonBlocking));
+    GSC_CU(ctx, cudaEventCreateWithFlags(&rs.ready, cudaEventDisableTiming));
+    gsc_batch_options opt = options ? *options : gsc_batch_options{};
+    // Reads of part k: after its solve, the control records on `ctl`, the
+    // unpacks and copies on `copy`.
+    auto read_part = [&](size_t k) -> int {
+        GSC_CU(ctx, cudaStreamWaitEvent(rs.ctl, rs.solved[k], 0));
+        GSC_CU(ctx, cudaStreamWaitEvent(rs.copy, rs.solved[k], 0));
+        return read_begin(parts[k].get(), results + first[k], rs.ctl, rs.copy, rows[k], true);
+    };
+    for (uint32_t f = 0; f < count; f += part) {
+        const uint32_t n = std::min(part, count - f);
+        std::unique_ptr<gsc_batch> b(new (std::nothrow) gsc_batch());
+        if (!b) return GSC_ERR_OUT_OF_MEMORY;
+        b->ctx = ctx;
+        int s = batch_create(b.get(), n, models + f, queries + f, &opt);
+        if (s == GSC_OK && !b->exec) s = build_batch_graph(b.get());
+        if (s != GSC_OK) {
+            cudaStreamSynchronize(ctx->stream);   // nothing of the failed part may still be in flight
+            return fail(ctx, s, "instances " + std::to_string(f) + ".." + std::to_string(f + n - 1) + ": " +
+                                    ctx->last_error);
+        }
+        if (parts.empty() && opt.autotune) {
+            // Later parts take the first part's shapes: no trials beside a solve.
+            opt.autotune = 0;
+            opt.sat_threads = b->shape.sat_threads;
+            opt.sat_blocks_per_sm = b->shape.sat_blocks / static_cast<uint32_t>(sms);
+            opt.chunk_words = b->shape.chunk;
+            opt.sat_warp_tasks = b->shape.warp;
+        }
+        // The solve follows the part's set-up (joined into the context stream).
+        GSC_CU(ctx, cudaEventRecord(rs.ready, ctx->stream));
+        GSC_CU(ctx, cudaStreamWaitEvent(rs.solve, rs.ready, 0));
+        GSC_CU(ctx, cudaGraphLaunch(b->exec, rs.solve));
+        // Unpack the reachable sets on the solve stream too, so the copy
+        // stream carries copies only (its kernels would wait for SMs behind
+        // the next part's solve).
+        for (uint32_t i = 0; i < n; ++i) {
+            gsc_problem* p = b->probs[i].get();
+            if (results[f + i].reachable_mask)
+                GSC_CU(ctx, launch_unpack_reach(p->g, p->fc, p->reach0, p->reach1, p->reach8, rs.solve));
+        }
+        cudaEvent_t ev = nullptr;
+        GSC_CU(ctx, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        rs.solved.push_back(ev);
+        GSC_CU(ctx, cudaEventRecord(ev, rs.solve));
+        parts.push_back(std::move(b));
+        first.push_back(f);
+        rows.emplace_back();
+        // The previous part is read while this one solves and the next is set up.
+        if (parts.size() >= 2) GSC_TRY(read_part(parts.size() - 2));
+    }
+    GSC_TRY(read_part(parts.size() - 1));
+    GSC_CU(ctx, cudaStreamSynchronize(rs.copy));
+    for (size_t k = 0; k < parts.size(); ++k) read_finish(parts[k].get(), results + first[k], rows[k]);
+    return GSC_OK;
+}
+
 int gsc_batch_read_all(gsc_batch* b, gsc_result* out) {
     if (!b || !out) return GSC_ERR_INVALID_ARGUMENT;
     gsc_context* ctx = b->ctx;
     cudaGetLastError();
     GSC_CU(ctx, cudaSetDevice(ctx->device));
-    cudaStream_t st = ctx->stream;
-    const size_t n = b->probs.size();
-    // Control records first, into pinned memory (the reachable set's buffer
-    // depends on the iteration count); then every unpack kernel, then every
-    // copy, so the copies run back to back; one wait each.
-    for (size_t i = 0; i < n; ++i)
-        GSC_CU(ctx, cudaMemcpyAsync(b->hfc + i, b->probs[i]->fc, sizeof(FixControl), cudaMemcpyDeviceToHost, st));
-    GSC_CU(ctx, cudaStreamSynchronize(st));
-    const FixControl* fc = b->hfc;
-    for (size_t i = 0; i < n; ++i) {
-        gsc_problem* p = b->probs[i].get();
-        if (out[i].reachable_mask)
-            GSC_CU(ctx, launch_unpack_bits(p->g, (fc[i].iter & 1) ? p->reach1 : p->reach0, p->reach8, st));
-    }
-    std::vector<uint32_t> rows(n, 0);
-    for (size_t i = 0; i < n; ++i) {
-        gsc_problem* p = b->probs[i].get();
-        const GridInfo& g = p->g;
-        gsc_result* r = out + i;
-        if (r->valid_mask) GSC_CU(ctx, cudaMemcpyAsync(r->valid_mask, p->valid, g.S, cudaMemcpyDeviceToHost, st));
-        if (r->candidate_mask)
-            GSC_CU(ctx, cudaMemcpyAsync(r->candidate_mask, p->cand, g.S, cudaMemcpyDeviceToHost, st));
-        if (r->reachable_mask)
-            GSC_CU(ctx, cudaMemcpyAsync(r->reachable_mask, p->reach8, g.S, cudaMemcpyDeviceToHost, st));
-        if (r->controller)
-            GSC_CU(ctx, cudaMemcpyAsync(r->controller, p->controller, g.S * 4, cudaMemcpyDeviceToHost, st));
-        if (r->reach_step)
-            GSC_CU(ctx, cudaMemcpyAsync(r->reach_step, p->reach_step, g.S * 4, cudaMemcpyDeviceToHost, st));
-        rows[i] = std::min<uint32_t>({fc[i].iter, r->iter_capacity, p->stats_cap - 1});
-        if (rows[i] && (r->iter_new_reachable || r->iter_new_certified))
-            GSC_CU(ctx, cudaMemcpyAsync(b->hstats + b->stats_off[i], p->stats,
-                                        sizeof(unsigned long long) * kStatsCols * (rows[i] + 1),
-                                        cudaMemcpyDeviceToHost, st));
-        else
-            rows[i] = 0;
-    }
-    GSC_CU(ctx, cudaStreamSynchronize(st));
-    for (size_t i = 0; i < n; ++i) {
-        const GridInfo& g = b->probs[i]->g;
-        gsc_result* r = out + i;
-        for (int d = 0; d < 4; ++d) r->shape[d] = g.n[d];
-        r->input_shape[0] = g.ma;
-        r->input_shape[1] = g.mw;
-        r->states = g.S;
-        r->inputs = g.M;
-        r->pairs = g.S * g.M;
-        r->iterations = fc[i].iter;
-        r->converged = static_cast<int32_t>(fc[i].converged);
-        r->message = static_cast<int32_t>(fc[i].message ? fc[i].message : GSC_MSG_MAX_ITERATIONS);
-        r->certified_candidates = fc[i].certified;
-        r->reachable_states = fc[i].reachable;
-        r->candidate_count = fc[i].candidate_count;
-        r->valid_count = fc[i].valid_count;
-        const unsigned long long* hs = b->hstats + b->stats_off[i];
-        for (uint32_t k = 0; k < rows[i]; ++k) {
-            if (r->iter_new_reachable) r->iter_new_reachable[k] = hs[kStatsCols * (k + 1)];
-            if (r->iter_new_certified) r->iter_new_certified[k] = hs[kStatsCols * (k + 1) + 1];
-        }
-    }
+    std::vector<uint32_t> rows;
+    GSC_TRY(read_begin(b, out, ctx->stream, ctx->stream, rows));
+    GSC_CU(ctx, cudaStreamSynchronize(ctx->stream));
+    read_finish(b, out, rows);
     return GSC_OK;
 }
 

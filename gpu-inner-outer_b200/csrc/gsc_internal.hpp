@@ -53,6 +53,11 @@ struct gsc_context {
     cudaEvent_t ev[2] = {nullptr, nullptr};
     int sm_count = 0;
     std::unique_ptr<DevicePool> pool;   // caching pool of the context's problems and abstractions
+    // Streams for the set-up of batch instances (created at the first batch,
+    // highest stream priority) and events to join them into `stream`.
+    static constexpr int kSetupStreams = 8;
+    cudaStream_t setup[kSetupStreams] = {};
+    cudaEvent_t setup_ev[kSetupStreams + 1] = {};
 };
 
 struct gsc_abstraction {
@@ -98,6 +103,10 @@ struct gsc_problem {
     gsc_b200::PlanRecord* dplan = nullptr;
     gsc_b200::PlanRecord* hplan = nullptr;   // host copy (caller-provided pinned memory, or hplan_own)
     gsc_b200::PlanRecord hplan_own{};
+    // Device address of *hplan when it is pinned host memory: the plan is then
+    // stored there by a kernel, not copied by a copy engine (whose queue may
+    // hold large result copies).
+    gsc_b200::PlanRecord* hplan_dev = nullptr;
     bool fused_candidate = false;
     // stored
     uint2* boxes = nullptr;

@@ -43,6 +43,13 @@ cudaError_t launch_axis_tables(const GridInfo& g, const QueryInfo& q, const doub
 cudaError_t launch_pack_bits(const GridInfo& g, int mode, const uint8_t* src, const uint8_t* src2, bword* out,
                              cudaStream_t st);
 cudaError_t launch_unpack_bits(const GridInfo& g, const bword* bits, uint8_t* out, cudaStream_t st);
+// n words from src to dst by one small kernel (dst may be pinned host memory
+// mapped into the device's address space).
+cudaError_t launch_store_words(const uint32_t* src, uint32_t* dst, uint32_t n, cudaStream_t st);
+// The fixpoint's current reachable set (reach0 or reach1 by fc->iter, read
+// on the device) as one byte per state.
+cudaError_t launch_unpack_reach(const GridInfo& g, const FixControl* fc, const bword* reach0, const bword* reach1,
+                                uint8_t* out, cudaStream_t st);
 
 // ---- 4-D inclusive prefix tables (int32, zero first plane per dimension) -----------------
 // mode 0: valid; 1: valid && !reach (b = reach); 2: !safe (4-D safe mask).

@@ -67,13 +67,14 @@ struct gsc_server {
     InstanceDesc* ddesc = nullptr;
     uint32_t* dlist = nullptr;         // every running query: status
     uint32_t* dlist_small = nullptr;   // the running queries the batched kernels run
-    FixControl* dstatus = nullptr;
     void* dmem = nullptr;
     // pinned host
     InstanceDesc* hdesc = nullptr;
     uint32_t* hlist = nullptr;   // both lists, the small one after the other
-    FixControl* hstatus = nullptr;
+    FixControl* hstatus = nullptr;       // pinned; the status kernel stores each step's records here
+    FixControl* hstatus_dev = nullptr;   // its device address
     PlanRecord* hplans = nullptr;
+    PlanRecord* hplans_dev = nullptr;   // their device address (stored by a kernel, not copied)
     unsigned long long* hstats = nullptr;   // [slot][kStatsRows][kStatsCols]
     // loop-thread state
     std::vector<uint32_t> free_slots;
@@ -148,6 +149,7 @@ bool admit(gsc_server* s) {
         p->stream = s->s_prep;
         p->method = GSC_METHOD_FUSED;
         p->hplan = s->hplans + r->slot;
+        p->hplan_dev = s->hplans_dev + r->slot;
         int status = problem_stage1(p, &r->q);
         if (status == GSC_OK && cudaEventRecord(r->ev, s->s_prep) != cudaSuccess) status = GSC_ERR_CUDA;
         if (status == GSC_ERR_OUT_OF_MEMORY && !nothing_in_flight(s)) {
@@ -387,7 +389,8 @@ void loop(gsc_server* s) {
             std::memcpy(s->hlist + hl.size(), hls.data(), hls.size() * 4);
             cudaMemcpyAsync(s->dlist, s->hlist, hl.size() * 4, cudaMemcpyHostToDevice, s->s_main);
             cudaMemcpyAsync(s->dlist_small, s->hlist + hl.size(), hls.size() * 4, cudaMemcpyHostToDevice, s->s_main);
-            wl = device_work_list(s->dlist, static_cast<uint32_t>(slots.size()), s->shape.chunk, s->dstatus, nullptr);
+            wl = device_work_list(s->dlist, static_cast<uint32_t>(slots.size()), s->shape.chunk, s->hstatus_dev,
+                                  nullptr);
             wl_small = device_work_list(s->dlist_small, static_cast<uint32_t>(sslots.size()), s->shape.chunk, nullptr,
                                         nullptr);
             list_dirty = false;
@@ -399,8 +402,6 @@ void loop(gsc_server* s) {
         for (uint32_t i = 0; e == cudaSuccess && i < K; ++i)
             e = launch_batch_step(s->ddesc, wl_small, tot_small, wl, big.data(), static_cast<uint32_t>(big.size()),
                                   shape, wmax, smem, sms, 0, 0, s->s_main, nullptr);
-        if (e == cudaSuccess)
-            e = cudaMemcpyAsync(s->hstatus, s->dstatus, sizeof(FixControl) * n, cudaMemcpyDeviceToHost, s->s_main);
         if (e == cudaSuccess) e = cudaEventRecord(s->ev_step, s->s_main);
         {
             std::lock_guard<std::mutex> lk(s->mu);
@@ -509,12 +510,15 @@ int gsc_server_create(gsc_context* ctx, const gsc_server_options* options, gsc_s
     s->ictx.sm_count = ctx->sm_count;
     GSC_CU(ctx, cudaStreamCreateWithFlags(&s->s_main, cudaStreamNonBlocking));
     GSC_CU(ctx, cudaStreamCreateWithFlags(&s->s_prep, cudaStreamNonBlocking));
-    GSC_CU(ctx, cudaStreamCreateWithFlags(&s->s_copy, cudaStreamNonBlocking));
+    // The copy stream's unpack kernels go ahead of the fixpoint steps' blocks.
+    int least = 0, greatest = 0;
+    GSC_CU(ctx, cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    GSC_CU(ctx, cudaStreamCreateWithPriority(&s->s_copy, cudaStreamNonBlocking, greatest));
     s->ictx.stream = s->s_prep;
     GSC_CU(ctx, cudaEventCreateWithFlags(&s->ev_step, cudaEventDisableTiming));
     const uint32_t n = o.max_slots;
     const size_t list_words = n + 4ull * (n + 1);
-    const size_t dbytes = sizeof(InstanceDesc) * n + sizeof(FixControl) * n + 2 * 4 * list_words + 256 * 4;
+    const size_t dbytes = sizeof(InstanceDesc) * n + 2 * 4 * list_words + 256 * 3;
     GSC_CU(ctx, cudaMalloc(&s->dmem, dbytes));
     char* d = static_cast<char*>(s->dmem);
     auto carve = [&](size_t bytes) {
@@ -523,13 +527,14 @@ int gsc_server_create(gsc_context* ctx, const gsc_server_options* options, gsc_s
         return r;
     };
     s->ddesc = reinterpret_cast<InstanceDesc*>(carve(sizeof(InstanceDesc) * n));
-    s->dstatus = reinterpret_cast<FixControl*>(carve(sizeof(FixControl) * n));
     s->dlist = reinterpret_cast<uint32_t*>(carve(4 * list_words));
     s->dlist_small = reinterpret_cast<uint32_t*>(carve(4 * list_words));
     GSC_CU(ctx, cudaMallocHost(&s->hdesc, sizeof(InstanceDesc) * n));
     GSC_CU(ctx, cudaMallocHost(&s->hlist, 2 * 4 * list_words));
     GSC_CU(ctx, cudaMallocHost(&s->hstatus, sizeof(FixControl) * n));
+    GSC_CU(ctx, cudaHostGetDevicePointer(reinterpret_cast<void**>(&s->hstatus_dev), s->hstatus, 0));
     GSC_CU(ctx, cudaMallocHost(&s->hplans, sizeof(PlanRecord) * n));
+    GSC_CU(ctx, cudaHostGetDevicePointer(reinterpret_cast<void**>(&s->hplans_dev), s->hplans, 0));
     GSC_CU(ctx, cudaMallocHost(&s->hstats, sizeof(unsigned long long) * kStatsCols * kStatsRows * n));
     for (uint32_t i = 0; i < n; ++i) s->free_slots.push_back(n - 1 - i);
     s->st.device_bytes_budget = s->pool->total;

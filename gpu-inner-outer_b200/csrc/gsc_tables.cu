@@ -306,9 +306,16 @@ __global__ void k_pack_bits(GridInfo g, int mode, const uint8_t* __restrict__ sr
     }
 }
 
-// One warp per x-row.
+__global__ void k_store_words(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst, uint32_t n) {
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+}
+
+// One warp per x-row.  With fc, the set is the fixpoint's current
+// reachable buffer (bits when fc->iter is even, odd otherwise).
 __global__ void __launch_bounds__(kPlaneThreads) k_unpack_bits(GridInfo g, const bword* __restrict__ bits,
-                                                              uint8_t* __restrict__ out) {
+                                                              uint8_t* __restrict__ out, const FixControl* fc,
+                                                              const bword* __restrict__ odd) {
+    if (fc && (fc->iter & 1)) bits = odd;
     const uint32_t lane = threadIdx.x & 31;
     const uint64_t wstride = static_cast<uint64_t>(gridDim.x) * (blockDim.x >> 5);
     for (uint64_t r = blockIdx.x * static_cast<uint64_t>(blockDim.x >> 5) + (threadIdx.x >> 5); r < g.rows;
@@ -600,7 +607,18 @@ cudaError_t launch_pack_bits(const GridInfo& g, int mode, const uint8_t* src, co
 }
 
 cudaError_t launch_unpack_bits(const GridInfo& g, const bword* bits, uint8_t* out, cudaStream_t st) {
-    k_unpack_bits<<<warp_blocks(g.rows), kPlaneThreads, 0, st>>>(g, bits, out);
+    k_unpack_bits<<<warp_blocks(g.rows), kPlaneThreads, 0, st>>>(g, bits, out, nullptr, nullptr);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_store_words(const uint32_t* src, uint32_t* dst, uint32_t n, cudaStream_t st) {
+    k_store_words<<<1, 32, 0, st>>>(src, dst, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_unpack_reach(const GridInfo& g, const FixControl* fc, const bword* reach0, const bword* reach1,
+                                uint8_t* out, cudaStream_t st) {
+    k_unpack_bits<<<warp_blocks(g.rows), kPlaneThreads, 0, st>>>(g, reach0, out, fc, reach1);
     return cudaGetLastError();
 }
 

@@ -146,6 +146,8 @@ SIGNATURES = {
     "gsc_batch_solve": (ctypes.c_int, [_P, ctypes.c_uint32]),
     "gsc_batch_read": (ctypes.c_int, [_P, ctypes.c_uint32, ctypes.POINTER(Result)]),
     "gsc_batch_read_all": (ctypes.c_int, [_P, ctypes.POINTER(Result)]),
+    "gsc_batch_run": (ctypes.c_int, [_P, ctypes.c_uint32, ctypes.POINTER(ModelDesc), ctypes.POINTER(QueryDesc),
+                                     ctypes.POINTER(BatchOptions), ctypes.c_uint32, ctypes.POINTER(Result)]),
     "gsc_batch_timings": (ctypes.c_int, [_P, ctypes.POINTER(BatchReport)]),
     "gsc_batch_destroy": (None, [_P]),
     "gsc_server_create": (ctypes.c_int, [_P, ctypes.POINTER(ServerOptions), ctypes.POINTER(_P)]),
@@ -494,6 +496,41 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def run_batch(ctx: Context, cases, outs=None, autotune=True, part_instances=0, iter_capacity=4096, sat_threads=0,
+              sat_blocks_per_sm=0, chunk_words=0, sat_warp_tasks=False) -> list:
+    """Set up, solve and read many instances in one pipelined call
+    (gsc_batch_run): parts of ``part_instances`` instances overlap their
+    set-up, solve and copies.  ``outs`` may supply each instance's five
+    arrays (pinned memory keeps the copies asynchronous)."""
+    n = len(cases)
+    queries = [_Query(c) for c in cases]
+    models = (ModelDesc * n)(*[model_desc(c) for c in cases])
+    qdescs = (QueryDesc * n)(*[q.desc for q in queries])
+    opt = BatchOptions(int(bool(autotune)), int(sat_threads), int(sat_blocks_per_sm), int(chunk_words),
+                       int(bool(sat_warp_tasks)))
+    rs = (Result * n)()
+    keep = []
+    nr_all = np.zeros((n, iter_capacity), np.uint64)
+    nc_all = np.zeros((n, iter_capacity), np.uint64)
+    for i, c in enumerate(cases):
+        S = int(np.prod(grid_shape(c)[0], dtype=np.uint64))
+        o = dict(outs[i]) if outs is not None else {
+            "valid_mask": np.zeros(S, np.uint8), "candidate_mask": np.zeros(S, np.uint8),
+            "reachable_mask": np.zeros(S, np.uint8), "controller": np.zeros(S, np.uint32),
+            "reach_step": np.zeros(S, np.uint32)}
+        for k, v in o.items():
+            if v.size != S or not v.flags["C_CONTIGUOUS"]:
+                raise ValueError(f"outs[{i}][{k}] must be a contiguous array of {S} elements")
+            setattr(rs[i], k, _ptr(v))
+        nr, nc = nr_all[i], nc_all[i]
+        rs[i].iter_new_reachable = _ptr(nr)
+        rs[i].iter_new_certified = _ptr(nc)
+        rs[i].iter_capacity = iter_capacity
+        keep.append((o, nr, nc))
+    ctx.check(lib().gsc_batch_run(ctx._h, n, models, qdescs, ctypes.byref(opt), int(part_instances), rs))
+    return [_result_dict(rs[i], keep[i][0], keep[i][1], keep[i][2], iter_capacity) for i in range(n)]
 
 
 class Server:

@@ -350,6 +350,17 @@ int gsc_batch_read(gsc_batch* batch, uint32_t index, gsc_result* out);
 int gsc_batch_read_all(gsc_batch* batch, gsc_result* out);
 int gsc_batch_timings(gsc_batch* batch, gsc_batch_report* out);
 void gsc_batch_destroy(gsc_batch* batch);
+/* Sets up, solves and reads `count` instances in one call (no reference
+ * counterpart), in parts of `part_instances` instances (0 = an eighth of
+ * them) that overlap: while part k solves (graph), part k+1 is set up and
+ * part k-1's results are copied into `results` (one gsc_result per
+ * instance, in order, buffers as for gsc_batch_read_all).  With autotune
+ * the first part chooses the launch shapes and the later parts reuse them.
+ * Returns when every result is in host memory; each result equals the
+ * instance's own gsc_problem solve.  A failing part fails the call, with
+ * the part's instance range in gsc_last_error. */
+int gsc_batch_run(gsc_context* ctx, uint32_t count, const gsc_model_desc* models, const gsc_query_desc* queries,
+                  const gsc_batch_options* options, uint32_t part_instances, gsc_result* results);
 
 /* ---- Serving loop ---------------------------------------------------------
  * No counterpart in the reference.  A loop thread serves K-invariance

@@ -141,3 +141,28 @@ def test_batch_with_instances_that_fill_the_gpu(ctx):
             assert got["iterations"] == want[i]["iterations"] and got["message"] == want[i]["message"]
         assert b.report()["max_iterations_run"] == max(w["iterations"] for w in want)
         b.close()
+
+
+@pytest.mark.parametrize("part", [1, 3, 0, 100])
+def test_batch_run_pipelined_matches_golden_and_solo(ctx, part):
+    """gsc_batch_run: parts that overlap set-up, solve and copies give every
+    instance its golden (reference) result or its solo solve, whatever the
+    part size (one instance a part, uneven parts, the default, one part)."""
+    names = sorted(INDEX)
+    cases = [INDEX[n]["case"] for n in names] + [C.random_instance(777, i) for i in range(3)]
+    got = G.run_batch(ctx, cases, autotune=(part == 3), part_instances=part)
+    for i, n in enumerate(names):
+        check_entry(got[i], n)
+    for i, c in enumerate(cases[len(names):], start=len(names)):
+        want = solo(ctx, c)
+        assert_same_result(got[i], want, f"part={part} instance {i}")
+        assert got[i]["iterations"] == want["iterations"] and got[i]["message"] == want["message"]
+
+
+def test_batch_run_reports_the_failing_part(ctx):
+    ok = INDEX["small"]["case"]
+    wide = C.unicycle_grid_case((300, 8, 8, 6), (3, 3))
+    with pytest.raises(G.GscError) as e:
+        G.run_batch(ctx, [ok, ok, wide, ok], part_instances=2)
+    assert e.value.status == 4 and "instances 2..3" in str(e.value)
+    check_entry(solo(ctx, ok), "small")
