@@ -205,8 +205,8 @@ int enqueue_iterations(gsc_batch* b, uint32_t count, uint32_t* launches) {
 // Time `reps` iterations from a fresh start under each candidate shape;
 // keep the fastest.  Candidates: one task per block (64 / 128 / 256
 // threads) and one task per warp (4 or 8 warps a block), each with one
-// block per task or a persistent grid, and two chunk sizes; a warp shape
-// whose staging does not fit a block's shared memory is left out.
+// block per task or a persistent grid, and chunks of 256 or 1,024 words; a
+// warp shape whose staging does not fit a block's shared memory is left out.
 int autotune(gsc_batch* b) {
     gsc_context* ctx = b->ctx;
     const int sms = sm_count(ctx);
@@ -215,7 +215,7 @@ int autotune(gsc_batch* b) {
     };
     const Trial trials[] = {{64, 0}, {128, 0}, {256, 0}, {128, 1}, {256, 1}};
     const uint32_t per_sm[] = {0, 4, 8, 16};
-    const uint32_t chunks[] = {1024, 4096};
+    const uint32_t chunks[] = {256, 1024};
     const uint32_t reps = 4;
     cudaEvent_t e0, e1;
     GSC_CU(ctx, cudaEventCreate(&e0));
