@@ -183,10 +183,6 @@ __device__ __forceinline__ int group_sync_or(int p) {
 // WARP: the task is one warp's (its own smem and s_meta), else the block's.
 // Every early return is taken by the whole group.
 constexpr unsigned long long kIncrementalRows = 16;
-// An incremental iteration after one that added at most one state per
-// kSparseRows x-rows: most blocks find no lost row, so a block tests its
-// windows before it stages anything.
-constexpr unsigned long long kSparseRows = 128;
 
 template <int WMAX, bool EXACTW, int NVMODE, bool WARP = false>
 __device__ __forceinline__ void sat_col_task(const GridInfo& g, const FusedFixArgs& a, uint32_t task,
@@ -223,8 +219,8 @@ __device__ __forceinline__ void sat_col_task(const GridInfo& g, const FusedFixAr
     // increasing acceleration order (warp ballot) with their v windows and
     // offset parts, the omega column's theta window and offset part, and
     // the control record (s_meta: [0] representatives, [1] theta window,
-    // [2] offset part, [3] iteration | incremental << 31 | sparse << 30, or
-    // all ones once stopped).
+    // [2] offset part, [3] iteration | incremental << 31, or all ones once
+    // stopped).
     int any = 0;
     for (uint32_t e0 = tid; e0 < nw; e0 += 2 * bd) {
         const uint32_t e1 = e0 + bd;
@@ -265,29 +261,26 @@ __device__ __forceinline__ void sat_col_task(const GridInfo& g, const FusedFixAr
         // that many rows), the iteration runs incrementally (phase B).
         const uint32_t stop = fc->stop, it = fc->iter, last = fc->last_new;
         const bool inc = it > 0 && static_cast<unsigned long long>(last) * kIncrementalRows <= g.rows;
-        const bool sparse = inc && static_cast<unsigned long long>(last) * kSparseRows <= g.rows;
         s_meta[1] = a.zt[i2 * mw + jw];
         s_meta[2] = a.offz[i2 * mw + jw];
-        s_meta[3] = stop ? 0xFFFFFFFFu : (it | (inc ? 0x80000000u : 0u) | (sparse ? 0x40000000u : 0u));
+        s_meta[3] = stop ? 0xFFFFFFFFu : (it | (inc ? 0x80000000u : 0u));
     }
     any = group_sync_or<WARP>(any);
     const uint32_t nrep = s_meta[0], ctl = s_meta[3];
     if (ctl == 0xFFFFFFFFu || !any || nrep == 0) return;
-    const uint32_t it = ctl & 0x3FFFFFFFu;
+    const uint32_t it = ctl & 0x7FFFFFFFu;
     const bool incremental = (ctl >> 31) != 0;
-    const bool sparse = ((ctl >> 30) & 1u) != 0;
     const uint32_t ze = s_meta[1], offz = s_meta[2];
     const uint32_t lz = lo16(ze), hz = hi16(ze);
     const uint32_t nz = (lz <= hz) ? hz - lz + 1 : n2 - lz + hz + 1;
 
-    // B. A second round, all in flight together: the dilated D' (and valid)
-    // rows at each representative's (theta, v) box corner, its class records
-    // and y tables, copied asynchronously into shared memory; and, in an
-    // incremental iteration, the rows of each representative's (theta, v)
-    // window that lost a cell (rowlost, from the finalize kernel).  A block
-    // with none, or a (representative, row) item whose y range has none, is
-    // skipped: its states still fail.  In a sparse iteration the windows are
-    // tested first and only a block with a lost row stages its rows.
+    // B. The dilated D' (and valid) rows at each representative's (theta, v)
+    // box corner, its class records and y tables, copied asynchronously into
+    // shared memory, all in flight together.  In an incremental iteration
+    // the rows of each representative's (theta, v) window that lost a cell
+    // (rowlost, from the finalize kernel) are gathered first: a block with
+    // none stages nothing and skips, and a (representative, row) item whose
+    // y range has none is skipped; their states still fail.
     auto stage = [&]() {
         for (uint32_t e = tid; e < nrep * nw; e += bd) {
             const uint32_t r = fdiv(e, g.magic_nw), rem = e - r * nw;
@@ -301,7 +294,7 @@ __device__ __forceinline__ void sat_col_task(const GridInfo& g, const FusedFixAr
             for (uint32_t e = lane; e < n1; e += 32) cp_async4(yts + r * n1 + e, a.yt + pl * n1 + e);
         }
     };
-    if (!sparse) stage();
+    if (!incremental) stage();
     int lost = 0;
     if (incremental) {
         const uint32_t* rl = a.rowlost + (it & 1) * a.rl_words;
@@ -321,19 +314,12 @@ __device__ __forceinline__ void sat_col_task(const GridInfo& g, const FusedFixAr
             lost |= m != 0;
         }
     }
-    if (sparse) {
+    if (incremental) {
         if (!group_sync_or<WARP>(lost)) return;
         stage();
-        cp_async_wait_all();
-        group_sync<WARP>();
-    } else {
-        cp_async_wait_all();
-        if (incremental) {
-            if (!group_sync_or<WARP>(lost)) return;
-        } else {
-            group_sync<WARP>();
-        }
     }
+    cp_async_wait_all();
+    group_sync<WARP>();
     if (tid == 0) atomicAdd(a.stats + kStatsCols * (it + 1) + 3, static_cast<unsigned long long>(nrep));
     // C. the (representative, row) items.
     unsigned long long ntest = 0;
