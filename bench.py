@@ -62,6 +62,8 @@ def parse():
     ap.add_argument("--serve-budget-gb", type=float, default=24.0)
     ap.add_argument("--sat-warp-tasks", type=int, default=0, choices=[0, 1],
                     help="served: one satisfaction task per warp in the serving loop's batched steps")
+    ap.add_argument("--serve-iterations-per-step", type=int, default=0,
+                    help="served: fixpoint iterations between the serving loop's host checks (0: the library's)")
     ap.add_argument("--host-loop", action="store_true",
                     help="batched: iterate from the host instead of one CUDA graph (for per-kernel profiling)")
     ap.add_argument("--trajectories", type=int, default=1 << 20)
@@ -510,7 +512,7 @@ def bench_served(args):
         return total, lat
 
     srv = G.Server(ctx, memory_budget=int(args.serve_budget_gb * (1 << 30)), max_slots=256,
-                   sat_warp_tasks=bool(args.sat_warp_tasks))
+                   sat_warp_tasks=bool(args.sat_warp_tasks), iterations_per_step=args.serve_iterations_per_step)
     # warm-up: a few queries of each model
     warm = [srv.submit(absn[k], C.random_query(models[k], args.seed + 1, i)) for i, k in enumerate(names * 4)]
     for t in warm:
@@ -527,6 +529,7 @@ def bench_served(args):
             rates.append({"fraction_of_saturation": f, "rate_qps": lam, "throughput_qps": n / tot,
                           "p50_ms": percentile(lat, 50), "p99_ms": percentile(lat, 99), "arrivals": arr})
     st = srv.stats()
+    st_ips = args.serve_iterations_per_step or 2
     srv.close()
 
     # Sequential plain solves: service time of every query (or a prefix).
@@ -560,7 +563,8 @@ def bench_served(args):
         "config": {"workload": f"served_{n}_queries_3_models_seed{args.seed}",
                    "models": {k: models[k]["name"] for k in names}, "queries": n,
                    "budget_gb": args.serve_budget_gb, "result_buffers_in_flight": depth,
-                   "sat_warp_tasks": args.sat_warp_tasks},
+                   "sat_warp_tasks": args.sat_warp_tasks,
+                   "iterations_per_step": st_ips},
         "saturation": {"throughput_qps": X, "p50_ms": percentile(sat_lat, 50), "p99_ms": percentile(sat_lat, 99)},
         "rates": rates,
         "e2e": {"value": X, "unit": "queries/s", "h2d_bytes_per_step": 0,
