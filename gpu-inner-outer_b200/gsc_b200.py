@@ -514,8 +514,12 @@ def run_batch(ctx: Context, cases, outs=None, autotune=True, part_instances=0, i
     keep = []
     nr_all = np.zeros((n, iter_capacity), np.uint64)
     nc_all = np.zeros((n, iter_capacity), np.uint64)
+    shape, ishape = (ctypes.c_uint32 * 4)(), (ctypes.c_uint32 * 2)()
     for i, c in enumerate(cases):
-        S = int(np.prod(grid_shape(c)[0], dtype=np.uint64))
+        st = lib().gsc_grid_shape(ctypes.byref(models[i]), shape, ishape)
+        if st != 0:
+            raise GscError(st, f"instance {i}")
+        S = shape[0] * shape[1] * shape[2] * shape[3]
         o = dict(outs[i]) if outs is not None else {
             "valid_mask": np.zeros(S, np.uint8), "candidate_mask": np.zeros(S, np.uint8),
             "reachable_mask": np.zeros(S, np.uint8), "controller": np.zeros(S, np.uint32),
