@@ -132,9 +132,13 @@ __global__ void __launch_bounds__(256) k_batch_finalize(const InstanceDesc* __re
         for (uint64_t e = b + threadIdx.x; e < end; e += blockDim.x) finalize_word(d.g, d.a, rprev, rnext, e, it, nr, nc);
         unsigned long long* row = d.a.stats + kStatsCols * it;
         add_counters(row, nr, nc);
-        __threadfence();
+        // The counters are atomics; the barrier orders them before the first
+        // thread's fence (cumulative) and ticket.
         __syncthreads();
-        if (threadIdx.x == 0) last = atomicAdd(&fc->ticket, 1u) == wl.fin_off[k + 1] - wl.fin_off[k] - 1;
+        if (threadIdx.x == 0) {
+            __threadfence();
+            last = atomicAdd(&fc->ticket, 1u) == wl.fin_off[k + 1] - wl.fin_off[k] - 1;
+        }
         __syncthreads();
         if (last && threadIdx.x == 0) {
             __threadfence();

@@ -199,12 +199,16 @@ __global__ void __launch_bounds__(256) k_fused_finalize(GridInfo g, FusedFixArgs
         finalize_word(g, a, rprev, rnext, e, it, nr, nc);
     unsigned long long* row = a.stats + kStatsCols * it;
     add_counters(row, nr, nc);
-    // Last block to finish: every block's counters are in (device-scope
-    // atomics, then a fence before taking a ticket).
+    // Last block to finish: every block's counters are in.  The counters are
+    // device-scope atomics; the barrier orders a block's atomics before its
+    // first thread's fence (cumulative) and ticket.  Nothing else the last
+    // block reads was written by this kernel's other blocks.
     __shared__ bool last;
-    __threadfence();
     __syncthreads();
-    if (threadIdx.x == 0) last = atomicAdd(&fc->ticket, 1u) == gridDim.x - 1;
+    if (threadIdx.x == 0) {
+        __threadfence();
+        last = atomicAdd(&fc->ticket, 1u) == gridDim.x - 1;
+    }
     __syncthreads();
     if (!last) return;
     if (threadIdx.x == 0) {
