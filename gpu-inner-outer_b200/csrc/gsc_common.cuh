@@ -188,6 +188,15 @@ __host__ __device__ __forceinline__ uint32_t pack8(uint32_t a, uint32_t b, uint3
 }
 
 // Fixpoint control block of one instance (device memory).
+// 4-byte asynchronous copy global -> shared (cp.async), complete after
+// cp_async_wait_all and the group's next barrier.
+__device__ __forceinline__ void cp_async4(void* smem_dst, const void* gmem_src) {
+    const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(smem_dst));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(gmem_src) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 struct FixControl {
     uint32_t iter;            // iterations completed
     uint32_t stop;            // 1 once a stop rule fired

@@ -137,14 +137,6 @@ __device__ __forceinline__ void dilate_position(const GridInfo& g, const bword* 
     }
 }
 
-// 4-byte asynchronous copy global -> shared (cp.async), complete after
-// cp_async_wait_all and the block's next barrier.
-__device__ __forceinline__ void cp_async4(void* smem_dst, const void* gmem_src) {
-    const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(smem_dst));
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(gmem_src) : "memory");
-}
-
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 // The group that runs one satisfaction task: the whole block, or one warp
 // (WARP), with its barrier and its barrier-with-OR.

@@ -455,18 +455,31 @@ __global__ void k_export(GridInfo g, ExportArgs a) {
 // [i0 + a, i0 + b] share the class (a, b).  Up to kClassMax classes with
 // |a|, |b| < 32, else the plane is marked irregular (0xFF) and tested state
 // by state.
+// One thread per plane; a block first copies its planes' x rows (contiguous)
+// into shared memory in one coalesced round, then each thread scans its row
+// there (a row stride of n0 words).
 __global__ void k_x_classes(GridInfo g, const uint32_t* __restrict__ xt, bword* __restrict__ out) {
+    extern __shared__ uint32_t s_xrows[];
     const uint32_t cw = 4 + kClassMax * g.W;
+    const uint32_t n0 = g.n[0];
     const uint64_t planes = static_cast<uint64_t>(g.slices) * g.M;
-    for (uint64_t plane = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; plane < planes;
-         plane += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    for (uint64_t first = blockIdx.x * static_cast<uint64_t>(blockDim.x); first < planes;
+         first += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint32_t np = static_cast<uint32_t>(min(static_cast<uint64_t>(blockDim.x), planes - first));
+        __syncthreads();   // the previous round's rows are read
+        for (uint32_t i = threadIdx.x; i < np * n0; i += blockDim.x) cp_async4(s_xrows + i, xt + first * n0 + i);
+        cp_async_wait_all();
+        __syncthreads();
+        if (threadIdx.x >= np) continue;
+        const uint64_t plane = first + threadIdx.x;
+        const uint32_t* row = s_xrows + threadIdx.x * n0;
         int cnt = 0, A[kClassMax], B[kClassMax];
         bword masks[kClassMax][kMaxWords];
         for (int c = 0; c < kClassMax; ++c)
             for (int w = 0; w < kMaxWords; ++w) masks[c][w] = 0;
         bool irregular = false;
         for (uint32_t i0 = 0; i0 < g.n[0] && !irregular; ++i0) {
-            const uint32_t xe = xt[plane * g.n[0] + i0];
+            const uint32_t xe = row[i0];
             if (xe == kReject) continue;
             const int a = static_cast<int>(lo16(xe)) - static_cast<int>(i0);
             const int b = static_cast<int>(hi16(xe)) - static_cast<int>(i0);
@@ -507,13 +520,21 @@ __global__ void k_x_classes(GridInfo g, const uint32_t* __restrict__ xt, bword* 
 constexpr int kThreadsReps = 128;
 
 __global__ void k_plane_reps(GridInfo g, const uint32_t* __restrict__ xt, const uint32_t* __restrict__ yt,
-                             const uint32_t* __restrict__ wt, uint8_t* __restrict__ rep, uint32_t* max_reps) {
+                             const uint32_t* __restrict__ wt, uint8_t* __restrict__ rep, uint32_t* max_reps,
+                             uint32_t stage_words) {
     // One warp per column; the lanes compare a pair of planes' x and y rows
     // together.  Representatives are kept in increasing order, so an input
-    // maps to the lowest earlier input with the same rows and v box.
+    // maps to the lowest earlier input with the same rows and v box.  With
+    // stage_words (= ma * (n0 + n1)), the column's x rows and then its y rows
+    // are first copied into the warp's shared memory in one round and
+    // compared there; else they are compared in global memory.
+    extern __shared__ uint32_t s_rows[];
     __shared__ uint8_t s_reps[kThreadsReps / 32][256];
     const uint32_t lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     uint8_t* reps = s_reps[wib];
+    uint32_t* rows = s_rows + static_cast<uint64_t>(wib) * stage_words;
+    const uint32_t n0 = g.n[0], n1 = g.n[1], ma = g.ma;
+    const uint32_t nx = ma * n0;
     const uint64_t columns = static_cast<uint64_t>(g.slices) * g.mw;
     const uint64_t wstride = static_cast<uint64_t>(gridDim.x) * (blockDim.x >> 5);
     uint32_t most = 0;
@@ -521,19 +542,27 @@ __global__ void k_plane_reps(GridInfo g, const uint32_t* __restrict__ xt, const 
         // Planes are ((i2 * n3 + i3) * M + j) with j = ja + ma * jw, so column
         // col = (i2 * n3 + i3) * mw + jw starts at plane col * ma.
         const uint32_t i3 = static_cast<uint32_t>((col / g.mw) % g.n[3]);
-        const uint64_t p0 = col * g.ma;
+        const uint64_t p0 = col * ma;
+        const uint32_t* X = xt + p0 * n0;
+        const uint32_t* Y = yt + p0 * n1;
+        if (stage_words) {
+            for (uint32_t i = lane; i < nx; i += 32) cp_async4(rows + i, X + i);
+            for (uint32_t i = lane; i < ma * n1; i += 32) cp_async4(rows + nx + i, Y + i);
+            cp_async_wait_all();
+            __syncwarp();
+            X = rows;
+            Y = rows + nx;
+        }
         uint32_t nrep = 0;
-        for (uint32_t ja = 0; ja < g.ma; ++ja) {
-            const uint32_t we = wt[i3 * g.ma + ja];
+        for (uint32_t ja = 0; ja < ma; ++ja) {
+            const uint32_t we = wt[i3 * ma + ja];
             uint32_t r = ja;
             for (uint32_t k = 0; k < nrep; ++k) {
                 const uint32_t jb = reps[k];
-                if (wt[i3 * g.ma + jb] != we) continue;
+                if (wt[i3 * ma + jb] != we) continue;
                 bool same = true;
-                for (uint32_t i = lane; i < g.n[0]; i += 32)
-                    same = same && xt[(p0 + jb) * g.n[0] + i] == xt[(p0 + ja) * g.n[0] + i];
-                for (uint32_t i = lane; i < g.n[1]; i += 32)
-                    same = same && yt[(p0 + jb) * g.n[1] + i] == yt[(p0 + ja) * g.n[1] + i];
+                for (uint32_t i = lane; i < n0; i += 32) same = same && X[jb * n0 + i] == X[ja * n0 + i];
+                for (uint32_t i = lane; i < n1; i += 32) same = same && Y[jb * n1 + i] == Y[ja * n1 + i];
                 if (__all_sync(0xFFFFFFFFu, same)) {
                     r = jb;
                     break;
@@ -633,7 +662,11 @@ cudaError_t launch_stored_build(const GridInfo& g, const StoredBuildArgs& a, cud
 }
 
 cudaError_t launch_x_classes(const GridInfo& g, const uint32_t* xt, bword* xcls, cudaStream_t st) {
-    k_x_classes<<<blocks_for(static_cast<uint64_t>(g.slices) * g.M, 128), 128, 0, st>>>(g, xt, xcls);
+    // Threads (planes) a block: as many rows as fit 44 KB of shared memory, 32 to 128.
+    uint32_t tpb = static_cast<uint32_t>((44u * 1024u) / (4u * std::max<uint32_t>(g.n[0], 1u)));
+    tpb = std::min<uint32_t>(128u, std::max<uint32_t>(32u, tpb & ~31u));
+    if (4ull * tpb * g.n[0] > 48 * 1024) return cudaErrorInvalidValue;
+    k_x_classes<<<blocks_for(static_cast<uint64_t>(g.slices) * g.M, tpb), tpb, 4ull * tpb * g.n[0], st>>>(g, xt, xcls);
     return cudaGetLastError();
 }
 
@@ -642,7 +675,12 @@ cudaError_t launch_plane_reps(const GridInfo& g, const uint32_t* xt, const uint3
     const uint64_t warps = static_cast<uint64_t>(g.slices) * g.mw;
     uint64_t b = (warps + kThreadsReps / 32 - 1) / (kThreadsReps / 32);
     if (b > 8192) b = 8192;
-    k_plane_reps<<<static_cast<unsigned int>(b), kThreadsReps, 0, st>>>(g, xt, yt, wt, xrep, max_reps);
+    // Stage a column's rows in shared memory when they fit 44 KB a block (the
+    // default 48 KB less the representatives' static arrays).
+    const uint64_t words = static_cast<uint64_t>(g.ma) * (g.n[0] + g.n[1]);
+    const uint32_t stage = words * 4 * (kThreadsReps / 32) <= 44 * 1024 ? static_cast<uint32_t>(words) : 0u;
+    k_plane_reps<<<static_cast<unsigned int>(b), kThreadsReps, 4ull * stage * (kThreadsReps / 32), st>>>(
+        g, xt, yt, wt, xrep, max_reps, stage);
     return cudaGetLastError();
 }
 
