@@ -155,6 +155,33 @@ void device_release_all(gsc_context* ctx, DevicePool* pool, std::vector<std::pai
     bytes = 0;
 }
 
+cudaError_t pinned_get(gsc_context* ctx, size_t bytes, void** p, size_t* got) {
+    {
+        std::lock_guard<std::mutex> lk(ctx->pin_mu);
+        auto it = ctx->pin_free.lower_bound(bytes);
+        if (it != ctx->pin_free.end() && it->first <= 2 * bytes + (64u << 10)) {
+            *p = it->second;
+            *got = it->first;
+            ctx->pin_free.erase(it);
+            return cudaSuccess;
+        }
+    }
+    *got = bytes;
+    return cudaMallocHost(p, bytes);
+}
+
+void pinned_put(gsc_context* ctx, void* p, size_t bytes) {
+    if (!p) return;
+    std::lock_guard<std::mutex> lk(ctx->pin_mu);
+    ctx->pin_free.emplace(bytes, p);
+}
+
+void pinned_trim(gsc_context* ctx) {
+    std::lock_guard<std::mutex> lk(ctx->pin_mu);
+    for (auto& kv : ctx->pin_free) cudaFreeHost(kv.second);
+    ctx->pin_free.clear();
+}
+
 int abstraction_enqueue(gsc_abstraction* a, cudaStream_t st, std::vector<std::pair<void*, uint64_t>>& tmp) {
     gsc_context* ctx = a->ctx;
     const GridInfo& g = a->g;
@@ -405,6 +432,7 @@ void gsc_context_destroy(gsc_context* ctx) {
     for (auto e : ctx->setup_ev)
         if (e) cudaEventDestroy(e);
     ctx->pool.reset();
+    pinned_trim(ctx);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -413,6 +441,7 @@ int gsc_context_trim(gsc_context* ctx) {
     if (!ctx) return GSC_ERR_INVALID_ARGUMENT;
     if (cudaSetDevice(ctx->device) != cudaSuccess) return GSC_ERR_CUDA;
     if (ctx->pool) ctx->pool->trim();
+    pinned_trim(ctx);
     return GSC_OK;
 }
 

@@ -90,6 +90,11 @@ uint32_t wmax_of(uint32_t w) { return w <= 1 ? 1 : w == 2 ? 2 : w <= 4 ? 4 : 8; 
 
 }  // namespace gsc_api
 
+struct gsc_batch;
+namespace {
+void release_batch_graph(gsc_batch* b);
+}
+
 struct gsc_batch {
     gsc_context* ctx = nullptr;
     DevicePool* pool = nullptr;   // the context's caching pool
@@ -115,8 +120,15 @@ struct gsc_batch {
     InstanceDesc* hdesc_pin = nullptr;
     uint32_t* hlist_pin = nullptr;   // [2][count + 4 * (count + 1)]
     bool lists_uploaded = false;
-    void* pin_early = nullptr;   // hplans, hrunning, hfc
-    void* pin_late = nullptr;    // hstats, hdesc_pin, hlist_pin
+    void* pin_early = nullptr;   // hplans, hrunning, hfc (from the context's pinned cache)
+    void* pin_late = nullptr;    // hstats, hdesc_pin, hlist_pin (from the context's pinned cache)
+    size_t pin_early_bytes = 0, pin_late_bytes = 0;
+    // Between the two set-up phases (batch_begin, batch_finish): the
+    // abstractions' temporary tables, the set-up streams in use and an
+    // event per stream after its stage-1 work.
+    std::vector<std::vector<std::pair<void*, uint64_t>>> setup_tmp;
+    uint32_t setup_base = 0, setup_count = gsc_context::kSetupStreams;
+    cudaEvent_t stage1_ev[gsc_context::kSetupStreams] = {};
     std::vector<uint32_t> small;     // indices of the instances the batched kernels run
     std::vector<BigInstance> big;    // the instances the one-problem kernels run
     WorkTotals tot{}, tot_all{};
@@ -131,13 +143,16 @@ struct gsc_batch {
     gsc_batch_report t{};
     uint32_t last_launches = 0;
     ~gsc_batch() {
-        if (exec) cudaGraphExecDestroy(exec);
-        if (graph) cudaGraphDestroy(graph);
+        release_batch_graph(this);
         probs.clear();
         abs.clear();
         device_release_all(ctx, pool, own, own_bytes);
-        if (pin_early) cudaFreeHost(pin_early);
-        if (pin_late) cudaFreeHost(pin_late);
+        uint64_t tb = 0;
+        for (auto& t : setup_tmp) device_release_all(ctx, pool, t, tb);
+        pinned_put(ctx, pin_early, pin_early_bytes);
+        pinned_put(ctx, pin_late, pin_late_bytes);
+        for (auto e : stage1_ev)
+            if (e) cudaEventDestroy(e);
     }
 };
 
@@ -260,13 +275,17 @@ int autotune(gsc_batch* b) {
     return upload_list(b, best_shape.chunk);
 }
 
-int build_batch_graph(gsc_batch* b) {
-    gsc_context* ctx = b->ctx;
-    cudaStream_t st = ctx->stream;
+void release_batch_graph(gsc_batch* b) {
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
     b->exec = nullptr;
     b->graph = nullptr;
+}
+
+int build_batch_graph(gsc_batch* b) {
+    gsc_context* ctx = b->ctx;
+    cudaStream_t st = ctx->stream;
+    release_batch_graph(b);
     const int sms = sm_count(ctx);
     cudaGraph_t g = nullptr, ginit = nullptr;
     GSC_CU(ctx, cudaGraphCreate(&g, 0));
@@ -300,24 +319,41 @@ int build_batch_graph(gsc_batch* b) {
     return GSC_OK;
 }
 
+// Carves `bytes` (rounded up to 16) off the front of a pinned block.
+char* carve16(char*& p, size_t bytes) {
+    char* r = p;
+    p += (bytes + 15) & ~size_t(15);
+    return r;
+}
+
 // The context's set-up streams for one batch (instance i on stream
-// i % kSetupStreams), so that the small set-up kernels of different
+// base + i % count), so that the small set-up kernels of different
 // instances run side by side.  They have the device's highest stream
 // priority: in a pipelined run their blocks go ahead of a solve that fills
 // the GPU.  They are created once per context; a batch that fails drains
-// them before its memory is released, a batch that succeeds only joins
-// them into the context stream (no host wait).
+// the streams it used before its memory is released, a batch that succeeds
+// only joins them into the context stream (no host wait).  The two set-up
+// phases of a batch (batch_begin, batch_finish) each hold one of these over
+// the same streams.
 struct SetupStreams {
     static constexpr int kSetupStreams = gsc_context::kSetupStreams;
     gsc_context* ctx = nullptr;
+    uint32_t base = 0, count = kSetupStreams;
     bool ok = false;
     ~SetupStreams() {
         if (ok || !ctx) return;
-        for (auto x : ctx->setup)
-            if (x) cudaStreamSynchronize(x);
+        for (uint32_t k = 0; k < count; ++k)
+            if (ctx->setup[base + k]) cudaStreamSynchronize(ctx->setup[base + k]);
     }
-    cudaError_t create(gsc_context* c, cudaStream_t after) {
+    void attach(gsc_context* c, uint32_t b0, uint32_t n) {
         ctx = c;
+        base = b0;
+        count = n;
+    }
+    // Creates the context's streams at first use; the streams in use start
+    // after the work queued on `after` so far.
+    cudaError_t create(gsc_context* c, cudaStream_t after, uint32_t b0, uint32_t n) {
+        attach(c, b0, n);
         cudaError_t r = cudaSuccess;
         if (!ctx->setup[0]) {
             int least = 0, greatest = 0;
@@ -329,46 +365,56 @@ struct SetupStreams {
             if (r != cudaSuccess) return r;
         }
         r = cudaEventRecord(ctx->setup_ev[kSetupStreams], after);
-        for (auto x : ctx->setup)
-            if (r == cudaSuccess) r = cudaStreamWaitEvent(x, ctx->setup_ev[kSetupStreams], 0);
+        for (uint32_t k = 0; k < count; ++k)
+            if (r == cudaSuccess) r = cudaStreamWaitEvent(ctx->setup[base + k], ctx->setup_ev[kSetupStreams], 0);
         return r;
     }
-    cudaStream_t of(uint32_t i) const { return ctx->setup[i % kSetupStreams]; }
-    cudaError_t sync() {
-        for (auto x : ctx->setup) {
-            const cudaError_t r = cudaStreamSynchronize(x);
+    cudaStream_t of(uint32_t i) const { return ctx->setup[base + i % count]; }
+    // evs[k] marks what stream base + k has queued so far.
+    cudaError_t mark(cudaEvent_t* evs) {
+        for (uint32_t k = 0; k < count; ++k) {
+            cudaError_t r = cudaSuccess;
+            if (!evs[k]) r = cudaEventCreateWithFlags(&evs[k], cudaEventDisableTiming);
+            if (r == cudaSuccess) r = cudaEventRecord(evs[k], ctx->setup[base + k]);
             if (r != cudaSuccess) return r;
         }
         return cudaSuccess;
     }
-    // `st` waits for everything enqueued on the set-up streams.
+    // Host wait for the marks (later work on the streams is not waited for).
+    cudaError_t wait(cudaEvent_t* evs) {
+        for (uint32_t k = 0; k < count; ++k) {
+            const cudaError_t r = cudaEventSynchronize(evs[k]);
+            if (r != cudaSuccess) return r;
+        }
+        return cudaSuccess;
+    }
+    // `st` waits for everything enqueued on the streams in use.
     cudaError_t join(cudaStream_t st) {
-        for (int k = 0; k < kSetupStreams; ++k) {
-            cudaError_t r = cudaEventRecord(ctx->setup_ev[k], ctx->setup[k]);
-            if (r == cudaSuccess) r = cudaStreamWaitEvent(st, ctx->setup_ev[k], 0);
+        for (uint32_t k = 0; k < count; ++k) {
+            cudaError_t r = cudaEventRecord(ctx->setup_ev[base + k], ctx->setup[base + k]);
+            if (r == cudaSuccess) r = cudaStreamWaitEvent(st, ctx->setup_ev[base + k], 0);
             if (r != cudaSuccess) return r;
         }
         return cudaSuccess;
     }
 };
 
-int batch_create(gsc_batch* b, uint32_t count, const gsc_model_desc* models, const gsc_query_desc* queries,
-                 const gsc_batch_options* opt) {
+// Set-up phase 1: stage 1 of every instance (abstraction tables, masks,
+// boxes, x classes, representatives, plan records) queued on set-up streams
+// base..base+streams-1, with no host wait.
+int batch_begin(gsc_batch* b, uint32_t count, const gsc_model_desc* models, const gsc_query_desc* queries,
+                uint32_t base, uint32_t streams) {
     gsc_context* ctx = b->ctx;
-    cudaStream_t st = ctx->stream;
     b->pool = ctx->pool.get();
+    b->setup_base = base;
+    b->setup_count = streams;
     SetupStreams ss;
-    GSC_CU(ctx, ss.create(ctx, st));
-    // Pinned host memory in two carved allocations (pinning is slow per call).
-    auto carve16 = [](char*& p, size_t bytes) {
-        char* r = p;
-        p += (bytes + 15) & ~size_t(15);
-        return r;
-    };
+    GSC_CU(ctx, ss.create(ctx, ctx->stream, base, streams));
+    // Pinned host memory in two carved blocks from the context's cache.
     {
         const size_t bytes = ((sizeof(PlanRecord) * count + 15) & ~size_t(15)) + 16 +
                              ((sizeof(FixControl) * count + 15) & ~size_t(15));
-        GSC_CU(ctx, cudaMallocHost(&b->pin_early, bytes));
+        GSC_CU(ctx, pinned_get(ctx, bytes, &b->pin_early, &b->pin_early_bytes));
         char* q = static_cast<char*>(b->pin_early);
         b->hplans = reinterpret_cast<PlanRecord*>(carve16(q, sizeof(PlanRecord) * count));
         b->hrunning = reinterpret_cast<uint32_t*>(carve16(q, sizeof(uint32_t)));
@@ -381,8 +427,7 @@ int batch_create(gsc_batch* b, uint32_t count, const gsc_model_desc* models, con
         b->hfc_dev = reinterpret_cast<FixControl*>(dq + (reinterpret_cast<char*>(b->hfc) -
                                                           static_cast<char*>(b->pin_early)));
     }
-    std::vector<std::vector<std::pair<void*, uint64_t>>> tmp(count);
-    // Stage 1 of every instance, then one wait for all plan records.
+    b->setup_tmp.assign(count, {});
     for (uint32_t i = 0; i < count; ++i) {
         std::unique_ptr<gsc_abstraction> a(new (std::nothrow) gsc_abstraction());
         if (!a) return GSC_ERR_OUT_OF_MEMORY;
@@ -394,7 +439,7 @@ int batch_create(gsc_batch* b, uint32_t count, const gsc_model_desc* models, con
         if (s != GSC_OK) return fail(ctx, s, "instance " + std::to_string(i) + ": " + err);
         if (a->g.rows * a->g.W >= 0xFFFFFFFFull)
             return fail(ctx, GSC_ERR_UNSUPPORTED, "instance " + std::to_string(i) + ": grid too large for a batch");
-        GSC_TRY(abstraction_enqueue(a.get(), ss.of(i), tmp[i]));
+        GSC_TRY(abstraction_enqueue(a.get(), ss.of(i), b->setup_tmp[i]));
         b->abs.push_back(std::move(a));
     }
     for (uint32_t i = 0; i < count; ++i) {
@@ -412,11 +457,26 @@ int batch_create(gsc_batch* b, uint32_t count, const gsc_model_desc* models, con
         if (s != GSC_OK) return fail(ctx, s, "instance " + std::to_string(i) + ": " + ctx->last_error);
         b->probs.push_back(std::move(p));
     }
-    GSC_CU(ctx, ss.sync());
-    for (uint32_t i = 0; i < count; ++i) {
+    GSC_CU(ctx, ss.mark(b->stage1_ev));
+    ss.ok = true;
+    return GSC_OK;
+}
+
+// Set-up phase 2: one host wait for the stage-1 work of batch_begin (the
+// plan records), then stage 2 of every instance, the instance table, work
+// lists and launch shapes (autotuned on request).
+int batch_finish(gsc_batch* b, const gsc_batch_options* opt) {
+    gsc_context* ctx = b->ctx;
+    cudaStream_t st = ctx->stream;
+    const uint32_t count = static_cast<uint32_t>(b->probs.size());
+    SetupStreams ss;
+    ss.attach(ctx, b->setup_base, b->setup_count);
+    GSC_CU(ctx, ss.wait(b->stage1_ev));
+    for (auto& t : b->setup_tmp) {
         uint64_t tb = 0;
-        device_release_all(ctx, b->pool, tmp[i], tb);
+        device_release_all(ctx, b->pool, t, tb);
     }
+    b->setup_tmp.clear();
     for (uint32_t i = 0; i < count; ++i) {
         gsc_problem* p = b->probs[i].get();
         int s = problem_plan(p);
@@ -437,7 +497,7 @@ int batch_create(gsc_batch* b, uint32_t count, const gsc_model_desc* models, con
     {
         const size_t bytes = ((sizeof(unsigned long long) * stats_words + 15) & ~size_t(15)) +
                              ((sizeof(InstanceDesc) * count + 15) & ~size_t(15)) + ((list_bytes + 15) & ~size_t(15));
-        GSC_CU(ctx, cudaMallocHost(&b->pin_late, bytes));
+        GSC_CU(ctx, pinned_get(ctx, bytes, &b->pin_late, &b->pin_late_bytes));
         char* q = static_cast<char*>(b->pin_late);
         b->hstats = reinterpret_cast<unsigned long long*>(carve16(q, sizeof(unsigned long long) * stats_words));
         b->hdesc_pin = reinterpret_cast<InstanceDesc*>(carve16(q, sizeof(InstanceDesc) * count));
@@ -520,30 +580,22 @@ int batch_create(gsc_batch* b, uint32_t count, const gsc_model_desc* models, con
     return GSC_OK;
 }
 
-// The reads of every instance of a solved batch: one host wait for `ctl`
-// (which follows the solve), after which the control records are in pinned
-// memory (the status kernel stores them there after every iteration; the
-// reachable set's buffer depends on the iteration count); the result fields
-// they give; then every unpack kernel and every copy on `st` (the copies back
-// to back), not waited for.
-// rows[i]: per-iteration counter rows staged for instance i.
-// unpacked: the reachable sets were unpacked already (launch_unpack_reach).
-int read_begin(gsc_batch* b, gsc_result* out, cudaStream_t ctl, cudaStream_t st, std::vector<uint32_t>& rows,
-               bool unpacked = false) {
+int batch_create(gsc_batch* b, uint32_t count, const gsc_model_desc* models, const gsc_query_desc* queries,
+                 const gsc_batch_options* opt) {
+    GSC_TRY(batch_begin(b, count, models, queries, 0, gsc_context::kSetupStreams));
+    return batch_finish(b, opt);
+}
+
+// Queues the copies of every instance's results on `st` (which must follow
+// the solve and the unpacking of the reachable sets): valid, candidate and
+// reachable masks, controller, reach_step, and rows[i] + 1 rows of
+// per-iteration counters into the pinned staging.
+int read_enqueue(gsc_batch* b, const gsc_result* out, cudaStream_t st, const std::vector<uint32_t>& rows) {
     gsc_context* ctx = b->ctx;
-    const size_t n = b->probs.size();
-    GSC_CU(ctx, cudaStreamSynchronize(ctl));
-    const FixControl* fc = b->hfc;
-    for (size_t i = 0; i < n && !unpacked; ++i) {
-        gsc_problem* p = b->probs[i].get();
-        if (out[i].reachable_mask)
-            GSC_CU(ctx, launch_unpack_bits(p->g, (fc[i].iter & 1) ? p->reach1 : p->reach0, p->reach8, st));
-    }
-    rows.assign(n, 0);
-    for (size_t i = 0; i < n; ++i) {
+    for (size_t i = 0; i < b->probs.size(); ++i) {
         gsc_problem* p = b->probs[i].get();
         const GridInfo& g = p->g;
-        gsc_result* r = out + i;
+        const gsc_result* r = out + i;
         if (r->valid_mask) GSC_CU(ctx, cudaMemcpyAsync(r->valid_mask, p->valid, g.S, cudaMemcpyDeviceToHost, st));
         if (r->candidate_mask)
             GSC_CU(ctx, cudaMemcpyAsync(r->candidate_mask, p->cand, g.S, cudaMemcpyDeviceToHost, st));
@@ -553,36 +605,46 @@ int read_begin(gsc_batch* b, gsc_result* out, cudaStream_t ctl, cudaStream_t st,
             GSC_CU(ctx, cudaMemcpyAsync(r->controller, p->controller, g.S * 4, cudaMemcpyDeviceToHost, st));
         if (r->reach_step)
             GSC_CU(ctx, cudaMemcpyAsync(r->reach_step, p->reach_step, g.S * 4, cudaMemcpyDeviceToHost, st));
-        rows[i] = std::min<uint32_t>({fc[i].iter, r->iter_capacity, p->stats_cap - 1});
         if (rows[i] && (r->iter_new_reachable || r->iter_new_certified))
             GSC_CU(ctx, cudaMemcpyAsync(b->hstats + b->stats_off[i], p->stats,
                                         sizeof(unsigned long long) * kStatsCols * (rows[i] + 1),
                                         cudaMemcpyDeviceToHost, st));
-        else
-            rows[i] = 0;
+    }
+    return GSC_OK;
+}
+
+// Counter rows of instance i that a read returns: the iterations run, at most
+// the caller's capacity and the staged rows.
+uint32_t read_rows(const gsc_batch* b, const gsc_result* r, size_t i) {
+    return std::min<uint32_t>({b->hfc[i].iter, r->iter_capacity, b->probs[i]->stats_cap - 1});
+}
+
+// Once the solve has finished: the result fields from the control records
+// (the status kernel stores them in pinned memory after every iteration)
+// and, once the copies of read_enqueue have finished, the per-iteration
+// counters.
+void read_finish(gsc_batch* b, gsc_result* out) {
+    for (size_t i = 0; i < b->probs.size(); ++i) {
+        const gsc_problem* p = b->probs[i].get();
+        const GridInfo& g = p->g;
+        const FixControl& fc = b->hfc[i];
+        gsc_result* r = out + i;
         for (int d = 0; d < 4; ++d) r->shape[d] = g.n[d];
         r->input_shape[0] = g.ma;
         r->input_shape[1] = g.mw;
         r->states = g.S;
         r->inputs = g.M;
         r->pairs = g.S * g.M;
-        r->iterations = fc[i].iter;
-        r->converged = static_cast<int32_t>(fc[i].converged);
-        r->message = static_cast<int32_t>(fc[i].message ? fc[i].message : GSC_MSG_MAX_ITERATIONS);
-        r->certified_candidates = fc[i].certified;
-        r->reachable_states = fc[i].reachable;
-        r->candidate_count = fc[i].candidate_count;
-        r->valid_count = fc[i].valid_count;
-    }
-    return GSC_OK;
-}
-
-// After the stream of read_begin finished: the per-iteration counters.
-void read_finish(gsc_batch* b, gsc_result* out, const std::vector<uint32_t>& rows) {
-    for (size_t i = 0; i < rows.size(); ++i) {
-        gsc_result* r = out + i;
+        r->iterations = fc.iter;
+        r->converged = static_cast<int32_t>(fc.converged);
+        r->message = static_cast<int32_t>(fc.message ? fc.message : GSC_MSG_MAX_ITERATIONS);
+        r->certified_candidates = fc.certified;
+        r->reachable_states = fc.reachable;
+        r->candidate_count = fc.candidate_count;
+        r->valid_count = fc.valid_count;
         const unsigned long long* hs = b->hstats + b->stats_off[i];
-        for (uint32_t k = 0; k < rows[i]; ++k) {
+        const uint32_t rows = read_rows(b, r, i);
+        for (uint32_t k = 0; k < rows; ++k) {
             if (r->iter_new_reachable) r->iter_new_reachable[k] = hs[kStatsCols * (k + 1)];
             if (r->iter_new_certified) r->iter_new_certified[k] = hs[kStatsCols * (k + 1) + 1];
         }
@@ -697,18 +759,24 @@ int gsc_batch_timings(gsc_batch* b, gsc_batch_report* out) {
     return GSC_OK;
 }
 
-// Streams of a pipelined run; every exit drains them before the parts'
-// memory is released.
+// Streams of a pipelined run.  Every exit drains them, the context stream
+// and the set-up streams before the parts' memory is released.
 struct RunStreams {
-    cudaStream_t solve = nullptr, copy = nullptr, ctl = nullptr;
+    gsc_context* ctx = nullptr;
+    cudaStream_t solve[2] = {nullptr, nullptr}, copy = nullptr;
     cudaEvent_t ready = nullptr;
     std::vector<cudaEvent_t> solved;
     ~RunStreams() {
-        for (auto s : {solve, copy, ctl})
+        for (auto s : {solve[0], solve[1], copy})
             if (s) {
                 cudaStreamSynchronize(s);
                 cudaStreamDestroy(s);
             }
+        if (ctx) {
+            cudaStreamSynchronize(ctx->stream);
+            for (auto s : ctx->setup)
+                if (s) cudaStreamSynchronize(s);
+        }
         if (ready) cudaEventDestroy(ready);
         for (auto e : solved) cudaEventDestroy(e);
     }
@@ -720,68 +788,90 @@ int gsc_batch_run(gsc_context* ctx, uint32_t count, const gsc_model_desc* models
     cudaGetLastError();
     GSC_CU(ctx, cudaSetDevice(ctx->device));
     const uint32_t part = part_instances ? part_instances : std::max<uint32_t>(1, (count + 7) / 8);
+    const uint32_t nparts = (count + part - 1) / part;
     const int sms = sm_count(ctx);
     std::vector<std::unique_ptr<gsc_batch>> parts;   // destroyed after `rs` drained the streams
-    std::vector<uint32_t> first;
-    std::vector<std::vector<uint32_t>> rows;
     RunStreams rs;
-    GSC_CU(ctx, cudaStreamCreateWithFlags(&rs.solve, cudaStreamNonBlocking));
+    rs.ctx = ctx;
+    for (auto& x : rs.solve) GSC_CU(ctx, cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking));
     GSC_CU(ctx, cudaStreamCreateWithFlags(&rs.copy, cudaStreamNonBlocking));
-    GSC_CU(ctx, cudaStreamCreateWithFlags(&rs.ctl, cudaStreamNonBlocking));
     GSC_CU(ctx, cudaEventCreateWithFlags(&rs.ready, cudaEventDisableTiming));
     gsc_batch_options opt = options ? *options : gsc_batch_options{};
-    // Reads of part k: after its solve, the control records on `ctl`, the
-    // unpacks and copies on `copy`.
-    auto read_part = [&](size_t k) -> int {
-        GSC_CU(ctx, cudaStreamWaitEvent(rs.ctl, rs.solved[k], 0));
-        GSC_CU(ctx, cudaStreamWaitEvent(rs.copy, rs.solved[k], 0));
-        return read_begin(parts[k].get(), results + first[k], rs.ctl, rs.copy, rows[k], true);
+    auto range = [&](uint32_t k) {
+        const uint32_t f = k * part, n = std::min(part, count - f);
+        return "instances " + std::to_string(f) + ".." + std::to_string(f + n - 1) + ": ";
     };
-    for (uint32_t f = 0; f < count; f += part) {
-        const uint32_t n = std::min(part, count - f);
+    // Stage 1 of part k, queued on half of the set-up streams (even parts
+    // the first half, odd parts the second), so that the next part's stage 1
+    // and this part's stage 2 do not queue behind each other.
+    auto begin_part = [&](uint32_t k) -> int {
+        const uint32_t f = k * part, n = std::min(part, count - f);
         std::unique_ptr<gsc_batch> b(new (std::nothrow) gsc_batch());
         if (!b) return GSC_ERR_OUT_OF_MEMORY;
         b->ctx = ctx;
-        int s = batch_create(b.get(), n, models + f, queries + f, &opt);
-        if (s == GSC_OK && !b->exec) s = build_batch_graph(b.get());
-        if (s != GSC_OK) {
-            cudaStreamSynchronize(ctx->stream);   // nothing of the failed part may still be in flight
-            return fail(ctx, s, "instances " + std::to_string(f) + ".." + std::to_string(f + n - 1) + ": " +
-                                    ctx->last_error);
-        }
-        if (parts.empty() && opt.autotune) {
+        parts.push_back(std::move(b));
+        const uint32_t half = gsc_context::kSetupStreams / 2;
+        const int s = batch_begin(parts.back().get(), n, models + f, queries + f, (k & 1) * half, half);
+        return s == GSC_OK ? GSC_OK : fail(ctx, s, range(k) + ctx->last_error);
+    };
+    GSC_TRY(begin_part(0));
+    for (uint32_t k = 0; k < nparts; ++k) {
+        const uint32_t f = k * part, n = std::min(part, count - f);
+        // The next part's stage 1 is queued before this part's plan wait,
+        // except while this part tunes the launch shapes (its trials run alone).
+        const bool tunes = k == 0 && opt.autotune;
+        if (!tunes && k + 1 < nparts) GSC_TRY(begin_part(k + 1));
+        gsc_batch* b = parts[k].get();
+        int s = batch_finish(b, &opt);
+        if (s == GSC_OK && !b->exec) s = build_batch_graph(b);
+        if (s != GSC_OK) return fail(ctx, s, range(k) + ctx->last_error);
+        if (tunes) {
             // Later parts take the first part's shapes: no trials beside a solve.
             opt.autotune = 0;
             opt.sat_threads = b->shape.sat_threads;
             opt.sat_blocks_per_sm = b->shape.sat_blocks / static_cast<uint32_t>(sms);
             opt.chunk_words = b->shape.chunk;
             opt.sat_warp_tasks = b->shape.warp;
+            if (k + 1 < nparts) GSC_TRY(begin_part(k + 1));
         }
-        // The solve follows the part's set-up (joined into the context stream).
+        // The solve follows the part's set-up (joined into the context
+        // stream).  Parts alternate between two solve streams, so that a
+        // part's last iterations, which few instances still run, share the
+        // GPU with the next part's solve.
+        cudaStream_t solve = rs.solve[k & 1];
         GSC_CU(ctx, cudaEventRecord(rs.ready, ctx->stream));
-        GSC_CU(ctx, cudaStreamWaitEvent(rs.solve, rs.ready, 0));
-        GSC_CU(ctx, cudaGraphLaunch(b->exec, rs.solve));
+        GSC_CU(ctx, cudaStreamWaitEvent(solve, rs.ready, 0));
+        GSC_CU(ctx, cudaGraphLaunch(b->exec, solve));
         // Unpack the reachable sets on the solve stream too, so the copy
         // stream carries copies only (its kernels would wait for SMs behind
         // the next part's solve).
         for (uint32_t i = 0; i < n; ++i) {
             gsc_problem* p = b->probs[i].get();
             if (results[f + i].reachable_mask)
-                GSC_CU(ctx, launch_unpack_reach(p->g, p->fc, p->reach0, p->reach1, p->reach8, rs.solve));
+                GSC_CU(ctx, launch_unpack_reach(p->g, p->fc, p->reach0, p->reach1, p->reach8, solve));
         }
         cudaEvent_t ev = nullptr;
         GSC_CU(ctx, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
         rs.solved.push_back(ev);
-        GSC_CU(ctx, cudaEventRecord(ev, rs.solve));
-        parts.push_back(std::move(b));
-        first.push_back(f);
-        rows.emplace_back();
-        // The previous part is read while this one solves and the next is set up.
-        if (parts.size() >= 2) GSC_TRY(read_part(parts.size() - 2));
+        GSC_CU(ctx, cudaEventRecord(ev, solve));
+        // The part's copies follow its solve with no host wait: the
+        // iteration counts are not known yet, so every counter row a result
+        // can take is staged.
+        std::vector<uint32_t> rows(n);
+        for (uint32_t i = 0; i < n; ++i)
+            rows[i] = std::min<uint32_t>(results[f + i].iter_capacity, b->probs[i]->stats_cap - 1);
+        GSC_CU(ctx, cudaStreamWaitEvent(rs.copy, ev, 0));
+        GSC_TRY(read_enqueue(b, results + f, rs.copy, rows));
     }
-    GSC_TRY(read_part(parts.size() - 1));
+    // While the last copies run, each part's graph goes as soon as its solve
+    // has finished (destroying a graph costs the host about as much as
+    // building it).
+    for (uint32_t k = 0; k < nparts; ++k) {
+        GSC_CU(ctx, cudaEventSynchronize(rs.solved[k]));
+        release_batch_graph(parts[k].get());
+    }
     GSC_CU(ctx, cudaStreamSynchronize(rs.copy));
-    for (size_t k = 0; k < parts.size(); ++k) read_finish(parts[k].get(), results + first[k], rows[k]);
+    for (uint32_t k = 0; k < nparts; ++k) read_finish(parts[k].get(), results + k * part);
     return GSC_OK;
 }
 
@@ -790,10 +880,20 @@ int gsc_batch_read_all(gsc_batch* b, gsc_result* out) {
     gsc_context* ctx = b->ctx;
     cudaGetLastError();
     GSC_CU(ctx, cudaSetDevice(ctx->device));
-    std::vector<uint32_t> rows;
-    GSC_TRY(read_begin(b, out, ctx->stream, ctx->stream, rows));
-    GSC_CU(ctx, cudaStreamSynchronize(ctx->stream));
-    read_finish(b, out, rows);
+    cudaStream_t st = ctx->stream;
+    // One host wait for the solve: the control records are then final and
+    // give each reachable set's buffer and counter rows.
+    GSC_CU(ctx, cudaStreamSynchronize(st));
+    std::vector<uint32_t> rows(b->probs.size());
+    for (size_t i = 0; i < b->probs.size(); ++i) {
+        gsc_problem* p = b->probs[i].get();
+        if (out[i].reachable_mask)
+            GSC_CU(ctx, launch_unpack_bits(p->g, (b->hfc[i].iter & 1) ? p->reach1 : p->reach0, p->reach8, st));
+        rows[i] = read_rows(b, out + i, i);
+    }
+    GSC_TRY(read_enqueue(b, out, st, rows));
+    GSC_CU(ctx, cudaStreamSynchronize(st));
+    read_finish(b, out);
     return GSC_OK;
 }
 

@@ -5,6 +5,7 @@
 
 #include <atomic>
 #include <cstdint>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -58,6 +59,11 @@ struct gsc_context {
     static constexpr int kSetupStreams = 8;
     cudaStream_t setup[kSetupStreams] = {};
     cudaEvent_t setup_ev[kSetupStreams + 1] = {};
+    // Pinned host blocks of finished batches, kept for the next ones
+    // (size -> block): freeing pinned memory costs far more host time than
+    // taking a cached block.  Freed by gsc_context_trim and at destruction.
+    std::mutex pin_mu;
+    std::multimap<size_t, void*> pin_free;
 };
 
 struct gsc_abstraction {
@@ -173,6 +179,14 @@ int device_alloc(gsc_context* ctx, DevicePool* pool, std::vector<std::pair<void*
                  uint64_t& bytes, void** p, uint64_t nbytes);
 void device_release_all(gsc_context* ctx, DevicePool* pool, std::vector<std::pair<void*, uint64_t>>& allocs,
                         uint64_t& bytes);
+
+// Pinned (page-locked, mapped) host memory through the context's cache: a
+// cached block of at least `bytes` and at most twice that (plus 64 KB) is
+// taken before a new one is allocated.  A block goes back with pinned_put
+// once no device work uses it any more.
+cudaError_t pinned_get(gsc_context* ctx, size_t bytes, void** p, size_t* got);
+void pinned_put(gsc_context* ctx, void* p, size_t bytes);
+void pinned_trim(gsc_context* ctx);
 
 template <typename T>
 int palloc(gsc_problem* p, T** out, uint64_t count) {

@@ -215,7 +215,8 @@ const char* gsc_last_error(const gsc_context* ctx);
 int gsc_context_set_memory_budget(gsc_context* ctx, uint64_t bytes);
 /* Device memory the context holds now (pool regions, in use or cached). */
 uint64_t gsc_context_memory_in_use(const gsc_context* ctx);
-/* Returns the pool regions no handle uses to the driver. */
+/* Returns the pool regions no handle uses to the driver, and the pinned host
+ * blocks that destroyed batches left in the context's cache for reuse. */
 int gsc_context_trim(gsc_context* ctx);
 
 /* The nominal successor tables of abstraction_kernel (kernels.cu:164-217,
