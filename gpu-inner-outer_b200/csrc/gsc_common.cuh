@@ -56,6 +56,16 @@ __host__ __device__ __forceinline__ uint32_t fdiv_magic(uint32_t d) {
 }
 __device__ __forceinline__ uint32_t fdiv(uint32_t x, uint32_t m) { return m ? __umulhi(x, m) : x; }
 
+// Programmatic dependent launch (PTX griddepcontrol, sm_90 and later): wait
+// until the kernel this one was launched after has completed and its writes
+// are visible.  Called first in a kernel, before any load or store of global
+// memory.  The launch of such a kernel is prepared while its predecessor
+// runs and its blocks start as the predecessor's blocks exit (no explicit
+// early trigger: releasing dependents at the start of a kernel measured
+// slower).  For a kernel launched without the programmatic-serialization
+// attribute the instruction has no effect.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // Per-query constants.
 struct QueryInfo {
     double dhw[4];

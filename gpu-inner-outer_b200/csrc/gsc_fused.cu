@@ -50,6 +50,7 @@ __global__ void k_fused_init(GridInfo g, FusedFixArgs a, const uint8_t* __restri
 // position (dilate_position).
 __global__ void k_dilate(GridInfo g, const bword* __restrict__ src, bword* __restrict__ dst, DilateArgs d,
                          const FixControl* fc, uint32_t* rowlost, uint32_t rl_words) {
+    pdl_wait();
     if (fc && fc->stop) return;
     const uint32_t c = fc ? fc->iter : 0;
     const uint32_t* lost = (rowlost && c > 0) ? rowlost + (c & 1) * rl_words : nullptr;
@@ -177,12 +178,14 @@ template <int W, bool NV>
 __global__ void __launch_bounds__(kFusedWarps * 32) k_sat_col(GridInfo g, FusedFixArgs a) {
     extern __shared__ __align__(16) bword smem[];
     __shared__ uint32_t s_meta[4];
+    pdl_wait();
     sat_col_task<W, true, NV ? 1 : 0>(g, a, blockIdx.x, smem, s_meta);
 }
 
 // Apply the iteration's hits, build next iteration's D', count, and let the
 // last block to finish apply the stop rules (reachability.hpp:133-144).
 __global__ void __launch_bounds__(256) k_fused_finalize(GridInfo g, FusedFixArgs a) {
+    pdl_wait();
     FixControl* fc = a.fc;
     if (fc->stop) {
         // Already stopped (e.g. max_iterations == 0): the graph loop must still end.
@@ -234,8 +237,7 @@ cudaError_t launch_sat_col_t(const GridInfo& g, const FusedFixArgs& a, size_t sm
         if (e != cudaSuccess) return e;
         if (dev >= 0 && dev < 64) configured[dev].store(true);
     }
-    k_sat_col<W, NV><<<g.slices * g.mw, a.sat_threads, sm, st>>>(g, a);
-    return cudaGetLastError();
+    return launch_pdl(k_sat_col<W, NV>, dim3(g.slices * g.mw), dim3(a.sat_threads), sm, st, g, a);
 }
 
 }  // namespace
@@ -269,8 +271,8 @@ cudaError_t launch_dilate(const GridInfo& g, const bword* src, bword* dst, const
     const uint64_t pos = g.rows * g.W;
     uint64_t b = (pos + 255) / 256;
     if (b > 8192) b = 8192;
-    k_dilate<<<static_cast<unsigned int>(b ? b : 1), 256, 0, st>>>(g, src, dst, d, fc, rowlost, rl_words);
-    return cudaGetLastError();
+    return launch_pdl(k_dilate, dim3(static_cast<unsigned int>(b ? b : 1)), dim3(256), 0, st, g, src, dst, d, fc,
+                      rowlost, rl_words);
 }
 
 cudaError_t launch_sat_offsets(const GridInfo& g, const uint32_t* zt, const uint32_t* wt, const uint8_t* kidx,
@@ -315,9 +317,8 @@ cudaError_t launch_fused_iteration(const GridInfo& g, const FusedFixArgs& a, cud
     const uint64_t words = g.rows * g.W;
     uint64_t fb = (words + 255) / 256;
     if (fb > 4096) fb = 4096;
-    k_fused_finalize<<<static_cast<unsigned int>(fb ? fb : 1), 256, 0, st>>>(g, a);
     if (launches) *launches += 3;
-    return cudaGetLastError();
+    return launch_pdl(k_fused_finalize, dim3(static_cast<unsigned int>(fb ? fb : 1)), dim3(256), 0, st, g, a);
 }
 
 }  // namespace gsc_b200

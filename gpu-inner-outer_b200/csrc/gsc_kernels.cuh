@@ -8,6 +8,24 @@
 
 namespace gsc_b200 {
 
+// Launch of `k` that may begin while the kernel queued before it on `st`
+// drains (programmatic stream serialization); `k` starts with pdl_wait().
+// Under stream capture the dependency becomes a programmatic graph edge.
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k, static_cast<KArgs>(args)...);
+}
+
 // ---- abstraction (resident nominal successors) ------------------------------------------
 // xn[((i2*n3 + i3)*M + j)*n0 + i0] = nominal x after K Euler substeps (model.hpp:26-46),
 // yn likewise over i1.  cosT/sinT[(i2*mw + jw)*K + k], vseq[(i3*ma + ja)*K + k].
