@@ -174,6 +174,15 @@ void pinned_put(gsc_context* ctx, void* p, size_t bytes) {
     if (!p) return;
     std::lock_guard<std::mutex> lk(ctx->pin_mu);
     ctx->pin_free.emplace(bytes, p);
+    size_t held = 0;
+    for (const auto& kv : ctx->pin_free) held += kv.first;
+    // Past the cap the largest cached blocks go back to the driver.
+    while (held > kPinnedCacheMax && !ctx->pin_free.empty()) {
+        auto it = std::prev(ctx->pin_free.end());
+        held -= it->first;
+        cudaFreeHost(it->second);
+        ctx->pin_free.erase(it);
+    }
 }
 
 void pinned_trim(gsc_context* ctx) {

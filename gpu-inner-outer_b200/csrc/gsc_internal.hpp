@@ -183,7 +183,9 @@ void device_release_all(gsc_context* ctx, DevicePool* pool, std::vector<std::pai
 // Pinned (page-locked, mapped) host memory through the context's cache: a
 // cached block of at least `bytes` and at most twice that (plus 64 KB) is
 // taken before a new one is allocated.  A block goes back with pinned_put
-// once no device work uses it any more.
+// once no device work uses it any more; the cache keeps at most
+// kPinnedCacheMax bytes.
+constexpr size_t kPinnedCacheMax = size_t(256) << 20;
 cudaError_t pinned_get(gsc_context* ctx, size_t bytes, void** p, size_t* got);
 void pinned_put(gsc_context* ctx, void* p, size_t bytes);
 void pinned_trim(gsc_context* ctx);
