@@ -416,7 +416,8 @@ def bench_batched(args):
         "config": {"workload": f"batched_{n}_random_instances_seed{args.seed}", "instances": n,
                    "states_total": sum(sizes), "max_iterations_run": rep["max_iterations_run"],
                    "shapes": {"sat_threads": rep["sat_threads"], "sat_blocks_per_sm": rep["sat_blocks_per_sm"],
-                              "chunk_words": rep["chunk_words"], "tuned": rep0["tuned"],
+                              "chunk_words": rep["chunk_words"], "sat_warp_tasks": rep["sat_warp_tasks"],
+                              "tuned": rep0["tuned"],
                               "tune_ms": rep0["tune_ms"]},
                    "l2": "flushed before every step (256 MiB write)"},
         "e2e": {"value": n / (e2e_ms * 1e-3), "unit": "instances/s", "h2d_bytes_per_step": h2d,

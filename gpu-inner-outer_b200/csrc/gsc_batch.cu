@@ -217,11 +217,16 @@ int enqueue_iterations(gsc_batch* b, uint32_t count, uint32_t* launches) {
     return GSC_OK;
 }
 
-// Time `reps` iterations from a fresh start under each candidate shape;
-// keep the fastest.  Candidates: one task per block (64 / 128 / 256
+// Time the solve from a fresh start (up to kTuneIterations iterations,
+// checked every kTuneChunk: the first iterations test every pair, the later
+// ones only the pairs near states that left D', and the best shape differs
+// between the two) under each candidate shape; keep the fastest.  Candidates: one task per block (64 / 128 / 256
 // threads) and one task per warp (4 or 8 warps a block), each with one
 // block per task or a persistent grid, and chunks of 256 or 1,024 words; a
 // warp shape whose staging does not fit a block's shared memory is left out.
+// A single trial of a few iterations varies by a few percent between runs,
+// so the three fastest shapes are timed twice more and each keeps its best
+// time.
 int autotune(gsc_batch* b) {
     gsc_context* ctx = b->ctx;
     const int sms = sm_count(ctx);
@@ -231,48 +236,72 @@ int autotune(gsc_batch* b) {
     const Trial trials[] = {{64, 0}, {128, 0}, {256, 0}, {128, 1}, {256, 1}};
     const uint32_t per_sm[] = {0, 4, 8, 16};
     const uint32_t chunks[] = {256, 1024};
-    const uint32_t reps = 4;
+    constexpr uint32_t kTuneChunk = 8, kTuneIterations = 32;
     cudaEvent_t e0, e1;
     GSC_CU(ctx, cudaEventCreate(&e0));
     GSC_CU(ctx, cudaEventCreate(&e1));
-    float best = 1e30f;
-    BatchShape best_shape = b->shape;
+    uint32_t listed = 0;   // chunk of the uploaded work lists
+    auto time_shape = [&](const BatchShape& cand, float* ms) -> int {
+        if (cand.chunk != listed) {
+            GSC_TRY(upload_list(b, cand.chunk));
+            listed = cand.chunk;
+        }
+        b->shape = cand;
+        cudaError_t e = launch_batch_init(b->ddesc, b->wl, b->tot, sms, ctx->stream);
+        if (e == cudaSuccess) e = cudaEventRecord(e0, ctx->stream);
+        for (uint32_t done = 0; e == cudaSuccess && done < kTuneIterations; done += kTuneChunk) {
+            for (uint32_t r = 0; e == cudaSuccess && r < kTuneChunk; ++r)
+                e = launch_batch_iteration(b->ddesc, b->wl, b->tot, b->shape, b->wmax, b->smem, sms, 0, 0,
+                                           ctx->stream, nullptr);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(b->hrunning, b->drunning, 4, cudaMemcpyDeviceToHost, ctx->stream);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+            if (e == cudaSuccess && *b->hrunning == 0) break;
+        }
+        if (e == cudaSuccess) e = cudaEventRecord(e1, ctx->stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+        if (e == cudaSuccess) e = cudaEventElapsedTime(ms, e0, e1);
+        if (e != cudaSuccess) return fail(ctx, GSC_ERR_CUDA, std::string("autotune: ") + cudaGetErrorString(e));
+        return GSC_OK;
+    };
+    std::vector<std::pair<float, BatchShape>> timed;
     int status = GSC_OK;
     for (uint32_t ch : chunks) {
-        status = upload_list(b, ch);
-        if (status != GSC_OK) break;
         for (const Trial& tr : trials) {
             for (uint32_t ps : per_sm) {
                 const BatchShape cand{tr.threads, ps * static_cast<uint32_t>(sms), ch, tr.warp};
                 if (batch_sat_smem(cand, b->smem) > kFusedSmemMax) continue;
-                b->shape = cand;
-                cudaError_t e = launch_batch_init(b->ddesc, b->wl, b->tot, sms, ctx->stream);
-                if (e == cudaSuccess) e = cudaEventRecord(e0, ctx->stream);
-                for (uint32_t r = 0; e == cudaSuccess && r < reps; ++r)
-                    e = launch_batch_iteration(b->ddesc, b->wl, b->tot, b->shape, b->wmax, b->smem, sms, 0, 0,
-                                               ctx->stream, nullptr);
-                if (e == cudaSuccess) e = cudaEventRecord(e1, ctx->stream);
-                if (e == cudaSuccess) e = cudaEventSynchronize(e1);
                 float ms = 0.f;
-                if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
-                if (e != cudaSuccess) {
-                    status = fail(ctx, GSC_ERR_CUDA, std::string("autotune: ") + cudaGetErrorString(e));
-                    break;
-                }
-                if (ms < best) {
-                    best = ms;
-                    best_shape = b->shape;
-                }
+                status = time_shape(cand, &ms);
+                if (status != GSC_OK) break;
+                timed.emplace_back(ms, cand);
             }
             if (status != GSC_OK) break;
         }
         if (status != GSC_OK) break;
     }
+    if (status == GSC_OK && timed.empty()) status = fail(ctx, GSC_ERR_UNSUPPORTED, "autotune: no shape fits");
+    if (status == GSC_OK) {
+        std::stable_sort(timed.begin(), timed.end(),
+                         [](const std::pair<float, BatchShape>& x, const std::pair<float, BatchShape>& y) {
+                             return x.first < y.first;
+                         });
+        timed.resize(std::min<size_t>(timed.size(), 3));
+        for (int round = 0; round < 2 && status == GSC_OK; ++round)
+            for (auto& t : timed) {
+                float ms = 0.f;
+                status = time_shape(t.second, &ms);
+                if (status != GSC_OK) break;
+                t.first = std::min(t.first, ms);
+            }
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (status != GSC_OK) return status;
-    b->shape = best_shape;
-    return upload_list(b, best_shape.chunk);
+    const auto best = std::min_element(timed.begin(), timed.end(),
+                                       [](const std::pair<float, BatchShape>& x,
+                                          const std::pair<float, BatchShape>& y) { return x.first < y.first; });
+    b->shape = best->second;
+    return upload_list(b, b->shape.chunk);
 }
 
 void release_batch_graph(gsc_batch* b) {
