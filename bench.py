@@ -64,6 +64,10 @@ def parse():
                     help="served: one satisfaction task per warp in the serving loop's batched steps")
     ap.add_argument("--serve-iterations-per-step", type=int, default=0,
                     help="served: fixpoint iterations between the serving loop's host checks (0: the library's)")
+    ap.add_argument("--serve-sat-threads", type=int, default=0, choices=[0, 64, 128, 256],
+                    help="served: satisfaction block size of the serving loop's batched steps (0: the library's)")
+    ap.add_argument("--serve-sat-blocks-per-sm", type=int, default=0,
+                    help="served: persistent satisfaction blocks per SM (0: the library's)")
     ap.add_argument("--host-loop", action="store_true",
                     help="batched: iterate from the host instead of one CUDA graph (for per-kernel profiling)")
     ap.add_argument("--trajectories", type=int, default=1 << 20)
@@ -513,7 +517,8 @@ def bench_served(args):
         return total, lat
 
     srv = G.Server(ctx, memory_budget=int(args.serve_budget_gb * (1 << 30)), max_slots=256,
-                   sat_warp_tasks=bool(args.sat_warp_tasks), iterations_per_step=args.serve_iterations_per_step)
+                   sat_warp_tasks=bool(args.sat_warp_tasks), iterations_per_step=args.serve_iterations_per_step,
+                   sat_threads=args.serve_sat_threads, sat_blocks_per_sm=args.serve_sat_blocks_per_sm)
     # warm-up: a few queries of each model
     warm = [srv.submit(absn[k], C.random_query(models[k], args.seed + 1, i)) for i, k in enumerate(names * 4)]
     for t in warm:
