@@ -165,8 +165,8 @@ def run_reference_arm(args, case):
         "impl": "reference", "metric": metric, "value": v, "unit": "pair-checks/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": it_ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-        "config": {"workload": case["name"], "states": vals[0]["raw"]["grid_states"],
-                   "inputs": vals[0]["raw"]["inputs"], "sample": sample},
+        "config": {"workload": case["name"], "states": int(vals[0]["raw"]["grid_states"]),
+                   "inputs": int(vals[0]["raw"]["inputs"]), "sample": sample},
         "cpu_baseline": {"value": v, "unit": "pair-checks/s", "cores": threads, "kind": "reference",
                          "sample": sample},
         "e2e": {"value": v, "unit": "pair-checks/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
