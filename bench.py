@@ -14,8 +14,11 @@ Under torchrun (N > 1) every rank solves its own replica of the workload
 the max over ranks, and value = the pair-checks of all ranks / that time.
 
 `--impl reference` times the reference's own CPU method (oracle/_ref/gsc_ref,
-compiled from its sources) on the host cores, on a seeded sample of states of
-the same workload.
+compiled from its sources) on the host cores: every step is one full-grid
+fixpoint iteration of the same workload, states split over the host threads.
+The default run also times the reference's own CUDA backend (oracle/_ref/
+gsc_ref_gpu, built for sm_100a) on the published demo next to this library's
+solve of the same case (`reference_gpu`).
 """
 from __future__ import annotations
 
@@ -50,8 +53,9 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(C.PRESETS) + ["batched", "served", "simulate"], default="demo_scale")
     ap.add_argument("--method", choices=["auto", "stored", "fused"], default="auto")
-    ap.add_argument("--cpu-sample-states", type=int, default=160000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip the reference's CUDA backend on the published demo beside this library's")
     ap.add_argument("--e2e-steps", type=int, default=5)
     # batched / served workloads
     ap.add_argument("--instances", type=int, default=64)
@@ -77,37 +81,7 @@ def parse():
     return ap.parse_args()
 
 
-# ---- CPU: the reference's own method on a sample of states ------------------------------
-
-def reference_sample(case, n_states, seed, threads):
-    """One run of `gsc_ref sample`: the reference's abstraction rows and
-    iteration-1 state bodies for n_states seeded states, split over threads.
-    Returns the nominal pair-checks/s of a full fixpoint iteration, computed as
-    states x inputs / (prefix build + per-state loop scaled to all states)."""
-    sys.path.insert(0, ORACLE)
-    import oracle as O
-
-    with tempfile.TemporaryDirectory() as d:
-        path = os.path.join(d, "case.bin")
-        with open(path, "wb") as f:
-            f.write(bytes(O.to_struct(case)))
-        out = subprocess.run([REF_BIN, "sample", path, str(n_states), str(seed), str(threads)], check=True,
-                             capture_output=True, text=True).stdout
-    line = [ln for ln in out.splitlines() if ln.startswith("SAMPLE")][0]
-    kv = dict(t.split("=") for t in line.split()[1:])
-    S, M = int(kv["grid_states"]), int(kv["inputs"])
-    n = int(kv["states"])
-    iter_ms = float(kv["prefix_ms"]) + float(kv["iteration_ms"]) * S / n
-    full_ms = iter_ms + float(kv["abstraction_ms"]) * S / n
-    return {
-        "pair_checks_per_s": S * M / (iter_ms * 1e-3),
-        "iteration_ms_full_grid": iter_ms,
-        "abstraction_plus_iteration_ms_full_grid": full_ms,
-        "sample_states": n,
-        "threads": threads,
-        "raw": kv,
-    }
-
+# ---- CPU and GPU: the reference's own code --------------------------------------------------
 
 def reference_gpu_runs(case, runs):
     """The reference's own CUDA backend (cuda/kernels.cu, rebuilt for sm_100a
@@ -141,7 +115,44 @@ def cpu_threads():
         return os.cpu_count() or 1
 
 
+def reference_bench(case, threads, warmup, steps, single):
+    """One run of `gsc_ref bench`: the reference's CPU method on the whole
+    grid.  Set-up (untimed) builds the full abstraction with the reference's
+    per-pair steps, its states split over `threads`; then warmup + steps
+    full-grid fixpoint iterations from the start state are timed one by one
+    (the reachable prefix build plus every state's body,
+    reachability.hpp:53-109, states split over `threads`).  With `single` it
+    also times one iteration of solve_backward_cpu itself, single-threaded as
+    shipped.  Returns the parsed SETUP, STEP and SINGLE records."""
+    sys.path.insert(0, ORACLE)
+    import oracle as O
+
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "case.bin")
+        with open(path, "wb") as f:
+            f.write(bytes(O.to_struct(case)))
+        out = subprocess.run([REF_BIN, "bench", path, str(threads), str(warmup), str(steps), "1" if single else "0"],
+                             check=True, capture_output=True, text=True).stdout
+    recs = {"steps": []}
+    for ln in out.splitlines():
+        tag, *rest = ln.split()
+        kv = dict(t.split("=") for t in rest)
+        if tag == "SETUP":
+            recs["setup"] = kv
+        elif tag == "STEP" and kv["warm"] == "0":
+            recs["steps"].append({k: float(v) for k, v in kv.items()})
+        elif tag == "SINGLE":
+            recs["single"] = kv
+    return recs
+
+
 def run_reference_arm(args, case):
+    """The reference's own CPU method on the host cores, on the same workload:
+    every step is one full-grid fixpoint iteration (all states x all inputs),
+    timed as it runs, so ms_per_step is the time each step really took and
+    value = states x inputs / that time (the nominal accounting of the GPU
+    arm).  A single-threaded iteration of the reference's solver as shipped
+    is reported beside it."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
@@ -150,25 +161,29 @@ def run_reference_arm(args, case):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/gsc_ref was not built"}))
         return
     threads = cpu_threads()
-    vals = []
-    for i in range(args.warmup + args.steps):
-        r = reference_sample(case, args.cpu_sample_states, 1000 + i, threads)
-        if i >= args.warmup:
-            vals.append(r)
-    v = statistics.median(x["pair_checks_per_s"] for x in vals)
-    it_ms = statistics.median(x["iteration_ms_full_grid"] for x in vals)
-    S, M = C.grid_shape(case)
-    sample = (f"{args.cpu_sample_states} seeded states per step of the {case['name']} grid: the reference's "
-              f"abstraction rows and iteration-1 bodies (abstraction.hpp:168-208, reachability.hpp:59-109) on "
-              f"{threads} threads, plus one full-grid build_prefix_sum_cpu; scaled to all states")
+    r = reference_bench(case, threads, args.warmup, args.steps, single=True)
+    S, M = int(r["setup"]["states"]), int(r["setup"]["inputs"])
+    step_ms = [x["step_ms"] for x in r["steps"]]
+    ms = statistics.mean(step_ms)
+    v = S * M / (ms * 1e-3)
+    single_ms = float(r["single"]["solve_ms"])
+    sample = (f"every step = one full fixpoint iteration of the {case['name']} grid ({S} states x {M} inputs) "
+              f"from the start state: build_prefix_sum_cpu plus every state's body (reachability.hpp:53-109), "
+              f"states split over {threads} threads; the abstraction is built once before the steps (untimed)")
     line = {
         "impl": "reference", "metric": metric, "value": v, "unit": "pair-checks/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": it_ms, "higher_is_better": True,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-        "config": {"workload": case["name"], "states": int(vals[0]["raw"]["grid_states"]),
-                   "inputs": int(vals[0]["raw"]["inputs"]), "sample": sample},
+        "config": {"workload": case["name"], "states": S, "inputs": M, "pairs": S * M,
+                   "step": "one full-grid fixpoint iteration", "threads": threads,
+                   "abstraction_setup_ms": float(r["setup"]["abstraction_ms"]),
+                   "step_ms": {"median": statistics.median(step_ms), "min": min(step_ms), "max": max(step_ms)}},
         "cpu_baseline": {"value": v, "unit": "pair-checks/s", "cores": threads, "kind": "reference",
                          "sample": sample},
+        "single_thread_as_shipped": {
+            "value": S * M / (single_ms * 1e-3), "unit": "pair-checks/s", "cores": 1, "iteration_ms": single_ms,
+            "note": "one iteration of the reference's solve_backward_cpu (reachability.hpp:30-155) on the same "
+                    "prepared case, single-threaded as shipped"},
         "e2e": {"value": v, "unit": "pair-checks/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     # The reference's CUDA backend expresses the published demo (built-in
@@ -177,6 +192,57 @@ def run_reference_arm(args, case):
     if args.workload == "hyperbolic_demo" and os.path.exists(REF_GPU_BIN):
         line["reference_gpu"] = reference_gpu_runs(case, 3)
     print(json.dumps(line))
+
+
+def reference_gpu_beside_ours(G, torch, dev, stream, runs=3, steps=10):
+    """The published demo (examples/hyperbolic_case.cfg, 70x70x63x13 x 100)
+    through the reference's own CUDA backend on this GPU, next to this
+    library's fixpoint (graph solve, device events, L2 flushed) and its
+    end-to-end gsc_run_case on the same case."""
+    if not os.path.exists(REF_GPU_BIN):
+        return {"unavailable": "oracle/_ref/gsc_ref_gpu was not built"}
+    case = C.checked(C.hyperbolic_demo_case())
+    ref = reference_gpu_runs(case, runs)
+    if "unavailable" in ref:
+        return ref
+    ctx = G.Context(dev.index, stream.cuda_stream)
+    absn = G.Abstraction(ctx, case)
+    prob = G.Problem(ctx, absn, case, G.METHOD_AUTO)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    for _ in range(3):
+        prob.solve(graph=True)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for a, b in evs:
+        flush.fill_(3)
+        a.record(stream)
+        prob.solve(graph=True)
+        b.record(stream)
+    torch.cuda.synchronize(dev)
+    ours_ms = statistics.median(a.elapsed_time(b) for a, b in evs)
+    got = prob.read(masks=False)
+    prob.close()
+    absn.close()
+    ctx.close()
+    e2e = []
+    for k in range(runs + 1):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        G.run_case(case, graph=True, device=dev.index)
+        if k:
+            e2e.append((time.perf_counter() - t0) * 1e3)
+    ours_e2e = statistics.median(e2e)
+    same = (got["iterations"] == ref["iterations"] and got["reachable_states"] == ref["reachable_states"] and
+            got["certified_candidates"] == ref["certified_candidates"])
+    return {"workload": case["name"], "reference": ref,
+            "ours": {"fixpoint_ms": ours_ms, "e2e_ms": ours_e2e, "iterations": got["iterations"],
+                     "reachable_states": got["reachable_states"],
+                     "certified_candidates": got["certified_candidates"]},
+            "same_counts": same,
+            "fixpoint_speedup": ref["solve_ms"] / ours_ms, "e2e_speedup": ref["total_ms"] / ours_e2e,
+            "published_rtx4090_fixpoint_ms": PUBLISHED_DEMO_SOLVE_MS,
+            "note": "reference: cuda/kernels.cu built for sm_100a, run_case_cuda_u32 (solve_ms = its fixpoint "
+                    "loop, total_ms = the whole call with its abstraction and result copies); ours: the graph "
+                    "solve with device events and gsc_run_case end to end (host description in, host arrays out)"}
 
 
 # ---- GPU --------------------------------------------------------------------------------
@@ -769,11 +835,16 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(REF_BIN):
         threads = cpu_threads()
-        rs = reference_sample(case, args.cpu_sample_states, 7, threads)
-        cpu = {"value": rs["pair_checks_per_s"], "unit": "pair-checks/s", "cores": threads, "kind": "reference",
-               "sample": f"{args.cpu_sample_states} seeded states of the same grid, the reference's "
-                         f"iteration-1 state bodies on {threads} threads plus one full-grid prefix build, "
-                         f"scaled to all states"}
+        rb = reference_bench(case, threads, 0, 1, single=False)
+        st = rb["steps"][0]
+        cpu = {"value": S * M / (st["step_ms"] * 1e-3), "unit": "pair-checks/s", "cores": threads,
+               "kind": "reference",
+               "sample": f"one full-grid fixpoint iteration of the same workload through the reference's own CPU "
+                         f"method (prefix build + every state's body, reachability.hpp:53-109), states split over "
+                         f"{threads} threads: {st['step_ms']:.0f} ms; the abstraction built once before it, untimed"}
+    refgpu = None
+    if rank == 0 and world == 1 and not args.no_reference_gpu:
+        refgpu = reference_gpu_beside_ours(G, torch, dev, stream)
 
     vs = None
     if args.workload == "hyperbolic_demo":
@@ -794,9 +865,15 @@ def main():
         "cpu_baseline": cpu,
         "e2e": {"value": replica_value(world, P * r["iterations"], e2e_step), "unit": "pair-checks/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_step},
+        "pair_tests": {"per_step": tp["pair_tests"], "per_s": tp["pair_tests"] / (ms_per_step * 1e-3),
+                       "note": "(state, input) tests the kernels actually performed per fixpoint; the rest of the "
+                               "nominal pair-checks were skipped exactly (states already decided, inputs after the "
+                               "first satisfied one, boxes with no cell that left the set)"},
         "gpu_launches": launches,
         "clocks": clocks.summary(),
     }
+    if refgpu is not None:
+        line["reference_gpu"] = refgpu
     if rank == 0:
         print(json.dumps(line))
     prob.close()

@@ -18,7 +18,14 @@
 // Set-up: the first call on a device looks up the array's device address with
 // cudaGetSymbolAddress (a host-side name is not a device address) and caches
 // it per device.  Make that first call before any stream capture, since the
-// lookup may load the module.
+// lookup may load the module.  The cached address belongs to the device's
+// primary context: after cudaDeviceReset on a device this entry point must not
+// be called on that device again in the same process.
+//
+// Errors: when a launch or copy fails part-way, the call waits for the work it
+// already queued on the caller's stream (ignoring that wait's own result)
+// before it returns, so nothing it started still touches the shared array or
+// the caller's outputs when it returns.
 #include <algorithm>
 #include <cstring>
 #include <mutex>
@@ -47,7 +54,8 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
 struct NoAllocCtl {
     FixControl fc;
-    unsigned long long counts[4];   // [0] valid states, [1] candidate states
+    unsigned long long counts[4];   // [0] valid states, [1] candidate states,
+                                    // [2] candidate states that are not valid
 };
 static_assert(sizeof(NoAllocCtl) <= kCtlBytes, "control block must fit its slot");
 
@@ -76,24 +84,28 @@ __global__ void k_noalloc_init(GridInfo g, const uint8_t* __restrict__ valid, co
                                uint8_t* __restrict__ reach, uint32_t* __restrict__ controller,
                                uint32_t* __restrict__ reach_step, NoAllocCtl* ctl, unsigned long long* stats,
                                uint32_t stats_words) {
-    unsigned long long nv = 0, nc = 0;
+    unsigned long long nv = 0, nc = 0, nbad = 0;
     for (uint64_t s = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; s < g.S;
          s += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
         const uint8_t c = cand[s] ? 1 : 0;
+        const bool v = valid[s] != 0;
         reach[s] = c;
         controller[s] = kInvalid32;
         reach_step[s] = c ? 0u : kInvalid32;
-        nv += valid[s] != 0;
+        nv += v;
         nc += c;
+        nbad += (c && !v);
     }
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < stats_words; i += gridDim.x * blockDim.x) stats[i] = 0;
     for (int off = 16; off > 0; off >>= 1) {
         nv += __shfl_down_sync(0xFFFFFFFFu, nv, off);
         nc += __shfl_down_sync(0xFFFFFFFFu, nc, off);
+        nbad += __shfl_down_sync(0xFFFFFFFFu, nbad, off);
     }
     if ((threadIdx.x & 31) == 0) {
         if (nv) atomicAdd(&ctl->counts[0], nv);
         if (nc) atomicAdd(&ctl->counts[1], nc);
+        if (nbad) atomicAdd(&ctl->counts[2], nbad);
     }
 }
 
@@ -107,8 +119,11 @@ __global__ void k_noalloc_start(NoAllocCtl* ctl, uint32_t max_iterations, uint32
     fc->certified = 0;
     fc->reachable = ctl->counts[1];
     fc->converged = 0;
-    fc->stop = (max_iterations == 0) ? 1u : 0u;
-    fc->message = (max_iterations == 0) ? 3u : 0u;
+    // A candidate set with invalid states is refused before any iteration
+    // (abstraction.hpp:268-272); the host turns it into an error status.
+    const bool refused = ctl->counts[2] != 0;
+    fc->stop = (max_iterations == 0 || refused) ? 1u : 0u;
+    fc->message = refused ? 0u : (max_iterations == 0) ? 3u : 0u;
 }
 
 __device__ __forceinline__ uint32_t nq16(const int32_t* __restrict__ P, const GridInfo& g, uint32_t l0, uint32_t l1,
@@ -283,9 +298,14 @@ extern "C" int gsc_fixpoint_noalloc(const uint32_t shape[4], uint32_t inputs, in
     const uint32_t stats_words = kStatsCols * stats_cap;
     cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
 
+    // On failure, wait for what this call already queued (its own result is
+    // ignored) so that no earlier launch still writes the shared array or the
+    // caller's outputs once the call has returned.
 #define NA_CU(expr)                                  \
     do {                                             \
         if ((expr) != cudaSuccess) {                 \
+            cudaGetLastError();                      \
+            cudaStreamSynchronize(st);               \
             cudaGetLastError();                      \
             return GSC_ERR_CUDA;                     \
         }                                            \
@@ -304,7 +324,8 @@ extern "C" int gsc_fixpoint_noalloc(const uint32_t shape[4], uint32_t inputs, in
     NA_CU(launch_prefix4(g, 0, valid_mask, nullptr, pvalid, nullptr, st));
     NA_CU(cudaMemcpyAsync(reachable_next, reachable_mask, S, cudaMemcpyDeviceToDevice, st));
 
-    FixControl h;
+    NoAllocCtl hc;
+    FixControl& h = hc.fc;
     for (;;) {
         for (int k = 0; k < 8; ++k) {
             NA_CU(launch_prefix4(g, 0, reachable_mask, nullptr, preach, &ctl->fc, st));
@@ -315,11 +336,12 @@ extern "C" int gsc_fixpoint_noalloc(const uint32_t shape[4], uint32_t inputs, in
             k_noalloc_control<<<1, 1, 0, st>>>(ctl, stats);
             NA_CU(cudaGetLastError());
         }
-        NA_CU(cudaMemcpyAsync(&h, &ctl->fc, sizeof(h), cudaMemcpyDeviceToHost, st));
+        NA_CU(cudaMemcpyAsync(&hc, ctl, sizeof(hc), cudaMemcpyDeviceToHost, st));
         NA_CU(cudaStreamSynchronize(st));
         if (h.stop) break;
     }
 #undef NA_CU
+    if (hc.counts[2] != 0) return GSC_ERR_CANDIDATE_INVALID;
     if (summary) {
         for (int d = 0; d < 4; ++d) summary->shape[d] = shape[d];
         summary->states = S;

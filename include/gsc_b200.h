@@ -270,12 +270,20 @@ int gsc_run_case(int device, const gsc_model_desc* model, const gsc_query_desc* 
  * message and set sizes.  The working tables live in one fixed device array
  * inside the library (about 40 MiB, held by every GPU that loads the library
  * until the process exits).  Grids whose padded table
- * (nx+1)(ny+1)(ntheta+1)(nv+1) has more than 4,718,592 entries, or that could
- * need more than 4,094 iterations, are refused with GSC_ERR_OUT_OF_MEMORY
- * before any device work.  All calls share that array, so calls that overlap
- * on the GPU race: serialise them.  The first call on a device looks the
- * array's address up (cudaGetSymbolAddress); make that first call before any
- * stream capture.  Returns after synchronising `cuda_stream`. */
+ * (nx+1)(ny+1)(ntheta+1)(nv+1) has more than 4,718,592 entries are refused
+ * with GSC_ERR_OUT_OF_MEMORY before any device work, and so is a
+ * `max_iterations` argument that, capped at states + 1, exceeds 4,094 (the
+ * limit applies to the argument, not to the iterations a solve ends up
+ * running).  A candidate set holding invalid states is refused with
+ * GSC_ERR_CANDIDATE_INVALID, as the reference refuses it
+ * (abstraction.hpp:268-272).  All calls share the array, so calls that
+ * overlap on the GPU race: serialise them.  The first call on a device looks
+ * the array's address up (cudaGetSymbolAddress) and keeps it for the life of
+ * the process; make that first call before any stream capture, and do not call
+ * this entry point on a device again after cudaDeviceReset of that device.
+ * When a launch or copy fails part-way the call first waits for the work it
+ * had queued on `cuda_stream`, then returns GSC_ERR_CUDA.  Returns after
+ * synchronising `cuda_stream`. */
 int gsc_fixpoint_noalloc(const uint32_t shape[4], uint32_t inputs, int32_t wrap_dim, const uint32_t* min_flat,
                          const uint32_t* max_flat, const uint8_t* pair_valid, const uint8_t* valid_mask,
                          const uint8_t* candidate_mask, uint32_t max_iterations, uint8_t* reachable_mask,

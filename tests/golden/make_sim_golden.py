@@ -111,7 +111,9 @@ def run(sim, x0s, steps, seed, K, dhw):
 
 
 def main():
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    # default: the reference checkout beside this repository
+    here = os.path.dirname(os.path.abspath(__file__))
+    root = sys.argv[1] if len(sys.argv) > 1 else os.path.normpath(os.path.join(here, "..", "..", "..", "reference"))
     pp = load_reference(root)
     with open(os.path.join(HERE, "index.json")) as f:
         index = json.load(f)
