@@ -191,7 +191,8 @@ void pinned_trim(gsc_context* ctx) {
     ctx->pin_free.clear();
 }
 
-int abstraction_enqueue(gsc_abstraction* a, cudaStream_t st, std::vector<std::pair<void*, uint64_t>>& tmp) {
+int abstraction_enqueue(gsc_abstraction* a, cudaStream_t st, std::vector<std::pair<void*, uint64_t>>& tmp,
+                        cudaEvent_t* h2d_ev) {
     gsc_context* ctx = a->ctx;
     const GridInfo& g = a->g;
     const uint32_t K = g.K;
@@ -245,14 +246,45 @@ int abstraction_enqueue(gsc_abstraction* a, cudaStream_t st, std::vector<std::pa
     double* d_tab = static_cast<double*>(q);
     // One upload of the trajectory tables; cudaMemcpyAsync from pageable
     // memory has returned once the source may be reused.
+    if (h2d_ev) GSC_CU(ctx, cudaEventRecord(h2d_ev[0], st));
     GSC_CU(ctx, cudaMemcpyAsync(d_tab, cosT, (2 * ncs + nvs) * 8, cudaMemcpyHostToDevice, st));
     GSC_CU(ctx, cudaMemcpyAsync(a->thf, thf, nth * 8, cudaMemcpyHostToDevice, st));
     GSC_CU(ctx, cudaMemcpyAsync(a->vf, vf, nvf * 8, cudaMemcpyHostToDevice, st));
+    if (h2d_ev) GSC_CU(ctx, cudaEventRecord(h2d_ev[1], st));
     GSC_CU(ctx, launch_nominal_xy(g, d_tab, d_tab + ncs, d_tab + 2 * ncs, a->xn, a->yn, st));
     return GSC_OK;
 }
 
 int sm_count(gsc_context* ctx) { return ctx->sm_count > 0 ? ctx->sm_count : 148; }
+
+// The stored method takes every grid whose bounds fit 16 bits and whose
+// padded prefix table is indexed in 32 bits (the reference's own StateIndex
+// is 32-bit, grid.hpp:135).
+bool stored_fits(const GridInfo& g) {
+    return g.n[0] <= 65535 && g.n[1] <= 65535 && g.n[2] <= 65535 && g.n[3] <= 65535 && g.tsize < 0xFFFFFFFFull;
+}
+
+// The context's profiling events, created at first use.
+cudaError_t profile_events(gsc_context* ctx, cudaEvent_t** out) {
+    for (auto& e : ctx->pev)
+        if (!e) {
+            const cudaError_t err = cudaEventCreate(&e);
+            if (err != cudaSuccess) return err;
+        }
+    *out = ctx->pev;
+    return cudaSuccess;
+}
+
+// Device memory in use on the current GPU (all processes), as the reference
+// samples it (kernels.cu:30-42).
+uint64_t device_used_bytes() {
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return static_cast<uint64_t>(tot - fr);
+}
 
 }  // namespace gsc_api
 
@@ -433,6 +465,8 @@ void gsc_context_destroy(gsc_context* ctx) {
     cudaSetDevice(ctx->device);
     if (ctx->ev[0]) cudaEventDestroy(ctx->ev[0]);
     if (ctx->ev[1]) cudaEventDestroy(ctx->ev[1]);
+    for (auto e : ctx->pev)
+        if (e) cudaEventDestroy(e);
     for (auto s : ctx->setup)
         if (s) {
             cudaStreamSynchronize(s);
@@ -480,8 +514,10 @@ int gsc_abstraction_create(gsc_context* ctx, const gsc_model_desc* model, gsc_ab
     if (s != GSC_OK) return fail(ctx, s, err);
     std::vector<std::pair<void*, uint64_t>> tmp;
     uint64_t tmp_bytes = 0;
+    cudaEvent_t* pev = nullptr;
+    GSC_CU(ctx, profile_events(ctx, &pev));
     GSC_CU(ctx, cudaEventRecord(ctx->ev[0], ctx->stream));
-    int st = abstraction_enqueue(a.get(), ctx->stream, tmp);
+    int st = abstraction_enqueue(a.get(), ctx->stream, tmp, pev);
     cudaError_t e = cudaSuccess;
     if (st == GSC_OK) e = cudaEventRecord(ctx->ev[1], ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
@@ -494,6 +530,8 @@ int gsc_abstraction_create(gsc_context* ctx, const gsc_model_desc* model, gsc_ab
         return fail(ctx, e == cudaErrorMemoryAllocation ? GSC_ERR_OUT_OF_MEMORY : GSC_ERR_CUDA,
                     std::string("abstraction: ") + cudaGetErrorString(e));
     a->build_ms = ms;
+    if (cudaEventElapsedTime(&ms, pev[0], pev[1]) == cudaSuccess) a->h2d_ms = ms;
+    cudaGetLastError();
     *out = a.release();
     return GSC_OK;
 }
@@ -539,10 +577,11 @@ int problem_stage1(gsc_problem* p, const gsc_query_desc* qd) {
     q.max_iterations = qd->max_iterations;
 
     // Method pre-check by shape.
-    const bool stored_ok = g.n[0] <= 255 && g.n[1] <= 255 && g.n[2] <= 255 && g.n[3] <= 255;
+    const bool stored_ok = stored_fits(g);
     const bool fused_shape = g.n[0] <= kBits * kMaxWords && g.ma <= 255 && g.n[2] <= 65535 && g.n[3] <= 65535;
     if (method == GSC_METHOD_STORED && !stored_ok)
-        return fail(ctx, GSC_ERR_UNSUPPORTED, "stored method needs at most 255 cells per dimension");
+        return fail(ctx, GSC_ERR_UNSUPPORTED,
+                    "stored method needs at most 65535 cells per dimension and a prefix table under 2^32 entries");
     if (method == GSC_METHOD_FUSED && !fused_shape)
         return fail(ctx, GSC_ERR_UNSUPPORTED, "fused method needs at most 256 cells along x");
     if (method > GSC_METHOD_FUSED) return fail(ctx, GSC_ERR_INVALID_ARGUMENT, "unknown method");
@@ -555,6 +594,7 @@ int problem_stage1(gsc_problem* p, const gsc_query_desc* qd) {
     GSC_TRY(palloc(p, &p->flags, 1));
     GSC_CU(ctx, cudaMemsetAsync(p->counts, 0, 8 * sizeof(unsigned long long), st));
     GSC_CU(ctx, cudaMemsetAsync(p->flags, 0, sizeof(unsigned int), st));
+    if (p->time_h2d) GSC_CU(ctx, cudaEventRecord(ctx->pev[0], st));
     if (qd->obstacle_count) {
         GSC_TRY(palloc(p, &p->obstacles, 8ull * qd->obstacle_count));
         GSC_CU(ctx, cudaMemcpyAsync(p->obstacles, qd->obstacles, 64ull * qd->obstacle_count, cudaMemcpyHostToDevice, st));
@@ -566,7 +606,9 @@ int problem_stage1(gsc_problem* p, const gsc_query_desc* qd) {
         const uint64_t n = (p->safe_rank == 4) ? g.S : static_cast<uint64_t>(g.n[0]) * g.n[1];
         GSC_TRY(palloc(p, &p->safe, n));
         GSC_CU(ctx, cudaMemcpyAsync(p->safe, qd->safe_mask, n, cudaMemcpyHostToDevice, st));
-    } else if (q.ckind != GSC_CONSTRAINT_NONE) {
+    }
+    if (p->time_h2d) GSC_CU(ctx, cudaEventRecord(ctx->pev[1], st));
+    if (!qd->safe_mask && q.ckind != GSC_CONSTRAINT_NONE) {
         p->safe_rank = 2;
         GSC_TRY(palloc(p, &p->safe, static_cast<uint64_t>(g.n[0]) * g.n[1]));
         GSC_CU(ctx, launch_safe2(g, q, p->safe, st));
@@ -624,7 +666,7 @@ int problem_plan(gsc_problem* p) {
     p->candidate_count = pl.counts[1];
     // need the valid-cell test when some cell's validity is not its safety
     p->need_valid = p->safe ? (pl.counts[4] != 0) : (p->valid_count != g.S);
-    const bool stored_ok = g.n[0] <= 255 && g.n[1] <= 255 && g.n[2] <= 255 && g.n[3] <= 255;
+    const bool stored_ok = stored_fits(g);
     // An empty or over-wide interval, or too many box widths: only the
     // stored count is exact.
     bool fused_ok = p->fused_candidate && pl.fused && pl.flags == 0 && !pl.width_overflow;
@@ -675,7 +717,11 @@ int problem_stage2(gsc_problem* p) {
             GSC_CU(ctx, launch_prefix4(g, 2, p->safe, nullptr, p->unsafe4, nullptr, st));
         }
         p->S_pad = (g.S + 1) & ~1ull;
-        GSC_TRY(palloc(p, &p->boxes, p->S_pad * g.M));
+        p->wide = g.n[0] > 255 || g.n[1] > 255 || g.n[2] > 255 || g.n[3] > 255;
+        if (p->wide)
+            GSC_TRY(palloc(p, &p->boxes16, g.S * g.M));
+        else
+            GSC_TRY(palloc(p, &p->boxes, p->S_pad * g.M));
         StoredBuildArgs sb{};
         sb.xt = p->xt;
         sb.yt = p->yt;
@@ -688,6 +734,8 @@ int problem_stage2(gsc_problem* p) {
         sb.pvalid = p->pvalid;
         sb.boxes = p->boxes;
         sb.S_pad = p->S_pad;
+        sb.boxes16 = p->boxes16;
+        sb.wide = p->wide ? 1 : 0;
         sb.valid_pairs = p->counts + 3;
         GSC_CU(ctx, launch_stored_build(g, sb, st));
         GSC_TRY(palloc(p, &p->pd, g.tsize));
@@ -709,6 +757,8 @@ int problem_stage2(gsc_problem* p) {
     GSC_TRY(palloc(p, &p->dzw, combos * words));
     p->rl_words = static_cast<uint32_t>(g.rows / 32 + 2);
     GSC_TRY(palloc(p, &p->rowlost, 2ull * p->rl_words));
+    GSC_TRY(palloc(p, &p->slice_ticket, g.slices));
+    GSC_CU(ctx, cudaMemsetAsync(p->slice_ticket, 0, static_cast<size_t>(g.slices) * sizeof(uint32_t), st));
     GSC_TRY(palloc(p, &p->offz, static_cast<uint64_t>(g.n[2]) * g.mw));
     GSC_TRY(palloc(p, &p->offv, static_cast<uint64_t>(g.n[3]) * g.ma));
     GSC_CU(ctx, launch_sat_offsets(g, p->zt, p->wt, p->kidx, p->lidx, p->dil.nl, p->offz, p->offv, st));
@@ -739,6 +789,8 @@ StoredFixArgs stored_args(const gsc_problem* p, cudaGraphConditionalHandle cond,
     StoredFixArgs a{};
     a.boxes = p->boxes;
     a.S_pad = p->S_pad;
+    a.boxes16 = p->boxes16;
+    a.wide = p->wide ? 1 : 0;
     a.pd = p->pd;
     a.valid = p->valid;
     a.cand = p->cand;
@@ -784,6 +836,7 @@ FusedFixArgs fused_args(const gsc_problem* p, cudaGraphConditionalHandle cond, i
     a.sat_threads = fused_sat_threads(p->g, p->max_reps);
     a.dzw = p->dzw;
     a.rowlost = p->rowlost;
+    a.slice_ticket = p->slice_ticket;
     a.rl_words = p->rl_words;
     a.vzw = p->vzw;
     a.kidx = p->kidx;
@@ -874,6 +927,9 @@ int gsc_problem_create(gsc_context* ctx, const gsc_abstraction* abs, const gsc_q
     p->method = method;
     p->pool = ctx->pool.get();
     p->sync_release = true;
+    cudaEvent_t* pev = nullptr;
+    GSC_CU(ctx, profile_events(ctx, &pev));
+    p->time_h2d = true;
     GSC_CU(ctx, cudaEventRecord(ctx->ev[0], ctx->stream));
     GSC_TRY(problem_stage1(p.get(), query));
     GSC_CU(ctx, cudaStreamSynchronize(ctx->stream));
@@ -888,6 +944,9 @@ int gsc_problem_create(gsc_context* ctx, const gsc_abstraction* abs, const gsc_q
     GSC_CU(ctx, cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));
     p->timings.prepare_ms = ms;
     p->timings.abstraction_ms = abs->build_ms;
+    if (cudaEventElapsedTime(&ms, pev[0], pev[1]) == cudaSuccess) p->h2d_ms = ms;
+    cudaGetLastError();
+    p->peak_used = device_used_bytes();
     p->timings.device_bytes = p->bytes;
     p->timings.method = p->method;
     if (p->method == GSC_METHOD_FUSED) {
@@ -914,33 +973,44 @@ int gsc_problem_solve(gsc_problem* p, uint32_t flags) {
     uint32_t launches = 0;
     double sat_ms = 0.0, scan_ms = 0.0;
     uint32_t sat_launches = 0;
-    const uint32_t per_iter = (p->method == GSC_METHOD_STORED) ? 6 : 3;
+    const uint32_t per_iter = (p->method == GSC_METHOD_STORED) ? prefix4_launches(p->g) + 2 : 2;
     if (flags & GSC_SOLVE_PROFILE) {
         GSC_CU(ctx, enqueue_init(p));
         launches += 2;
-        cudaEvent_t ev[3];
-        for (auto& e : ev) GSC_CU(ctx, cudaEventCreate(&e));
+        cudaEvent_t* ev = nullptr;
+        GSC_CU(ctx, profile_events(ctx, &ev));
+        for (double& v : p->pass_ms) v = 0.0;
+        p->prof_sat_ms = p->prof_reduce_ms = p->prof_memcpy_ms = 0.0;
+        p->iter_prof.clear();
         FixControl hfc;
         cudaError_t err = cudaSuccess;
         uint32_t guard = 0;
         while (err == cudaSuccess) {
             // The stop rules fire by iteration stats_cap - 1 at the latest.
-            if (++guard > p->stats_cap + 2) {
-                for (auto& e : ev) cudaEventDestroy(e);
+            if (++guard > p->stats_cap + 2)
                 return fail(ctx, GSC_ERR_TIMEOUT, "fixpoint did not stop within its iteration bound");
-            }
             err = enqueue_iteration(p, 0, 0, &launches, ev);
             if (err == cudaSuccess) err = cudaMemcpyAsync(&hfc, p->fc, sizeof(hfc), cudaMemcpyDeviceToHost, st);
+            if (err == cudaSuccess) err = cudaEventRecord(ev[7], st);
             if (err == cudaSuccess) err = cudaStreamSynchronize(st);
-            float a = 0.f, b = 0.f;
-            if (err == cudaSuccess) err = cudaEventElapsedTime(&a, ev[0], ev[1]);
-            if (err == cudaSuccess) err = cudaEventElapsedTime(&b, ev[1], ev[2]);
-            scan_ms += a;
-            sat_ms += b;
+            float d[kProfileEvents - 1] = {};
+            for (int k = 0; err == cudaSuccess && k < kProfileEvents - 1; ++k)
+                err = cudaEventElapsedTime(&d[k], ev[k], ev[k + 1]);
+            if (err != cudaSuccess) break;
+            float prefix = 0.f;
+            for (int k = 0; k < 4; ++k) {
+                p->pass_ms[k] += d[k];
+                prefix += d[k];
+            }
+            scan_ms += prefix;
+            sat_ms += d[4];
+            p->prof_sat_ms += d[4];
+            p->prof_reduce_ms += d[5];
+            p->prof_memcpy_ms += d[6];
+            p->iter_prof.push_back({prefix + d[4] + d[5] + d[6], prefix, d[4], d[5] + d[6]});
             ++sat_launches;
             if (hfc.stop) break;
         }
-        for (auto& e : ev) cudaEventDestroy(e);
         GSC_CU(ctx, err);
     } else if (flags & GSC_SOLVE_GRAPH) {
         if (!p->exec) GSC_TRY(build_graph(p));
@@ -986,6 +1056,7 @@ int gsc_problem_solve(gsc_problem* p, uint32_t flags) {
     if (flags & GSC_SOLVE_GRAPH && !(flags & GSC_SOLVE_PROFILE))
         launches = 2 + per_iter * std::max<uint32_t>(hfc.iter, 1);   // init child graph + loop bodies
     p->timings.kernel_launches = launches;
+    p->peak_used = std::max(p->peak_used, device_used_bytes());
     if (flags & GSC_SOLVE_PROFILE) {
         p->timings.sat_kernel_ms = sat_ms;
         p->timings.scan_kernel_ms = scan_ms;
@@ -1103,6 +1174,74 @@ int gsc_problem_export_abstraction(gsc_problem* p, uint32_t* min_flat, uint32_t*
 int gsc_problem_timings(const gsc_problem* p, gsc_timings* out) {
     if (!p || !out) return GSC_ERR_INVALID_ARGUMENT;
     *out = p->timings;
+    return GSC_OK;
+}
+
+namespace {
+
+uint64_t alloc_bytes(const gsc_problem* p, const void* ptr) {
+    if (!ptr) return 0;
+    for (const auto& a : p->allocs)
+        if (a.first == ptr) return a.second;
+    return 0;
+}
+
+}  // namespace
+
+int gsc_problem_phase_timings(const gsc_problem* p, gsc_phase_timings* out) {
+    if (!p || !out) return GSC_ERR_INVALID_ARGUMENT;
+    std::memset(out, 0, sizeof(*out));
+    const gsc_timings& t = p->timings;
+    out->abstraction_kernel_ms = t.abstraction_ms + t.prepare_ms;
+    out->abstraction_memcpy_h2d_ms = p->abs->h2d_ms + p->h2d_ms;
+    out->scatter_mask_ms = 0.0;
+    for (int k = 0; k < 4; ++k) out->scan_axis_ms[k] = p->pass_ms[k];
+    out->prefix_build_total_ms = p->pass_ms[0] + p->pass_ms[1] + p->pass_ms[2] + p->pass_ms[3];
+    out->pair_satisfaction_ms = p->prof_sat_ms;
+    out->reduce_inputs_ms = p->prof_reduce_ms;
+    out->iteration_memcpy_ms = p->prof_memcpy_ms;
+    out->result_memcpy_d2h_ms = t.readback_ms;
+    out->total_kernel_ms =
+        out->abstraction_kernel_ms + out->prefix_build_total_ms + out->pair_satisfaction_ms + out->reduce_inputs_ms;
+    out->total_memcpy_ms = out->abstraction_memcpy_h2d_ms + out->iteration_memcpy_ms + out->result_memcpy_d2h_ms;
+    out->total_compute_ms = out->total_kernel_ms + out->total_memcpy_ms;
+    // Memory by role, from the problem's own allocations.
+    uint64_t boxes = 0;
+    for (const void* q : {static_cast<const void*>(p->xt), static_cast<const void*>(p->yt),
+                          static_cast<const void*>(p->zt), static_cast<const void*>(p->wt),
+                          static_cast<const void*>(p->boxes), static_cast<const void*>(p->boxes16),
+                          static_cast<const void*>(p->xcls),
+                          static_cast<const void*>(p->xrep), static_cast<const void*>(p->offz),
+                          static_cast<const void*>(p->offv), static_cast<const void*>(p->kidx),
+                          static_cast<const void*>(p->lidx), static_cast<const void*>(p->unsafe2),
+                          static_cast<const void*>(p->unsafe4), static_cast<const void*>(p->safe),
+                          static_cast<const void*>(p->obstacles)})
+        boxes += alloc_bytes(p, q);
+    uint64_t prefix = 0;
+    for (const void* q : {static_cast<const void*>(p->pd), static_cast<const void*>(p->pvalid),
+                          static_cast<const void*>(p->dzw), static_cast<const void*>(p->vzw),
+                          static_cast<const void*>(p->dp), static_cast<const void*>(p->rowlost)})
+        prefix += alloc_bytes(p, q);
+    out->abstraction_bytes = p->abs->bytes + boxes;
+    out->prefix_bytes = prefix;
+    out->iteration_bytes = p->bytes - boxes - prefix;
+    out->total_allocated_bytes = p->abs->bytes + p->bytes;
+    out->peak_usage_bytes = p->peak_used;
+    out->result_bytes = 11 * p->g.S + 16ull * t.iterations;
+    out->profiled_iterations = static_cast<uint32_t>(p->iter_prof.size());
+    return GSC_OK;
+}
+
+int gsc_problem_iteration_timings(const gsc_problem* p, uint32_t capacity, double* iteration_ms,
+                                  double* prefix_build_ms, double* satisfaction_ms, double* reduction_ms) {
+    if (!p) return GSC_ERR_INVALID_ARGUMENT;
+    const uint32_t n = std::min<uint32_t>(capacity, static_cast<uint32_t>(p->iter_prof.size()));
+    for (uint32_t i = 0; i < n; ++i) {
+        if (iteration_ms) iteration_ms[i] = p->iter_prof[i][0];
+        if (prefix_build_ms) prefix_build_ms[i] = p->iter_prof[i][1];
+        if (satisfaction_ms) satisfaction_ms[i] = p->iter_prof[i][2];
+        if (reduction_ms) reduction_ms[i] = p->iter_prof[i][3];
+    }
     return GSC_OK;
 }
 

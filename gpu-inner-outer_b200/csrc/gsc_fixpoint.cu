@@ -18,6 +18,8 @@
 // Every iteration's kernels first read the control block and return at once
 // when a stop rule has fired, so extra queued iterations are no-ops and the
 // loop can run as a CUDA graph whose while-condition the control kernel sets.
+#include <atomic>
+
 #include "gsc_kernels.cuh"
 
 namespace gsc_b200 {
@@ -99,6 +101,103 @@ __global__ void k_prefix_axis(GridInfo g, int dim, int32_t* __restrict__ T, cons
     }
 }
 
+// Two-pass build of the same table.  Pass 1 (x and y): one block per
+// (theta, v) slice.  Each warp scans rows of the slice's mask along x with
+// warp shuffles into shared memory; then one thread per x column scans along
+// y and writes the slice's table rows (coalesced along x).
+constexpr uint32_t kPrefixXYSmemMax = 96u << 10;
+constexpr uint32_t kPrefixZWSmemMax = 64u << 10;
+
+__global__ void __launch_bounds__(128) k_prefix_xy(GridInfo g, int mode, const uint8_t* __restrict__ a,
+                                                   const uint8_t* __restrict__ b, int32_t* __restrict__ T,
+                                                   const FixControl* fc) {
+    if (fc && fc->stop) return;
+    extern __shared__ int32_t sxy[];   // [n1][n0]
+    const uint32_t n0 = g.n[0], n1 = g.n[1];
+    const uint32_t slice = blockIdx.x;   // theta + n2 * v
+    const uint32_t z = slice % g.n[2], w = slice / g.n[2];
+    const uint64_t src = static_cast<uint64_t>(slice) * n0 * n1;
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    for (uint32_t y = warp; y < n1; y += nwarps) {
+        const uint64_t row = src + static_cast<uint64_t>(y) * n0;
+        int32_t carry = 0;
+        for (uint32_t x0 = 0; x0 < n0; x0 += 32) {
+            const uint32_t x = x0 + lane;
+            int32_t v = 0;
+            if (x < n0) {
+                const uint64_t s = row + x;
+                v = (mode == 0) ? (a[s] != 0) : (mode == 1) ? (a[s] != 0 && b[s] == 0) : (a[s] == 0);
+            }
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const int32_t t = __shfl_up_sync(0xFFFFFFFFu, v, off);
+                if (lane >= static_cast<uint32_t>(off)) v += t;
+            }
+            v += carry;
+            if (x < n0) sxy[y * n0 + x] = v;
+            carry = __shfl_sync(0xFFFFFFFFu, v, 31);
+        }
+    }
+    __syncthreads();
+    const uint64_t base = static_cast<uint64_t>(z + 1) * g.ps[2] + static_cast<uint64_t>(w + 1) * g.ps[3] + 1;
+    for (uint32_t x = threadIdx.x; x < n0; x += blockDim.x) {
+        int32_t acc = 0;
+        uint64_t o = base + g.ps[1] + x;
+        for (uint32_t y = 0; y < n1; ++y, o += g.ps[1]) {
+            acc += sxy[y * n0 + x];
+            T[o] = acc;
+        }
+    }
+}
+
+// Pass 2 (theta and v): one block per (tile of 2^lt x cells, y row).  The
+// tile's n3 x n2 x 2^lt values are loaded into shared memory (rows of the
+// tile are contiguous in the table), scanned along theta by one thread per
+// (v, x) line, then along v by one thread per (theta, x) line, which writes
+// the table back.
+__global__ void __launch_bounds__(256) k_prefix_zw(GridInfo g, uint32_t lt, int32_t* __restrict__ T,
+                                                   const FixControl* fc) {
+    if (fc && fc->stop) return;
+    extern __shared__ int32_t szw[];   // [n3][n2][tw]
+    const uint32_t tw = 1u << lt;
+    const uint32_t n0 = g.n[0], n2 = g.n[2], n3 = g.n[3];
+    const uint32_t tiles = (n0 + tw - 1) >> lt;
+    const uint32_t y = blockIdx.x / tiles;
+    const uint32_t x0 = (blockIdx.x - y * tiles) << lt;
+    const uint32_t nx = min(tw, n0 - x0);
+    const uint64_t base = static_cast<uint64_t>(y + 1) * g.ps[1] + x0 + 1;
+    const uint32_t lines = n2 * n3;
+    for (uint32_t i = threadIdx.x; i < (lines << lt); i += blockDim.x) {
+        const uint32_t tx = i & (tw - 1);
+        const uint32_t zw = i >> lt;
+        const uint32_t w = zw / n2, z = zw - w * n2;
+        szw[i] = (tx < nx) ? T[base + tx + static_cast<uint64_t>(z + 1) * g.ps[2] + static_cast<uint64_t>(w + 1) * g.ps[3]]
+                           : 0;
+    }
+    __syncthreads();
+    for (uint32_t l = threadIdx.x; l < (n3 << lt); l += blockDim.x) {
+        const uint32_t tx = l & (tw - 1), w = l >> lt;
+        int32_t* q = szw + ((w * n2) << lt) + tx;
+        int32_t acc = 0;
+        for (uint32_t z = 0; z < n2; ++z) {
+            acc += q[z << lt];
+            q[z << lt] = acc;
+        }
+    }
+    __syncthreads();
+    for (uint32_t l = threadIdx.x; l < (n2 << lt); l += blockDim.x) {
+        const uint32_t tx = l & (tw - 1), z = l >> lt;
+        if (tx >= nx) continue;
+        const int32_t* q = szw + (z << lt) + tx;
+        uint64_t o = base + tx + static_cast<uint64_t>(z + 1) * g.ps[2] + g.ps[3];
+        int32_t acc = 0;
+        for (uint32_t w = 0; w < n3; ++w, o += g.ps[3]) {
+            acc += q[(w * n2) << lt];
+            T[o] = acc;
+        }
+    }
+}
+
 // ---- stored method ---------------------------------------------------------------------
 
 __device__ __forceinline__ uint32_t q16(const int32_t* __restrict__ P, const GridInfo& g, uint32_t l0, uint32_t l1,
@@ -122,6 +221,14 @@ __device__ __forceinline__ uint32_t q16(const int32_t* __restrict__ P, const Gri
 __device__ __forceinline__ uint32_t dcount(const int32_t* __restrict__ P, const GridInfo& g, uint32_t lo, uint32_t hi) {
     const uint32_t l0 = lo & 255u, l1 = (lo >> 8) & 255u, l2 = (lo >> 16) & 255u, l3 = lo >> 24;
     const uint32_t r0 = (hi & 255u) + 1, r1 = ((hi >> 8) & 255u) + 1, h2 = (hi >> 16) & 255u, r3 = (hi >> 24) + 1;
+    if (l2 <= h2) return q16(P, g, l0, l1, l2, l3, r0, r1, h2 + 1, r3);
+    return q16(P, g, l0, l1, l2, l3, r0, r1, g.n[2], r3) + q16(P, g, l0, l1, 0, l3, r0, r1, h2 + 1, r3);
+}
+
+// D(box) for a wide box (16 bits per bound).
+__device__ __forceinline__ uint32_t dcount16(const int32_t* __restrict__ P, const GridInfo& g, uint4 b) {
+    const uint32_t l0 = lo16(b.x), l1 = hi16(b.x), l2 = lo16(b.y), l3 = hi16(b.y);
+    const uint32_t r0 = lo16(b.z) + 1, r1 = hi16(b.z) + 1, h2 = lo16(b.w), r3 = hi16(b.w) + 1;
     if (l2 <= h2) return q16(P, g, l0, l1, l2, l3, r0, r1, h2 + 1, r3);
     return q16(P, g, l0, l1, l2, l3, r0, r1, g.n[2], r3) + q16(P, g, l0, l1, 0, l3, r0, r1, h2 + 1, r3);
 }
@@ -219,6 +326,67 @@ __global__ void __launch_bounds__(256) k_sat_stored(GridInfo g, StoredFixArgs a)
     }
 }
 
+// The same test on a wide grid (a dimension of more than 255 cells): one
+// thread per state, one 16-byte load per input (boxes16[j * S + s]).
+__global__ void __launch_bounds__(256) k_sat_stored_wide(GridInfo g, StoredFixArgs a) {
+    const FixControl* fc = a.fc;
+    if (fc->stop) return;
+    const uint32_t it = fc->iter + 1;
+    const uint64_t s = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    unsigned long long nr = 0, nc = 0, nload = 0, ncount = 0;
+    if (s < g.S) {
+        const bool v = a.valid[s] != 0;
+        const bool isc = a.cand[s] != 0;
+        const bool rch = a.reach[s] != 0;
+        const bool cert = a.controller[s] != kInvalid32;
+        const bool act = v && !((!isc && rch) || (isc && cert));
+        bool found = false;
+        uint32_t chosen = 0;
+        if (act) {
+            const uint4* bx = reinterpret_cast<const uint4*>(a.boxes16) + s;
+            uint4 nb = ld_stream(bx);
+            for (uint32_t j = 0; j < g.M; ++j) {
+                const uint4 b = nb;
+                ++nload;
+                if (j + 1 < g.M) nb = ld_stream(bx + static_cast<uint64_t>(j + 1) * g.S);
+                if (b.x == kBoxSentinel) continue;
+                ++ncount;
+                if (dcount16(a.pd, g, b) == 0) {
+                    found = true;
+                    chosen = j;
+                    break;
+                }
+            }
+        }
+        if (found) {
+            if (!rch) {
+                a.reach[s] = 1;
+                ++nr;
+            }
+            if (!cert) {
+                a.controller[s] = chosen;
+                if (isc)
+                    ++nc;
+                else
+                    a.reach_step[s] = it;
+            }
+        }
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        nr += __shfl_down_sync(0xFFFFFFFFu, nr, off);
+        nc += __shfl_down_sync(0xFFFFFFFFu, nc, off);
+        nload += __shfl_down_sync(0xFFFFFFFFu, nload, off);
+        ncount += __shfl_down_sync(0xFFFFFFFFu, ncount, off);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        unsigned long long* row = a.stats + kStatsCols * it;
+        if (nr) atomicAdd(row, nr);
+        if (nc) atomicAdd(row + 1, nc);
+        if (nload) atomicAdd(row + 2, nload);
+        if (ncount) atomicAdd(row + 3, ncount);
+    }
+}
+
 // ---- control (device-side stop rules, reachability.hpp:133-144) -------------------------
 
 __global__ void k_fix_init(FixControl* fc, uint32_t max_iterations, uint32_t stats_cap,
@@ -272,13 +440,44 @@ __global__ void k_set_condition(const FixControl* fc, cudaGraphConditionalHandle
 }  // namespace
 
 cudaError_t launch_prefix4(const GridInfo& g, int mode, const uint8_t* a, const uint8_t* b, int32_t* table,
-                           const FixControl* ctl, cudaStream_t st) {
+                           const FixControl* ctl, cudaStream_t st, cudaEvent_t* ev) {
+    const uint64_t xy_bytes = static_cast<uint64_t>(g.n[0]) * g.n[1] * 4;
+    const uint64_t zw_line = static_cast<uint64_t>(g.n[2]) * g.n[3] * 4;
+    if (xy_bytes <= kPrefixXYSmemMax && zw_line <= kPrefixZWSmemMax) {
+        // Two passes: x and y per (theta, v) slice, then theta and v per
+        // (x tile, y) with the widest tile (up to 32 x cells) that fits.
+        static std::atomic<bool> configured[64];
+        int dev = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e != cudaSuccess) return e;
+        if (dev < 0 || dev >= 64 || !configured[dev].load()) {
+            e = cudaFuncSetAttribute(k_prefix_xy, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(kPrefixXYSmemMax));
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(k_prefix_zw, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(kPrefixZWSmemMax));
+            if (e != cudaSuccess) return e;
+            if (dev >= 0 && dev < 64) configured[dev].store(true);
+        }
+        uint32_t lt = 5;
+        while (lt > 0 && (zw_line << lt) > kPrefixZWSmemMax) --lt;
+        k_prefix_xy<<<g.slices, 128, static_cast<size_t>(xy_bytes), st>>>(g, mode, a, b, table, ctl);
+        if (ev) cudaEventRecord(ev[0], st);
+        const uint32_t tiles = (g.n[0] + (1u << lt) - 1) >> lt;
+        k_prefix_zw<<<tiles * g.n[1], 256, static_cast<size_t>(zw_line << lt), st>>>(g, lt, table, ctl);
+        if (ev)
+            for (int k = 1; k < 4; ++k) cudaEventRecord(ev[k], st);
+        return cudaGetLastError();
+    }
+    // Wide slices or theta-v planes: one pass per dimension.
     k_prefix_x<<<blocks_for(g.rows * 32, 256), 256, 0, st>>>(g, mode, a, b, table, ctl);
+    if (ev) cudaEventRecord(ev[0], st);
     for (int dim = 1; dim <= 3; ++dim) {
         const int d1 = (dim == 1) ? 2 : 1;
         const int d2 = (dim == 3) ? 2 : 3;
         const uint64_t lines = static_cast<uint64_t>(g.n[0]) * g.n[d1] * g.n[d2];
         k_prefix_axis<<<blocks_for(lines, 256), 256, 0, st>>>(g, dim, table, ctl);
+        if (ev) cudaEventRecord(ev[dim], st);
     }
     return cudaGetLastError();
 }
@@ -291,14 +490,23 @@ cudaError_t launch_stored_init(const GridInfo& g, const StoredFixArgs& a, cudaSt
 cudaError_t launch_stored_iteration(const GridInfo& g, const StoredFixArgs& a, cudaStream_t st, uint32_t* launches,
                                     cudaEvent_t* ev) {
     if (ev) cudaEventRecord(ev[0], st);
-    cudaError_t e = launch_prefix4(g, 1, a.valid, a.reach, a.pd, a.fc, st);
+    cudaError_t e = launch_prefix4(g, 1, a.valid, a.reach, a.pd, a.fc, st, ev ? ev + 1 : nullptr);
     if (e != cudaSuccess) return e;
-    if (ev) cudaEventRecord(ev[1], st);
-    k_sat_stored<<<blocks_for(a.S_pad / 2, 256), 256, 0, st>>>(g, a);
-    if (ev) cudaEventRecord(ev[2], st);
+    if (a.wide)
+        k_sat_stored_wide<<<blocks_for(g.S, 256), 256, 0, st>>>(g, a);
+    else
+        k_sat_stored<<<blocks_for(a.S_pad / 2, 256), 256, 0, st>>>(g, a);
+    if (ev) cudaEventRecord(ev[5], st);
     k_control<<<1, 1, 0, st>>>(a.fc, a.stats, a.cond, a.use_cond);
-    if (launches) *launches += 6;
+    if (ev) cudaEventRecord(ev[6], st);
+    if (launches) *launches += prefix4_launches(g) + 2;
     return cudaGetLastError();
+}
+
+uint32_t prefix4_launches(const GridInfo& g) {
+    const uint64_t xy_bytes = static_cast<uint64_t>(g.n[0]) * g.n[1] * 4;
+    const uint64_t zw_line = static_cast<uint64_t>(g.n[2]) * g.n[3] * 4;
+    return (xy_bytes <= kPrefixXYSmemMax && zw_line <= kPrefixZWSmemMax) ? 2u : 4u;
 }
 
 cudaError_t launch_fix_init(FixControl* fc, uint32_t max_iterations, uint32_t stats_cap,

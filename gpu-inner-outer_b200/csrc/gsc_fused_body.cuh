@@ -431,11 +431,15 @@ __device__ __forceinline__ void sat_col_task(const GridInfo& g, const FusedFixAr
 
 // Apply the iteration's hits to word e and build next iteration's D';
 // nr / nc collect newly reachable states and newly certified candidates.
+// L2: read hit and best[] from L2 (inside the satisfaction kernel, where
+// other blocks of the same launch wrote them with atomics and this SM's L1
+// may hold an older copy of their lines).
+template <bool L2 = false>
 __device__ __forceinline__ void finalize_word(const GridInfo& g, const FusedFixArgs& a, const bword* rprev,
                                               bword* rnext, uint64_t e, uint32_t it, unsigned long long& nr,
                                               unsigned long long& nc) {
     const bword rp = rprev[e];
-    const bword h = a.hit[e];
+    const bword h = L2 ? __ldcg(a.hit + e) : a.hit[e];
     const bword rn = rp | h;
     rnext[e] = rn;
     const bword dn = (a.validb[e] & ~rn) | a.unsafeb[e];
@@ -462,7 +466,8 @@ __device__ __forceinline__ void finalize_word(const GridInfo& g, const FusedFixA
                 m &= m - 1;
             }
 #pragma unroll
-            for (int k = 0; k < 4; ++k) j[k] = b[k] < kBits ? a.best[sbase + b[k]] : kInvalid32;
+            for (int k = 0; k < 4; ++k)
+                j[k] = b[k] < kBits ? (L2 ? __ldcg(a.best + sbase + b[k]) : a.best[sbase + b[k]]) : kInvalid32;
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
                 if (b[k] >= kBits) continue;

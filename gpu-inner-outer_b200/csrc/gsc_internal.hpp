@@ -3,6 +3,7 @@
 // serving loop (gsc_server.cu).
 #pragma once
 
+#include <array>
 #include <atomic>
 #include <cstdint>
 #include <map>
@@ -52,6 +53,8 @@ struct gsc_context {
     std::atomic<uint64_t> in_use{0};
     std::mutex mem_mu;   // budget check + in_use update
     cudaEvent_t ev[2] = {nullptr, nullptr};
+    // Events of profiled solves and set-up uploads (created at first use).
+    cudaEvent_t pev[gsc_b200::kProfileEvents] = {};
     int sm_count = 0;
     std::unique_ptr<DevicePool> pool;   // caching pool of the context's problems and abstractions
     // Streams for the set-up of batch instances (created at the first batch,
@@ -78,6 +81,7 @@ struct gsc_abstraction {
     std::vector<std::pair<void*, uint64_t>> allocs;
     uint64_t bytes = 0;
     double build_ms = 0.0;
+    double h2d_ms = 0.0;         // uploads of the trajectory tables
     bool sync_release = false;   // wait for the context stream before the memory is reused
     ~gsc_abstraction();
 };
@@ -117,6 +121,8 @@ struct gsc_problem {
     // stored
     uint2* boxes = nullptr;
     uint64_t S_pad = 0;
+    uint4* boxes16 = nullptr;     // wide grids (a dimension of more than 255 cells)
+    bool wide = false;
     int32_t* pd = nullptr;
     uint8_t* reach8 = nullptr;
     // fused
@@ -128,6 +134,7 @@ struct gsc_problem {
     uint32_t max_reps = 0;
     gsc_b200::bword *dzw = nullptr, *vzw = nullptr;
     uint32_t* rowlost = nullptr;
+    uint32_t* slice_ticket = nullptr;
     uint32_t rl_words = 0;
     uint32_t* offz = nullptr;   // per omega column and theta cell: part of a dilated row's offset
     uint32_t* offv = nullptr;   // per acceleration and v cell: the other part
@@ -145,6 +152,18 @@ struct gsc_problem {
     cudaGraphExec_t exec = nullptr;
     cudaGraph_t graph = nullptr;
     gsc_timings timings{};
+    // Per-phase device times (gsc_problem_phase_timings).  h2d_ms: uploads of
+    // the query's host arrays at creation; the rest from the last
+    // GSC_SOLVE_PROFILE solve: prefix passes, satisfaction, reduction
+    // (control or finalize kernel) and stop-record reads, summed, and per
+    // iteration {iteration, prefix build, satisfaction, reduction incl. the
+    // stop-record read}.
+    bool time_h2d = false;
+    double h2d_ms = 0.0;
+    double pass_ms[4] = {0, 0, 0, 0};
+    double prof_sat_ms = 0.0, prof_reduce_ms = 0.0, prof_memcpy_ms = 0.0;
+    std::vector<std::array<float, 4>> iter_prof;
+    uint64_t peak_used = 0;      // device memory in use on the GPU, highest sample
     ~gsc_problem();
 };
 
@@ -202,7 +221,9 @@ int palloc(gsc_problem* p, T** out, uint64_t count) {
 // trajectories, uploads them and launches the nominal-successor kernel on
 // `st`.  The three temporary tables are returned in `tmp` (owned by the
 // caller until the stream has passed the kernel).
-int abstraction_enqueue(gsc_abstraction* a, cudaStream_t st, std::vector<std::pair<void*, uint64_t>>& tmp);
+// h2d_ev (optional, 2 events) is recorded around the uploads.
+int abstraction_enqueue(gsc_abstraction* a, cudaStream_t st, std::vector<std::pair<void*, uint64_t>>& tmp,
+                        cudaEvent_t* h2d_ev = nullptr);
 
 // Problem set-up in three steps:
 //   stage1  masks, per-axis boxes and (for the fused method) the x classes,
@@ -217,6 +238,7 @@ int problem_stage2(gsc_problem* p);
 
 gsc_b200::FusedFixArgs fused_args(const gsc_problem* p, cudaGraphConditionalHandle cond, int use_cond);
 int sm_count(gsc_context* ctx);
+bool stored_fits(const gsc_b200::GridInfo& g);
 
 // Batched execution of fused problems (gsc_batch.cu).
 gsc_b200::InstanceDesc make_instance(const gsc_problem* p);

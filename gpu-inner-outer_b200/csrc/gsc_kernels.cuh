@@ -71,8 +71,14 @@ cudaError_t launch_unpack_reach(const GridInfo& g, const FixControl* fc, const b
 
 // ---- 4-D inclusive prefix tables (int32, zero first plane per dimension) -----------------
 // mode 0: valid; 1: valid && !reach (b = reach); 2: !safe (4-D safe mask).
+// Built in two passes (x-y per (theta, v) slice, then theta-v per (x tile,
+// y)) when a slice and a theta-v plane fit shared memory, else one pass per
+// dimension.  ev (optional, 4 events): ev[k] is recorded after pass k + 1; a
+// two-pass build records ev[1..3] after its second pass.
 cudaError_t launch_prefix4(const GridInfo& g, int mode, const uint8_t* a, const uint8_t* b, int32_t* table,
-                           const FixControl* ctl, cudaStream_t st);
+                           const FixControl* ctl, cudaStream_t st, cudaEvent_t* ev = nullptr);
+// Kernels launch_prefix4 launches for this grid.
+uint32_t prefix4_launches(const GridInfo& g);
 // 2-D prefix of !safe2 over (x, y): (n0+1)*(n1+1) entries, stride n0+1.
 cudaError_t launch_prefix2_unsafe(const GridInfo& g, const uint8_t* safe2, int32_t* table, cudaStream_t st);
 
@@ -84,8 +90,10 @@ struct StoredBuildArgs {
     const int32_t* unsafe2;   // rank 2 prefix
     const int32_t* unsafe4;   // rank 4 prefix
     const int32_t* pvalid;    // 4-D valid prefix
-    uint2* boxes;             // [M][S_pad]
+    uint2* boxes;             // [M][S_pad]: one byte per bound (every dimension <= 255 cells)
     uint64_t S_pad;
+    uint4* boxes16;           // [M][S]: 16 bits per bound, when a dimension has more than 255 cells
+    int wide;                 // 1: boxes16 in use
     unsigned long long* valid_pairs;   // abstraction-valid pairs (before the V(box) > 0 fold)
 };
 cudaError_t launch_stored_build(const GridInfo& g, const StoredBuildArgs& a, cudaStream_t st);
@@ -108,6 +116,8 @@ cudaError_t launch_export(const GridInfo& g, const ExportArgs& a, cudaStream_t s
 struct StoredFixArgs {
     const uint2* boxes;
     uint64_t S_pad;
+    const uint4* boxes16;     // wide grids: {lo0 | lo1 << 16, lo2 | lo3 << 16, hi0 | hi1 << 16, hi2 | hi3 << 16}
+    int wide;
     int32_t* pd;              // D-prefix table
     const uint8_t* valid;
     const uint8_t* cand;
@@ -120,7 +130,10 @@ struct StoredFixArgs {
     int use_cond;
 };
 cudaError_t launch_stored_init(const GridInfo& g, const StoredFixArgs& a, cudaStream_t st);
-// ev (optional, 3 events): recorded before the scan, before and after the satisfaction kernel.
+// ev (optional, kProfileEvents events): [0] before the prefix rebuild,
+// [1..4] after its passes (launch_prefix4), [5] after the satisfaction kernel,
+// [6] after the control kernel.
+constexpr int kProfileEvents = 8;
 cudaError_t launch_stored_iteration(const GridInfo& g, const StoredFixArgs& a, cudaStream_t st, uint32_t* launches,
                                     cudaEvent_t* ev = nullptr);
 
@@ -181,6 +194,8 @@ struct FusedFixArgs {
     // v cell (sums modulo 2^32, as dzw offsets are 32-bit):
     const uint32_t* offz;      // [n2 * mw]: kslot * nl * rows * W + n1 * lz * W
     const uint32_t* offv;      // [n3 * ma]: lslot * rows * W + n1 * n2 * lw * W
+    uint32_t* slice_ticket;    // [slices]: satisfaction blocks of the slice done this iteration
+                               // (one-problem kernel; zero between iterations)
     cudaGraphConditionalHandle cond;
     int use_cond;
 };
@@ -297,6 +312,11 @@ cudaError_t launch_fused_init(const GridInfo& g, const FusedFixArgs& a, const ui
 // The offz / offv tables of a problem (after its plan: kidx, lidx, nl).
 cudaError_t launch_sat_offsets(const GridInfo& g, const uint32_t* zt, const uint32_t* wt, const uint8_t* kidx,
                                const uint8_t* lidx, uint32_t nl, uint32_t* offz, uint32_t* offv, cudaStream_t st);
+// One iteration is two launches: the dilation, then the satisfaction kernel,
+// whose last block of each (theta, v) slice finalizes the slice and whose
+// last finalizing block applies the stop rules.
+// ev (optional, kProfileEvents events): [0] before the dilation, [1..4] after
+// it, [5] and [6] after the satisfaction kernel.
 cudaError_t launch_fused_iteration(const GridInfo& g, const FusedFixArgs& a, cudaStream_t st, uint32_t* launches,
                                    cudaEvent_t* ev = nullptr);
 

@@ -405,27 +405,38 @@ __device__ __forceinline__ PairBox pair_box(const GridInfo& g, const uint32_t* _
     return b;
 }
 
-// Stored layout: boxes[j * S_pad + s] = {pack8(lo), pack8(hi)}, or the
+// Stored layout: boxes[j * S_pad + s] = {pack8(lo), pack8(hi)} (or, on a
+// wide grid, boxes16[j * S + s] = the bounds as 16-bit halves), or the
 // sentinel when the pair can never satisfy: abstraction-invalid, or a box
 // with no valid cell (the iteration-invariant valid_count == 0 test of
-// reachability.hpp:78-84).
+// reachability.hpp:78-84).  A wide entry's first word is lo0 | lo1 << 16
+// with lo0 < 65535, so it never equals the sentinel.
 __global__ void k_stored_build(GridInfo g, StoredBuildArgs a) {
-    const uint64_t total = a.S_pad * g.M;
+    const uint64_t rowlen = a.wide ? g.S : a.S_pad;
+    const uint64_t total = rowlen * g.M;
     unsigned long long nvp = 0;
     for (uint64_t e = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; e < total;
          e += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        const uint32_t j = static_cast<uint32_t>(e / a.S_pad);
-        const uint64_t s = e - static_cast<uint64_t>(j) * a.S_pad;
-        uint2 out = make_uint2(kBoxSentinel, kBoxSentinel);
+        const uint32_t j = static_cast<uint32_t>(e / rowlen);
+        const uint64_t s = e - static_cast<uint64_t>(j) * rowlen;
+        bool keep = false;
+        PairBox b{};
         if (s < g.S) {
-            const PairBox b = pair_box(g, a.xt, a.yt, a.zt, a.wt, a.safe, a.safe_rank, s, j);
+            b = pair_box(g, a.xt, a.yt, a.zt, a.wt, a.safe, a.safe_rank, s, j);
             if (b.ok && box_safe(g, a.safe, a.safe_rank, a.unsafe2, a.unsafe4, b.lo, b.hi)) {
                 ++nvp;
-                if (count_box(a.pvalid, g, b.lo, b.hi) != 0)
-                    out = make_uint2(pack8(b.lo[0], b.lo[1], b.lo[2], b.lo[3]), pack8(b.hi[0], b.hi[1], b.hi[2], b.hi[3]));
+                keep = count_box(a.pvalid, g, b.lo, b.hi) != 0;
             }
         }
-        a.boxes[e] = out;
+        if (a.wide) {
+            a.boxes16[e] = keep ? make_uint4(pack16(b.lo[0], b.lo[1]), pack16(b.lo[2], b.lo[3]),
+                                             pack16(b.hi[0], b.hi[1]), pack16(b.hi[2], b.hi[3]))
+                                : make_uint4(kBoxSentinel, kBoxSentinel, kBoxSentinel, kBoxSentinel);
+        } else {
+            a.boxes[e] = keep ? make_uint2(pack8(b.lo[0], b.lo[1], b.lo[2], b.lo[3]),
+                                           pack8(b.hi[0], b.hi[1], b.hi[2], b.hi[3]))
+                              : make_uint2(kBoxSentinel, kBoxSentinel);
+        }
     }
     for (int off = 16; off > 0; off >>= 1) nvp += __shfl_down_sync(0xFFFFFFFFu, nvp, off);
     if ((threadIdx.x & 31) == 0 && nvp) atomicAdd(a.valid_pairs, nvp);
@@ -657,7 +668,7 @@ cudaError_t launch_prefix2_unsafe(const GridInfo& g, const uint8_t* safe2, int32
 }
 
 cudaError_t launch_stored_build(const GridInfo& g, const StoredBuildArgs& a, cudaStream_t st) {
-    k_stored_build<<<blocks_for(a.S_pad * g.M), kThreads, 0, st>>>(g, a);
+    k_stored_build<<<blocks_for((a.wide ? g.S : a.S_pad) * g.M), kThreads, 0, st>>>(g, a);
     return cudaGetLastError();
 }
 

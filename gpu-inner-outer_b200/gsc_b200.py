@@ -86,6 +86,18 @@ class Timings(ctypes.Structure):
     ]
 
 
+class PhaseTimings(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_double) for k in ("abstraction_kernel_ms", "abstraction_memcpy_h2d_ms",
+                                               "scatter_mask_ms")] + [
+        ("scan_axis_ms", ctypes.c_double * 4)] + [
+        (k, ctypes.c_double) for k in ("prefix_build_total_ms", "pair_satisfaction_ms", "reduce_inputs_ms",
+                                       "iteration_memcpy_ms", "result_memcpy_d2h_ms", "total_kernel_ms",
+                                       "total_memcpy_ms", "total_compute_ms")] + [
+        (k, ctypes.c_uint64) for k in ("total_allocated_bytes", "peak_usage_bytes", "abstraction_bytes",
+                                       "prefix_bytes", "iteration_bytes", "result_bytes")] + [
+        ("profiled_iterations", ctypes.c_uint32)]
+
+
 class BatchOptions(ctypes.Structure):
     _fields_ = [("autotune", ctypes.c_uint32), ("sat_threads", ctypes.c_uint32),
                 ("sat_blocks_per_sm", ctypes.c_uint32), ("chunk_words", ctypes.c_uint32),
@@ -137,6 +149,8 @@ SIGNATURES = {
     "gsc_problem_read": (ctypes.c_int, [_P, ctypes.POINTER(Result)]),
     "gsc_problem_export_abstraction": (ctypes.c_int, [_P, _P, _P, _P]),
     "gsc_problem_timings": (ctypes.c_int, [_P, ctypes.POINTER(Timings)]),
+    "gsc_problem_phase_timings": (ctypes.c_int, [_P, ctypes.POINTER(PhaseTimings)]),
+    "gsc_problem_iteration_timings": (ctypes.c_int, [_P, ctypes.c_uint32, _P, _P, _P, _P]),
     "gsc_run_case": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ModelDesc), ctypes.POINTER(QueryDesc),
                                     ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(Result),
                                     ctypes.POINTER(Timings)]),
@@ -341,6 +355,20 @@ class Problem:
     def read(self, iter_capacity=4096, masks=True, out=None) -> dict:
         return _read_result(lambda r: lib().gsc_problem_read(self._h, r), self.ctx, iter_capacity, masks, out,
                             self.states)
+
+    def phase_timings(self) -> dict:
+        """Per-phase times and memory in the reference's report terms
+        (gsc_problem_phase_timings), with the per-iteration times of the last
+        profiled solve under ``iterations``."""
+        t = PhaseTimings()
+        self.ctx.check(lib().gsc_problem_phase_timings(self._h, ctypes.byref(t)))
+        out = {k: (list(getattr(t, k)) if k == "scan_axis_ms" else getattr(t, k)) for k, _ in PhaseTimings._fields_}
+        n = t.profiled_iterations
+        cols = [np.zeros(n) for _ in range(4)]
+        self.ctx.check(lib().gsc_problem_iteration_timings(self._h, n, *[_ptr(c) for c in cols]))
+        out["iterations"] = {k: c for k, c in zip(("iteration_ms", "prefix_build_ms", "satisfaction_ms",
+                                                   "reduction_ms"), cols)}
+        return out
 
     def simulate(self, x0, steps, seed, trajectories=True) -> dict:
         """Closed-loop trajectories under the solved controller from each row

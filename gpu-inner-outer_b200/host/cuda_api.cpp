@@ -2,6 +2,7 @@
 // cuda/kernels.cu:492-875) implemented over libgsc_b200's C ABI.
 #include "gsc/cuda_api.hpp"
 
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <stdexcept>
@@ -115,6 +116,31 @@ void query_of(const CaseConfig& cfg, const std::uint32_t shape[4], QueryStorage*
     q.max_iterations = cfg.max_iterations;
 }
 
+// estimate_memory_budget (abstraction.hpp:211-243): the reference's byte
+// counts for its own device layout (u32 flats, u8 masks, u64 prefix tables).
+MemoryBudget reference_budget(const GridShape& sg, const GridShape& ig) {
+    const std::uint64_t S = sg.total_size, P = S * ig.total_size;
+    std::uint64_t T = 1;
+    for (int d = 0; d < kStateDim; ++d) T *= static_cast<std::uint64_t>(sg.shape[d]) + 1;
+    MemoryBudget b;
+    b.pair_min_bytes = P * 4;
+    b.pair_max_bytes = P * 4;
+    b.pair_valid_bytes = P;
+    b.pair_satisfied_bytes = P;
+    b.reachable_prev_bytes = S;
+    b.reachable_next_bytes = S;
+    b.valid_mask_bytes = S;
+    b.candidate_mask_bytes = S;
+    b.controller_bytes = S * 4;
+    b.reach_step_bytes = S * 4;
+    b.prefix_reachable_bytes = T * 8;
+    b.prefix_valid_bytes = T * 8;
+    b.total_bytes = b.pair_min_bytes + b.pair_max_bytes + b.pair_valid_bytes + b.pair_satisfied_bytes +
+                    b.reachable_prev_bytes + b.reachable_next_bytes + b.valid_mask_bytes + b.candidate_mask_bytes +
+                    b.controller_bytes + b.reach_step_bytes + b.prefix_reachable_bytes + b.prefix_valid_bytes;
+    return b;
+}
+
 }  // namespace
 
 bool cuda_backend_compiled() { return gsc_cuda_backend_compiled() != 0; }
@@ -164,7 +190,8 @@ GpuRunReport run_case_cuda_u32(const CaseConfig& cfg, const RunOptions& opt) {
     const auto t0 = std::chrono::steady_clock::now();
     st = gsc_abstraction_create(ctx, &m, &abs);
     if (st == GSC_OK) st = gsc_problem_create(ctx, abs, &qs.q, opt.method, &p);
-    if (st == GSC_OK) st = gsc_problem_solve(p, opt.graph ? GSC_SOLVE_GRAPH : 0);
+    const std::uint32_t solve_flags = opt.profile ? GSC_SOLVE_PROFILE : opt.graph ? GSC_SOLVE_GRAPH : 0;
+    if (st == GSC_OK) st = gsc_problem_solve(p, solve_flags);
     if (st == GSC_OK) {
         r.valid_mask.resize(S);
         r.candidate_mask.resize(S);
@@ -200,15 +227,42 @@ GpuRunReport run_case_cuda_u32(const CaseConfig& cfg, const RunOptions& opt) {
         r.reachable_states = out.reachable_states;
         r.certified_candidate_states = out.certified_candidates;
         r.solve_ms = report.solve_ms = t.solve_ms;
-        report.kernel_timings.abstraction_kernel_ms = t.abstraction_ms;
-        report.kernel_timings.prepare_ms = t.prepare_ms;
-        report.kernel_timings.solve_ms = t.solve_ms;
-        report.kernel_timings.result_memcpy_d2h_ms = t.readback_ms;
+        gsc_phase_timings ph{};
+        gsc_problem_phase_timings(p, &ph);
+        KernelTimings& k = report.kernel_timings;
+        k.abstraction_kernel_ms = ph.abstraction_kernel_ms;
+        k.abstraction_memcpy_h2d_ms = ph.abstraction_memcpy_h2d_ms;
+        k.scatter_mask_ms = ph.scatter_mask_ms;
+        k.scan_axis0_ms = ph.scan_axis_ms[0];
+        k.scan_axis1_ms = ph.scan_axis_ms[1];
+        k.scan_axis2_ms = ph.scan_axis_ms[2];
+        k.scan_axis3_ms = ph.scan_axis_ms[3];
+        k.prefix_build_total_ms = ph.prefix_build_total_ms;
+        k.pair_satisfaction_ms = ph.pair_satisfaction_ms;
+        k.reduce_inputs_ms = ph.reduce_inputs_ms;
+        k.iteration_memcpy_ms = ph.iteration_memcpy_ms;
+        k.result_memcpy_d2h_ms = ph.result_memcpy_d2h_ms;
+        k.total_kernel_ms = ph.total_kernel_ms;
+        k.total_memcpy_ms = ph.total_memcpy_ms;
+        k.total_compute_ms = ph.total_compute_ms;
+        k.prepare_ms = t.prepare_ms;
+        k.solve_ms = t.solve_ms;
+        GpuMemoryStats& ms = report.memory_stats;
+        ms.total_allocated_bytes = ph.total_allocated_bytes;
+        ms.peak_usage_bytes = ph.peak_usage_bytes;
+        ms.abstraction_bytes = ph.abstraction_bytes;
+        ms.prefix_bytes = ph.prefix_bytes;
+        ms.iteration_bytes = ph.iteration_bytes;
+        ms.result_bytes = ph.result_bytes;
+        report.budget = reference_budget(report.state_grid, report.input_grid);
         report.abstraction_ms = t.abstraction_ms + t.prepare_ms;
         report.total_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
-        report.memory_stats.total_allocated_bytes = t.device_bytes;
+        const std::uint32_t n = std::min<std::uint32_t>(out.iterations, out.iter_capacity);
+        std::vector<double> it_ms(n), pre_ms(n), sat_ms(n), red_ms(n);
+        gsc_problem_iteration_timings(p, n, it_ms.data(), pre_ms.data(), sat_ms.data(), red_ms.data());
+        const std::uint32_t timed = opt.profile ? std::min<std::uint32_t>(n, ph.profiled_iterations) : 0;
         std::uint64_t reach = out.candidate_count, cert = 0;
-        for (std::uint32_t i = 0; i < out.iterations && i < out.iter_capacity; ++i) {
+        for (std::uint32_t i = 0; i < n; ++i) {
             IterationStats s;
             s.iteration = i + 1;
             s.newly_reachable = nr[i];
@@ -217,6 +271,12 @@ GpuRunReport run_case_cuda_u32(const CaseConfig& cfg, const RunOptions& opt) {
             cert += nc[i];
             s.total_reachable = reach;
             s.total_certified = cert;
+            if (i < timed) {
+                s.iteration_ms = it_ms[i];
+                s.prefix_build_ms = pre_ms[i];
+                s.satisfaction_check_ms = sat_ms[i];
+                s.reduction_ms = red_ms[i];
+            }
             report.iteration_stats.push_back(s);
         }
     }

@@ -247,6 +247,51 @@ int gsc_problem_export_abstraction(gsc_problem* p, uint32_t* min_flat, uint32_t*
 
 int gsc_problem_timings(const gsc_problem* p, gsc_timings* out);
 
+/* Per-phase device times and memory of a problem in the terms of the
+ * reference's report: the fields of KernelTimings and GpuMemoryStats
+ * (include/gsc/cuda_api.hpp:24-58), which cuda/kernels.cu fills with CUDA
+ * events around each launch (kernels.cu:403-484, :605-640, :654-767,
+ * :785-851).  Set-up and readback times come from gsc_abstraction_create,
+ * gsc_problem_create and the last gsc_problem_read; the kernel breakdown
+ * from the last solve run with GSC_SOLVE_PROFILE (zero after any other
+ * solve).  The prefix build has no separate scatter: the set is read inside
+ * its first pass. */
+typedef struct {
+    double abstraction_kernel_ms;     /* abstraction tables + the problem's mask and box kernels      */
+    double abstraction_memcpy_h2d_ms; /* set-up uploads: trajectory tables, host masks, obstacles      */
+    double scatter_mask_ms;           /* 0: folded into the first prefix pass                          */
+    double scan_axis_ms[4];           /* stored: prefix passes in launch order (a two-pass build:
+                                         [0] x and y, [1] theta and v); fused: [0] = the (theta, v)
+                                         dilation of D'                                                */
+    double prefix_build_total_ms;     /* sum of scan_axis_ms                                           */
+    double pair_satisfaction_ms;      /* satisfaction kernels (exists-input reduction fused in)        */
+    double reduce_inputs_ms;          /* stored: control kernel; fused: finalize kernel                */
+    double iteration_memcpy_ms;       /* the host loop's reads of the stop record                      */
+    double result_memcpy_d2h_ms;      /* last gsc_problem_read                                         */
+    double total_kernel_ms;           /* abstraction + prefix + satisfaction + reduction (kernels.cu:841-845) */
+    double total_memcpy_ms;           /* h2d + iteration + result copies (kernels.cu:846-849)          */
+    double total_compute_ms;          /* kernel + memcpy (kernels.cu:850-851)                          */
+    uint64_t total_allocated_bytes;   /* device memory of the abstraction and the problem              */
+    uint64_t peak_usage_bytes;        /* device memory in use on the GPU (cudaMemGetInfo), highest
+                                         sample after creation and after each solve                    */
+    uint64_t abstraction_bytes;       /* abstraction tables + the problem's boxes, classes, safe tables */
+    uint64_t prefix_bytes;            /* stored: prefix tables; fused: D' and its dilated copies       */
+    uint64_t iteration_bytes;         /* masks, sets, controller, reach_step, counters, control        */
+    uint64_t result_bytes;            /* bytes a full gsc_problem_read copies to the host              */
+    uint32_t profiled_iterations;     /* iterations with per-iteration times                           */
+} gsc_phase_timings;
+
+int gsc_problem_phase_timings(const gsc_problem* p, gsc_phase_timings* out);
+
+/* Per-iteration device times of the last GSC_SOLVE_PROFILE solve, the time
+ * fields of IterationStats (cuda_api.hpp:11-21): entry i is iteration i + 1
+ * (capacity entries at most; gsc_phase_timings.profiled_iterations exist).
+ * iteration = prefix build + satisfaction + reduction; reduction includes the
+ * host loop's read of the stop record, as the reference's reduction_ms
+ * includes its counter copies (kernels.cu:687-721).  Any pointer may be NULL. */
+int gsc_problem_iteration_timings(const gsc_problem* p, uint32_t capacity, double* iteration_ms,
+                                  double* prefix_build_ms, double* satisfaction_ms, double* reduction_ms);
+
 /* Replaces gsc::run_case_cuda_u32 (cuda_api.hpp:88, kernels.cu:492-875):
  * abstraction, query, fixpoint and readback in one call on `device`. */
 int gsc_run_case(int device, const gsc_model_desc* model, const gsc_query_desc* query, uint32_t method,

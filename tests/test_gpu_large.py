@@ -4,9 +4,9 @@
     iteration k for 10^5 seeded states plus every state the GPU changed in
     iteration k (up to a cap), and must agree bit for bit with the GPU's
     solve capped at k iterations;
-  * the fused method's widest rows (256 x-cells, 8 words) and the first width
-    it refuses (257 x-cells: the automatic method falls back to the stored
-    one), both against the full oracle."""
+  * the fused method's widest rows (256 x-cells, 8 words) and grids wider
+    than that or than 255 cells in any dimension (the stored method with
+    16-bit box bounds), against the full oracle."""
 import numpy as np
 import pytest
 
@@ -73,14 +73,43 @@ def test_widest_fused_rows(ctx):
     absn.close()
 
 
-def test_no_method_beyond_both_limits(ctx):
-    """257 x-cells: wider than the fused rows and than the stored method's
-    one-byte box bounds (255 cells per dimension)."""
-    case = C.unicycle_grid_case((257, 16, 8, 6), (3, 3), "wide_257")
+def wide_demo_case(n):
+    """The published demo's geometry and dynamics on an n-cell grid, 5x5 inputs."""
+    c = dict(C.hyperbolic_demo_case())
+    c["name"] = "wide_demo_%dx%dx%dx%d" % tuple(n)
+    c["state_eta"] = [(c["state_ub"][d] - c["state_lb"][d]) / n[d] for d in range(4)]
+    c["input_eta"] = [0.4, 0.4]
+    c["expect_shape"] = list(n)
+    return C.checked(c)
+
+
+@pytest.mark.parametrize("shape,demo", [((257, 16, 8, 6), False), ((300, 12, 10, 6), False),
+                                        ((40, 300, 6, 4), False), ((300, 24, 20, 8), True)])
+def test_wide_grids_take_the_stored_method_with_16_bit_bounds(ctx, shape, demo):
+    """More than 256 x-cells is wider than the fused rows, and more than 255
+    cells in any dimension wider than one-byte box bounds: the automatic
+    choice is the stored method with 16-bit bounds, and the result is the
+    oracle's bit for bit (the reference takes any grid of 32-bit state
+    indices, grid.hpp:135).  The demo-geometry grid runs 52 iterations."""
+    if demo:
+        case = wide_demo_case(shape)
+    else:
+        case = C.unicycle_grid_case(shape, (3, 3), "wide_%dx%dx%dx%d" % shape, max_iterations=64)
+    want = O.solve(case)
     absn = G.Abstraction(ctx, case)
-    with pytest.raises(G.GscError) as e:
-        G.Problem(ctx, absn, case, G.METHOD_AUTO)
-    assert e.value.status == 4
+    for graph in (True, False):
+        p = G.Problem(ctx, absn, case, G.METHOD_AUTO)
+        p.solve(graph=graph)
+        got = p.read()
+        assert p.timings()["method"] == G.METHOD_STORED
+        p.close()
+        assert_same_result(got, want, "x".join(map(str, shape)))
+        assert got["iterations"] == want["iterations"] and got["message"] == want["message"]
+        assert list(got["iter_new_reachable"]) == list(want["iter_new_reachable"])
+    if shape[0] > 256:
+        with pytest.raises(G.GscError) as e:
+            G.Problem(ctx, absn, case, G.METHOD_FUSED)
+        assert e.value.status == 4
     absn.close()
 
 
