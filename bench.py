@@ -108,6 +108,24 @@ def reference_gpu_runs(case, runs):
                     "(solve_ms: its fixpoint loop; total_ms: with the abstraction and its copy to the host)"}
 
 
+def reference_full_runs(cases, budget_ms=20000.0):
+    """The reference's own CPU method as shipped (prepare_case_cpu +
+    solve_backward_cpu, single-threaded: oracle/_ref/gsc_ref full) on the
+    cases in order, until its own timers have counted budget_ms.  Returns the
+    number of cases run and their summed abstraction + solve milliseconds."""
+    sys.path.insert(0, ORACLE)
+    import oracle as O
+
+    n, total = 0, 0.0
+    for c in cases:
+        r = O.run_reference(c)
+        total += r["abstraction_ms"] + r["solve_ms"]
+        n += 1
+        if total >= budget_ms:
+            break
+    return n, total
+
+
 def cpu_threads():
     try:
         return len(os.sched_getaffinity(0))
@@ -223,11 +241,12 @@ def reference_gpu_beside_ours(G, torch, dev, stream, runs=3, steps=10):
     prob.close()
     absn.close()
     ctx.close()
+    outs = pinned_outputs(torch, int(got["states"]))
     e2e = []
     for k in range(runs + 1):
         torch.cuda.synchronize(dev)
         t0 = time.perf_counter()
-        G.run_case(case, graph=True, device=dev.index)
+        G.run_case(case, graph=True, device=dev.index, out=outs)
         if k:
             e2e.append((time.perf_counter() - t0) * 1e3)
     ours_e2e = statistics.median(e2e)
@@ -242,7 +261,8 @@ def reference_gpu_beside_ours(G, torch, dev, stream, runs=3, steps=10):
             "published_rtx4090_fixpoint_ms": PUBLISHED_DEMO_SOLVE_MS,
             "note": "reference: cuda/kernels.cu built for sm_100a, run_case_cuda_u32 (solve_ms = its fixpoint "
                     "loop, total_ms = the whole call with its abstraction and result copies); ours: the graph "
-                    "solve with device events and gsc_run_case end to end (host description in, host arrays out)"}
+                    "solve with device events and gsc_run_case end to end (host description in, results in pinned host "
+                    "arrays)"}
 
 
 # ---- GPU --------------------------------------------------------------------------------
@@ -478,6 +498,13 @@ def bench_batched(args):
     n = len(cases)
     h2d = 0
     d2h = sum(11 * S for S in sizes)
+    cpu = None
+    if not args.no_cpu_baseline and os.path.exists(REF_BIN):
+        k, ref_ms = reference_full_runs(cases)
+        cpu = {"value": k / (ref_ms * 1e-3), "unit": "instances/s", "cores": 1, "kind": "reference",
+               "sample": f"the first {k} of the {n} instances, each a full run of the reference's CPU method as "
+                         f"shipped (prepare_case_cpu + solve_backward_cpu, one thread): {ref_ms:.0f} ms by its own "
+                         f"timers"}
     line = {
         "metric": "batched instances/s", "value": n / (step_ms * 1e-3), "unit": "instances/s", "n_gpus": 1,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
@@ -501,6 +528,7 @@ def bench_batched(args):
             "p99_ms": percentile(plain_ms, 99),
             "note": "per instance: abstraction + problem set-up + graph solve + read into pinned memory"},
         "speedup_vs_plain": {"e2e": plain_total / e2e_ms, "fixpoint": sum(plain_dev) / step_ms},
+        "cpu_baseline": cpu,
         "gpu_launches": launches,
         "clocks": clocks.summary(),
     }
@@ -515,8 +543,8 @@ def bench_served(args):
     32x32x24x16 x 64 inputs).  First all queries at once (saturation), then
     three arrival rates as fractions of that throughput; latency = scheduled
     arrival to completion.  Beside it the same queries one at a time through
-    the plain API, and that sequential server's latencies at the same
-    arrival times (FIFO)."""
+    the plain API: its throughput, and its latencies measured at the same
+    arrival times."""
     import queue
     import numpy as np
     import torch
@@ -615,19 +643,34 @@ def bench_served(args):
         plain_solve(G, ctx, absn[k], q, plain_out[k])
         svc.append(time.perf_counter() - t0)
     plain_qps = m / sum(svc)
-    full_svc = [svc[i % m] for i in range(n)]
 
-    def fifo(arr):
-        done, lat = 0.0, []
-        for a, s_ in zip(arr, full_svc):
-            done = max(done, a) + s_
-            lat.append((done - a) * 1e3)
+    def plain_at(arr):
+        """The plain arm served one query at a time at the same arrival
+        times: latency = arrival to the read's return, measured."""
+        lat = []
+        t0 = time.perf_counter()
+        for (k, q), a in zip(qs[:m], arr):
+            dt = a - (time.perf_counter() - t0)
+            if dt > 0:
+                time.sleep(dt)
+            plain_solve(G, ctx, absn[k], q, plain_out[k])
+            lat.append((time.perf_counter() - t0 - a) * 1e3)
         return lat
 
     for r in rates:
-        pl = fifo(r.pop("arrivals"))
+        pl = plain_at(r.pop("arrivals"))
         r["plain_p50_ms"] = percentile(pl, 50)
         r["plain_p99_ms"] = percentile(pl, 99)
+        r["plain_queries"] = m
+    cpu = None
+    if not args.no_cpu_baseline and os.path.exists(REF_BIN):
+        sample = [q for k, q in qs if k != "demo"]
+        kq, ref_ms = reference_full_runs(sample)
+        cpu = {"value": kq / (ref_ms * 1e-3), "unit": "queries/s", "cores": 1, "kind": "reference",
+               "sample": f"the first {kq} queries of the stream against the 20x20x16x10 and 32x32x24x16 models, "
+                         f"each a full run of the reference's CPU method as shipped (one thread): {ref_ms:.0f} ms "
+                         f"by its own timers; the 65x65x38x25 model's queries are left out of the sample (its "
+                         f"abstraction alone takes about two minutes on one core), which favours the CPU"}
     line = {
         "metric": "served queries/s", "value": X, "unit": "queries/s", "n_gpus": 1, "steps": 1,
         "warmup": len(warm), "ms_per_step": sat_s * 1e3, "higher_is_better": True, "scaling": "weak",
@@ -646,6 +689,7 @@ def bench_served(args):
                              "p50_service_ms": percentile([x * 1e3 for x in svc], 50),
                              "p99_service_ms": percentile([x * 1e3 for x in svc], 99)},
         "speedup_vs_plain": X / plain_qps,
+        "cpu_baseline": cpu,
         "server": st,
         "gpu_launches": None,
         "clocks": clocks.summary(),
@@ -805,6 +849,13 @@ def main():
     # Dominant kernel: one profiled solve (events around each satisfaction launch).
     prob.solve(profile=True)
     tp = prob.timings()
+    ph = prob.phase_timings()
+    nit = max(ph["profiled_iterations"], 1)
+    phases = {"prefix_or_dilation_us": 1e3 * ph["prefix_build_total_ms"] / nit,
+              "pass_us": [1e3 * v / nit for v in ph["scan_axis_ms"]],
+              "satisfaction_us": 1e3 * ph["pair_satisfaction_ms"] / nit,
+              "finalize_or_control_us": 1e3 * ph["reduce_inputs_ms"] / nit,
+              "note": "per iteration of one host-loop solve with CUDA events around each phase"}
     used = tp["method"]
     kname = "k_sat_stored" if used == G.METHOD_STORED else "k_sat_col"
     per_launch_ms = tp["sat_kernel_ms"] / max(tp["sat_launches"], 1)
@@ -865,6 +916,7 @@ def main():
         "cpu_baseline": cpu,
         "e2e": {"value": replica_value(world, P * r["iterations"], e2e_step), "unit": "pair-checks/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_step},
+        "phases": phases,
         "pair_tests": {"per_step": tp["pair_tests"], "per_s": tp["pair_tests"] / (ms_per_step * 1e-3),
                        "note": "(state, input) tests the kernels actually performed per fixpoint; the rest of the "
                                "nominal pair-checks were skipped exactly (states already decided, inputs after the "

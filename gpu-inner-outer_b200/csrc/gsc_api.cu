@@ -629,7 +629,9 @@ int problem_stage1(gsc_problem* p, const gsc_query_desc* qd) {
     // Per-axis boxes.
     const uint64_t planes = static_cast<uint64_t>(g.slices) * g.M;
     GSC_TRY(palloc(p, &p->xt, planes * g.n[0]));
-    GSC_TRY(palloc(p, &p->yt, planes * g.n[1]));
+    // y tables, class records and dilated rows are read by 16-byte aligned
+    // bulk copies up to three words past their last entry: four spare words.
+    GSC_TRY(palloc(p, &p->yt, planes * g.n[1] + 4));
     GSC_TRY(palloc(p, &p->zt, static_cast<uint64_t>(g.n[2]) * g.mw));
     GSC_TRY(palloc(p, &p->wt, static_cast<uint64_t>(g.n[3]) * g.ma));
     GSC_CU(ctx, launch_axis_tables(g, q, p->abs->xn, p->abs->yn, p->abs->thf, p->abs->vf, p->xt, p->yt, p->zt, p->wt,
@@ -639,7 +641,7 @@ int problem_stage1(gsc_problem* p, const gsc_query_desc* qd) {
     GSC_TRY(palloc(p, &p->dplan, 1));
     GSC_CU(ctx, cudaMemsetAsync(p->dplan, 0, sizeof(PlanRecord), st));
     if (p->fused_candidate) {
-        GSC_TRY(palloc(p, &p->xcls, planes * class_words(g)));
+        GSC_TRY(palloc(p, &p->xcls, planes * class_words(g) + 4));
         GSC_CU(ctx, launch_x_classes(g, p->xt, p->xcls, st));
         GSC_TRY(palloc(p, &p->xrep, planes));
         GSC_CU(ctx, launch_plane_reps(g, p->xt, p->yt, p->wt, p->xrep, &p->dplan->max_reps, st));
@@ -675,7 +677,9 @@ int problem_plan(gsc_problem* p) {
         p->dil = pl.dil;
         // dilated-row offsets are 32-bit in the satisfaction kernel
         if (static_cast<uint64_t>(pl.dil.nk) * pl.dil.nl * g.rows * g.W >= 0xFFFFFFFFull) fused_ok = false;
-        if (fused_smem_bytes(g, class_words(g), p->need_valid, p->max_reps) > kFusedSmemMax) fused_ok = false;
+        if (fused_smem_bytes(g, class_words(g), p->need_valid, p->max_reps, true) > kFusedSmemMax ||
+            fused_smem_bytes(g, class_words(g), p->need_valid, p->max_reps, false) > kFusedSmemMax)
+            fused_ok = false;
     }
     uint32_t method = p->method;
     if (method == GSC_METHOD_AUTO) method = fused_ok ? GSC_METHOD_FUSED : (stored_ok ? GSC_METHOD_STORED : 0);
@@ -754,11 +758,9 @@ int problem_stage2(gsc_problem* p) {
     GSC_TRY(palloc(p, &p->hit, words));
     GSC_TRY(palloc(p, &p->best, g.S));
     const uint64_t combos = static_cast<uint64_t>(p->dil.nk) * p->dil.nl;
-    GSC_TRY(palloc(p, &p->dzw, combos * words));
+    GSC_TRY(palloc(p, &p->dzw, combos * words + 4));
     p->rl_words = static_cast<uint32_t>(g.rows / 32 + 2);
     GSC_TRY(palloc(p, &p->rowlost, 2ull * p->rl_words));
-    GSC_TRY(palloc(p, &p->slice_ticket, g.slices));
-    GSC_CU(ctx, cudaMemsetAsync(p->slice_ticket, 0, static_cast<size_t>(g.slices) * sizeof(uint32_t), st));
     GSC_TRY(palloc(p, &p->offz, static_cast<uint64_t>(g.n[2]) * g.mw));
     GSC_TRY(palloc(p, &p->offv, static_cast<uint64_t>(g.n[3]) * g.ma));
     GSC_CU(ctx, launch_sat_offsets(g, p->zt, p->wt, p->kidx, p->lidx, p->dil.nl, p->offz, p->offv, st));
@@ -775,7 +777,7 @@ int problem_stage2(gsc_problem* p) {
         GSC_CU(ctx, launch_pack_bits(g, 4, p->valid, p->safe, p->srcb, st));
     }
     if (p->need_valid) {
-        GSC_TRY(palloc(p, &p->vzw, combos * words));
+        GSC_TRY(palloc(p, &p->vzw, combos * words + 4));
         GSC_CU(ctx, launch_dilate(g, p->validb, p->vzw, p->dil, nullptr, nullptr, 0, st));
     }
     return GSC_OK;
@@ -836,7 +838,8 @@ FusedFixArgs fused_args(const gsc_problem* p, cudaGraphConditionalHandle cond, i
     a.sat_threads = fused_sat_threads(p->g, p->max_reps);
     a.dzw = p->dzw;
     a.rowlost = p->rowlost;
-    a.slice_ticket = p->slice_ticket;
+    a.shard_begin = p->shard_begin;
+    a.shard_slices = p->shard_slices;
     a.rl_words = p->rl_words;
     a.vzw = p->vzw;
     a.kidx = p->kidx;
@@ -967,13 +970,14 @@ int gsc_problem_solve(gsc_problem* p, uint32_t flags) {
     if (!p) return GSC_ERR_INVALID_ARGUMENT;
     cudaGetLastError();   // a failure of an unrelated earlier call must not be reported here
     gsc_context* ctx = p->ctx;
+    p->shard_begin = p->shard_slices = 0;   // a solve covers the whole grid
     GSC_CU(ctx, cudaSetDevice(ctx->device));
     cudaStream_t st = ctx->stream;
     GSC_CU(ctx, cudaEventRecord(ctx->ev[0], st));
     uint32_t launches = 0;
     double sat_ms = 0.0, scan_ms = 0.0;
     uint32_t sat_launches = 0;
-    const uint32_t per_iter = (p->method == GSC_METHOD_STORED) ? prefix4_launches(p->g) + 2 : 2;
+    const uint32_t per_iter = (p->method == GSC_METHOD_STORED) ? prefix4_launches(p->g) + 2 : 3;
     if (flags & GSC_SOLVE_PROFILE) {
         GSC_CU(ctx, enqueue_init(p));
         launches += 2;
@@ -1050,6 +1054,8 @@ int gsc_problem_solve(gsc_problem* p, uint32_t flags) {
         tests += hs[kStatsCols * i + 2];
         aux += hs[kStatsCols * i + 3];
     }
+    if (hfc.message == kMsgDeviceTimeout)
+        return fail(ctx, GSC_ERR_TIMEOUT, "a bounded device wait for staged rows gave up; the solve stopped");
     p->timings.iterations = hfc.iter;
     p->timings.pair_tests = tests;
     p->timings.aux_count = aux;
@@ -1062,6 +1068,69 @@ int gsc_problem_solve(gsc_problem* p, uint32_t flags) {
         p->timings.scan_kernel_ms = scan_ms;
         p->timings.sat_launches = sat_launches;
     }
+    return GSC_OK;
+}
+
+int gsc_problem_shard_begin(gsc_problem* p, uint32_t slice_begin, uint32_t slice_end) {
+    if (!p) return GSC_ERR_INVALID_ARGUMENT;
+    cudaGetLastError();   // a failure of an unrelated earlier call must not be reported here
+    gsc_context* ctx = p->ctx;
+    if (p->method != GSC_METHOD_FUSED) return fail(ctx, GSC_ERR_UNSUPPORTED, "a sharded solve needs the fused method");
+    if (slice_begin >= slice_end || slice_end > p->g.slices)
+        return fail(ctx, GSC_ERR_INVALID_ARGUMENT, "shard slices out of range");
+    GSC_CU(ctx, cudaSetDevice(ctx->device));
+    p->shard_begin = 0;
+    p->shard_slices = 0;
+    GSC_CU(ctx, enqueue_init(p));
+    GSC_CU(ctx, cudaStreamSynchronize(ctx->stream));
+    p->shard_begin = slice_begin;
+    p->shard_slices = slice_end - slice_begin;
+    p->shard_iter = 0;
+    p->shard_stopped = p->q.max_iterations == 0;
+    return GSC_OK;
+}
+
+int gsc_problem_shard_step(gsc_problem* p, uint64_t counts[2]) {
+    if (!p || !counts) return GSC_ERR_INVALID_ARGUMENT;
+    cudaGetLastError();   // a failure of an unrelated earlier call must not be reported here
+    gsc_context* ctx = p->ctx;
+    if (!p->shard_slices) return fail(ctx, GSC_ERR_INVALID_ARGUMENT, "gsc_problem_shard_begin first");
+    counts[0] = counts[1] = 0;
+    if (p->shard_stopped) return GSC_OK;
+    GSC_CU(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    GSC_CU(ctx, launch_shard_iteration(p->g, fused_args(p, 0, 0), st));
+    unsigned long long row[2];
+    GSC_CU(ctx, cudaMemcpyAsync(row, p->stats + static_cast<uint64_t>(kStatsCols) * (p->shard_iter + 1), sizeof(row),
+                                cudaMemcpyDeviceToHost, st));
+    GSC_CU(ctx, cudaStreamSynchronize(st));
+    counts[0] = row[0];
+    counts[1] = row[1];
+    return GSC_OK;
+}
+
+int gsc_problem_shard_words(const gsc_problem* p, void** dprime_words, uint64_t* words_per_slice) {
+    if (!p || !dprime_words || !words_per_slice) return GSC_ERR_INVALID_ARGUMENT;
+    if (p->method != GSC_METHOD_FUSED) return GSC_ERR_UNSUPPORTED;
+    *dprime_words = p->dp;
+    *words_per_slice = static_cast<uint64_t>(p->g.n[1]) * p->g.W;
+    return GSC_OK;
+}
+
+int gsc_problem_shard_control(gsc_problem* p, uint64_t new_reachable, uint64_t new_certified, int* stop) {
+    if (!p || !stop) return GSC_ERR_INVALID_ARGUMENT;
+    cudaGetLastError();   // a failure of an unrelated earlier call must not be reported here
+    gsc_context* ctx = p->ctx;
+    if (!p->shard_slices) return fail(ctx, GSC_ERR_INVALID_ARGUMENT, "gsc_problem_shard_begin first");
+    GSC_CU(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    if (!p->shard_stopped) GSC_CU(ctx, launch_shard_control(p->fc, p->stats, new_reachable, new_certified, st));
+    FixControl fc;
+    GSC_CU(ctx, cudaMemcpyAsync(&fc, p->fc, sizeof(fc), cudaMemcpyDeviceToHost, st));
+    GSC_CU(ctx, cudaStreamSynchronize(st));
+    p->shard_iter = fc.iter;
+    p->shard_stopped = fc.stop != 0;
+    *stop = p->shard_stopped ? 1 : 0;
     return GSC_OK;
 }
 
@@ -1082,6 +1151,8 @@ int gsc_problem_read(gsc_problem* p, gsc_result* r) {
     r->states = g.S;
     r->inputs = g.M;
     r->pairs = g.S * g.M;
+    if (fc.message == kMsgDeviceTimeout)
+        return fail(ctx, GSC_ERR_TIMEOUT, "the last solve stopped at a bounded device wait that gave up");
     r->iterations = fc.iter;
     r->converged = static_cast<int32_t>(fc.converged);
     r->message = static_cast<int32_t>(fc.message ? fc.message : GSC_MSG_MAX_ITERATIONS);

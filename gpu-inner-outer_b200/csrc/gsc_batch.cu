@@ -44,7 +44,7 @@ InstanceDesc make_instance(const gsc_problem* p) {
 }
 
 size_t instance_smem(const gsc_problem* p) {
-    return fused_smem_bytes(p->g, class_words(p->g), p->need_valid, p->max_reps);
+    return fused_smem_bytes(p->g, class_words(p->g), p->need_valid, p->max_reps, false);
 }
 
 void build_work_list(const std::vector<const gsc_problem*>& probs, const std::vector<uint32_t>& slots,

@@ -207,6 +207,48 @@ __device__ __forceinline__ void cp_async4(void* smem_dst, const void* gmem_src) 
 
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
+// ---- 1-D bulk copies global -> shared (the TMA engine, no tensor map, no
+// multicast) completing on an mbarrier.  Source and destination 16-byte
+// aligned, size a multiple of 16 bytes.
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* mbar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(mbar)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// One arrival that also announces `bytes` of copies completing on the barrier.
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* mbar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(mbar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* mbar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(mbar))
+                 : "memory");
+}
+
+// One bounded probe of the barrier's phase `parity` (the hardware may
+// suspend the thread for a while inside the probe).
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* mbar, uint32_t parity) {
+    uint32_t ok = 0;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_addr(mbar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Probes of a bulk-copy wait before it is given up as failed.
+constexpr uint32_t kBulkWaitProbes = 1u << 20;
+// FixControl::message of a solve stopped by a device wait that gave up.
+constexpr uint32_t kMsgDeviceTimeout = 4;
+
 struct FixControl {
     uint32_t iter;            // iterations completed
     uint32_t stop;            // 1 once a stop rule fired

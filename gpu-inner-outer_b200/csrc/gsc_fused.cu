@@ -11,16 +11,15 @@
 // valid cell already reachable) and, when validity is more than safety, at
 // least one valid cell.
 //
-// One iteration = two launches:
+// One iteration = three launches:
 //   k_dilate         (theta, v)-dilated copies of D' for the box widths in use;
 //   k_sat_col        one block per (theta, v) slice x omega column: tests
 //                    every active state of the slice against every input of
 //                    the column and, per state, records the lowest satisfied
-//                    input with an atomicMin into best[] plus a hit bit; the
-//                    last block of each slice then applies the slice's hits
-//                    (reachable, active, controller, reach_step, counters) and
-//                    builds its D' for the next iteration, and the last slice
-//                    applies the stop rules.
+//                    input with an atomicMin into best[] plus a hit bit;
+//   k_fused_finalize applies the hits (reachable, active, controller,
+//                    reach_step, counters), builds D' for the next iteration,
+//                    and its last block applies the stop rules.
 #include <atomic>
 
 #include "gsc_fused_body.cuh"
@@ -45,8 +44,6 @@ __global__ void k_fused_init(GridInfo g, FusedFixArgs a, const uint8_t* __restri
     for (uint64_t s = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; s < g.S;
          s += static_cast<uint64_t>(gridDim.x) * blockDim.x)
         init_state(a, cand, s);
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < g.slices; k += gridDim.x * blockDim.x)
-        a.slice_ticket[k] = 0;
 }
 
 // (theta, v)-dilated copies of a bit-sliced set, one thread per word
@@ -176,67 +173,71 @@ __global__ void k_sat_offsets(GridInfo g, const uint32_t* __restrict__ zt, const
     }
 }
 
-// One block per (theta, v) slice x omega column (sat_col_task), then the
-// finalize of the iteration without a launch of its own:
-//  - the last block of a slice to finish (a ticket per slice) applies the
-//    slice's hits, builds its next D' and records its rows that lost a D'
-//    cell (finalize_word).  Every block of the slice has written its hits
-//    and best[] entries before it took its ticket, and nothing else in the
-//    launch reads what the finalize writes: the satisfaction tasks read the
-//    dilated copies of D', the active rows of their own slice (changed only
-//    by that slice's finalize, after all of them) and the other row-lost
-//    buffer;
-//  - the last slice to be finalized (a ticket over slices) applies the stop
-//    rules (reachability.hpp:133-144) once every slice's counters are in.
-// Tickets follow the usual pattern: a barrier, then one thread's fence
-// (cumulative over the block's writes and atomics) and atomicAdd; the block
-// that takes the last ticket fences again before reading.
+// One block per (theta, v) slice x omega column (sat_col_task); a sharded
+// solve launches the shard's slices only (task offset shard_begin * mw).
 template <int W, bool NV>
 __global__ void __launch_bounds__(kFusedWarps * 32) k_sat_col(GridInfo g, FusedFixArgs a) {
     extern __shared__ __align__(16) bword smem[];
     __shared__ uint32_t s_meta[4];
-    __shared__ uint32_t s_last;
+    pdl_wait();
+    sat_col_task<W, true, NV ? 1 : 0, false, true>(g, a, blockIdx.x + a.shard_begin * g.mw, smem, s_meta);
+}
+
+// Apply the iteration's hits, build next iteration's D', count, and let the
+// last block to finish apply the stop rules (reachability.hpp:133-144).  A
+// sharded solve finalizes the shard's words only and leaves the stop rules
+// to the host, which applies them with every rank's counts.
+__global__ void __launch_bounds__(256) k_fused_finalize(GridInfo g, FusedFixArgs a) {
     pdl_wait();
     FixControl* fc = a.fc;
-    const uint32_t iter = fc->iter;
     if (fc->stop) {
         // Already stopped (e.g. max_iterations == 0): the graph loop must still end.
         if (a.use_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(a.cond, 0u);
         return;
     }
-    sat_col_task<W, true, NV ? 1 : 0>(g, a, blockIdx.x, smem, s_meta);
-
-    const uint32_t slice = blockIdx.x / g.mw;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        s_last = atomicAdd(a.slice_ticket + slice, 1u) == g.mw - 1;
-    }
-    __syncthreads();
-    if (!s_last) return;
-    __threadfence();
-    const uint32_t it = iter + 1;
-    const bword* __restrict__ rprev = (iter & 1) ? a.reach1 : a.reach0;
-    bword* __restrict__ rnext = (iter & 1) ? a.reach0 : a.reach1;
-    const uint32_t nw = g.n[1] * W;
-    const uint64_t wbase = static_cast<uint64_t>(slice) * nw;
+    const uint32_t it = fc->iter + 1;
+    const bword* __restrict__ rprev = (fc->iter & 1) ? a.reach1 : a.reach0;
+    bword* __restrict__ rnext = (fc->iter & 1) ? a.reach0 : a.reach1;
+    const uint64_t nw = static_cast<uint64_t>(g.n[1]) * g.W;
+    const uint64_t first = static_cast<uint64_t>(a.shard_begin) * nw;
+    const uint64_t words = a.shard_slices ? a.shard_slices * nw : g.rows * g.W;
     unsigned long long nr = 0, nc = 0;
-    for (uint32_t e = threadIdx.x; e < nw; e += blockDim.x)
-        finalize_word<true>(g, a, rprev, rnext, wbase + e, it, nr, nc);
+    for (uint64_t e = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; e < words;
+         e += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+        finalize_word(g, a, rprev, rnext, first + e, it, nr, nc);
     unsigned long long* row = a.stats + kStatsCols * it;
     add_counters(row, nr, nc);
+    // Last block to finish: every block's counters are in.  The counters are
+    // device-scope atomics; the barrier orders a block's atomics before its
+    // first thread's fence (cumulative) and ticket.  Nothing else the last
+    // block reads was written by this kernel's other blocks.
+    __shared__ bool last;
     __syncthreads();
     if (threadIdx.x == 0) {
-        a.slice_ticket[slice] = 0;
         __threadfence();
-        s_last = atomicAdd(&fc->ticket, 1u) == g.slices - 1;
+        last = atomicAdd(&fc->ticket, 1u) == gridDim.x - 1;
     }
     __syncthreads();
-    if (!s_last || threadIdx.x != 0) return;
-    __threadfence();
-    fc->ticket = 0;
+    if (!last) return;
+    if (threadIdx.x == 0) {
+        __threadfence();
+        fc->ticket = 0;
+        if (a.shard_slices) return;
+        control_step(fc, row, it);
+        if (a.use_cond) cudaGraphSetConditional(a.cond, fc->stop ? 0u : 1u);
+    }
+}
+
+// Stop rules of a sharded iteration with the summed counts of every rank.
+__global__ void k_shard_control(FixControl* fc, unsigned long long* stats, unsigned long long nr,
+                                unsigned long long nc) {
+    if (fc->stop) return;
+    const uint32_t it = fc->iter + 1;
+    unsigned long long* row = stats + kStatsCols * it;
+    row[0] = nr;
+    row[1] = nc;
     control_step(fc, row, it);
-    if (a.use_cond) cudaGraphSetConditional(a.cond, fc->stop ? 0u : 1u);
+    fc->last_new = 0xFFFFFFFFu;   // every iteration of a sharded solve tests every pair
 }
 
 template <int W, bool NV>
@@ -254,7 +255,8 @@ cudaError_t launch_sat_col_t(const GridInfo& g, const FusedFixArgs& a, size_t sm
         if (e != cudaSuccess) return e;
         if (dev >= 0 && dev < 64) configured[dev].store(true);
     }
-    return launch_pdl(k_sat_col<W, NV>, dim3(g.slices * g.mw), dim3(a.sat_threads), sm, st, g, a);
+    const uint32_t slices = a.shard_slices ? a.shard_slices : g.slices;
+    return launch_pdl(k_sat_col<W, NV>, dim3(slices * g.mw), dim3(a.sat_threads), sm, st, g, a);
 }
 
 }  // namespace
@@ -264,15 +266,10 @@ uint32_t fused_sat_threads(const GridInfo& g, uint32_t max_reps) {
     return work <= 1024 ? 64u : work <= 2304 ? 128u : 256u;
 }
 
-size_t fused_smem_bytes(const GridInfo& g, uint32_t cls_words, int need_valid, uint32_t max_reps) {
-    const size_t nw = static_cast<size_t>(g.n[1]) * g.W;
-    const size_t nv = need_valid ? 2 : 1;
-    const size_t mr = max_reps;
-    // act, E rows (D' and valid), sat, class records, y tables, representatives (acceleration, v window,
-    // offset part), changed-row masks
-    const size_t words = nw + mr * nw * nv + mr * nw + mr * cls_words + mr * g.n[1] + 3 * static_cast<size_t>(g.ma) +
-                         mr * ((g.n[1] + 31) / 32);
-    return sizeof(bword) * words;
+size_t fused_smem_bytes(const GridInfo& g, uint32_t cls_words, int need_valid, uint32_t max_reps, bool bulk) {
+    const FusedSmemLayout L =
+        fused_smem_layout(g.n[1] * g.W, need_valid ? 2u : 1u, max_reps, cls_words, g.n[1], g.ma, bulk);
+    return sizeof(bword) * static_cast<size_t>(L.total);
 }
 
 cudaError_t launch_plan(const GridInfo& g, const uint32_t* zt, const uint32_t* wt, const uint8_t* xrep,
@@ -304,14 +301,26 @@ cudaError_t launch_fused_init(const GridInfo& g, const FusedFixArgs& a, const ui
     return cudaGetLastError();
 }
 
+cudaError_t launch_shard_iteration(const GridInfo& g, const FusedFixArgs& a, cudaStream_t st) {
+    return launch_fused_iteration(g, a, st, nullptr, nullptr);
+}
+
+cudaError_t launch_shard_control(FixControl* fc, unsigned long long* stats, unsigned long long new_reachable,
+                                 unsigned long long new_certified, cudaStream_t st) {
+    k_shard_control<<<1, 1, 0, st>>>(fc, stats, new_reachable, new_certified);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_fused_iteration(const GridInfo& g, const FusedFixArgs& a, cudaStream_t st, uint32_t* launches,
                                    cudaEvent_t* ev) {
     if (ev) cudaEventRecord(ev[0], st);
-    cudaError_t derr = launch_dilate(g, a.dp, a.dzw, a.dil, a.fc, a.rowlost, a.rl_words, st);
+    // A sharded solve dilates the whole grid every iteration: the other
+    // ranks' D' slabs arrive without row-lost records.
+    cudaError_t derr = launch_dilate(g, a.dp, a.dzw, a.dil, a.fc, a.shard_slices ? nullptr : a.rowlost, a.rl_words, st);
     if (derr != cudaSuccess) return derr;
     if (ev)
         for (int k = 1; k <= 4; ++k) cudaEventRecord(ev[k], st);
-    const size_t sm = fused_smem_bytes(g, a.cls_words, a.need_valid, a.max_reps);
+    const size_t sm = fused_smem_bytes(g, a.cls_words, a.need_valid, a.max_reps, true);
     cudaError_t err;
 #define GSC_SAT_CASE(Wn)                                                                         \
     case Wn:                                                                                     \
@@ -331,11 +340,13 @@ cudaError_t launch_fused_iteration(const GridInfo& g, const FusedFixArgs& a, cud
     }
 #undef GSC_SAT_CASE
     if (err != cudaSuccess) return err;
-    if (ev) {
-        cudaEventRecord(ev[5], st);
-        cudaEventRecord(ev[6], st);
-    }
-    if (launches) *launches += 2;
+    if (ev) cudaEventRecord(ev[5], st);
+    const uint64_t words = a.shard_slices ? static_cast<uint64_t>(a.shard_slices) * g.n[1] * g.W : g.rows * g.W;
+    uint64_t fb = (words + 255) / 256;
+    if (fb > 4096) fb = 4096;
+    if (launches) *launches += 3;
+    err = launch_pdl(k_fused_finalize, dim3(static_cast<unsigned int>(fb ? fb : 1)), dim3(256), 0, st, g, a);
+    if (ev) cudaEventRecord(ev[6], st);
     return err;
 }
 

@@ -26,21 +26,15 @@ __device__ __forceinline__ bword extract_bits(const bword (&F)[W], uint32_t lx, 
     return len >= kBits ? v : (v & ((bword(1) << len) - 1));
 }
 
-// acc |= F shifted so that bit i of the result is bit i + d of F (|d| < 32):
-// one funnel shift per word.
-template <int W>
-__device__ __forceinline__ void or_shifted(const bword (&F)[W], int d, bword (&acc)[W]) {
-    if (d >= 0) {
-#pragma unroll
-        for (int w = 0; w < W; ++w) acc[w] |= __funnelshift_r(F[w], (w + 1 < W) ? F[w + 1] : 0u, d);
-    } else {
-#pragma unroll
-        for (int w = 0; w < W; ++w) acc[w] |= __funnelshift_l((w > 0) ? F[w - 1] : 0u, F[w], -d);
-    }
-}
-
-__device__ __forceinline__ int hdr_byte(const bword* rec, int k) {
-    return static_cast<int8_t>((rec[k >> 2] >> (8 * (k & 3))) & 0xFFu);
+// Word w (0 <= w <= WMAX) of the row F moved by d (|d| < 32): bit j of the
+// result is bit 32 w + j + d of F, with F zero outside its WMAX words.
+template <int WMAX>
+__device__ __forceinline__ bword moved_word(const bword (&F)[WMAX], int w, int d) {
+    const bword fm1 = (w >= 1 && w - 1 < WMAX) ? F[w - 1] : 0u;
+    const bword f0 = (w < WMAX) ? F[w] : 0u;
+    const bword fp1 = (w + 1 < WMAX) ? F[w + 1] : 0u;
+    const bool up = d >= 0;
+    return __funnelshift_r(up ? f0 : fm1, up ? fp1 : f0, static_cast<uint32_t>(d) & 31u);
 }
 
 // Initial sets of word e: reachable = candidate, active = valid && safe
@@ -163,22 +157,30 @@ __device__ __forceinline__ int group_sync_or(int p) {
 //     whose boxes coincide), E[y] = the (theta, v)-dilated D' row at the
 //     input's box corner: one load per word;
 //  C. each (representative, i1) item: F = OR of E over row i1's y range, then
-//     the x test 32 states per word: the x boxes of a plane fall into a few
-//     classes (lo - i0, hi - i0) = (a, b), and a state of class (a, b) is
-//     blocked when F has a bit in [i0 + a, i0 + b], i.e. bit i0 of
-//     OR_{d=a..b} (F >> d); a plane with more than kClassMax classes is tested
-//     state by state;
+//     the x test 32 states per word: a state whose x box is [i0 + a, i0 + b]
+//     is blocked when F has a bit in it, i.e. bit i0 of OR_{d=a..b} (F >> d);
+//     with the plane's shift masks M_d (the states whose box holds i0 + d,
+//     launch_x_classes) that is bit i0 of OR_d ((F >> d) & M_d), one funnel
+//     shift per word and shift for the whole word of states; a plane with
+//     boxes of more than kShiftMax shifts is tested state by state;
 //  D. per state, the lowest satisfied input of the column goes to best[]
 //     (atomicMin, so the lowest over all columns wins) and the hit bit is set.
 // WMAX: register words per row; EXACTW: g.W == WMAX (else g.W <= WMAX at run
 // time).  NVMODE: 0 / 1 = validity test off / on, 2 = a.need_valid decides.
 // WARP: the task is one warp's (its own smem and s_meta), else the block's.
+// BULK (one task per block only): phase B stages each representative's rows,
+// class record and y table with three 1-D bulk copies (the TMA engine) that
+// complete on an mbarrier, instead of one cp.async per word.  A bulk copy
+// needs 16-byte aligned ends, so each copies the aligned span around its
+// words into a 16-byte aligned slot, and readers add the span's leading
+// offset (fused_smem_layout).
 // Every early return is taken by the whole group.
 constexpr unsigned long long kIncrementalRows = 16;
 
-template <int WMAX, bool EXACTW, int NVMODE, bool WARP = false>
+template <int WMAX, bool EXACTW, int NVMODE, bool WARP = false, bool BULK = false>
 __device__ __forceinline__ void sat_col_task(const GridInfo& g, const FusedFixArgs& a, uint32_t task,
                                              bword* smem, uint32_t* s_meta) {
+    static_assert(!(BULK && WARP), "bulk staging is for one task per block");
     const FixControl* fc = a.fc;
     const uint32_t W = EXACTW ? static_cast<uint32_t>(WMAX) : g.W;
     const bool NV = NVMODE == 2 ? (a.need_valid != 0) : (NVMODE == 1);
@@ -194,16 +196,20 @@ __device__ __forceinline__ void sat_col_task(const GridInfo& g, const FusedFixAr
     const uint32_t cw = a.cls_words;
     const uint32_t mr = a.max_reps;
 
-    bword* act = smem;
-    bword* Eall = act + nw;                               // max_reps * nw * nv
-    bword* sat = Eall + mr * nw * nv;                     // max_reps * nw
-    bword* cls = sat + mr * nw;                           // max_reps * cw
-    uint32_t* yts = cls + mr * cw;                        // max_reps * n1
-    uint32_t* reps = yts + mr * n1;                       // ma: acceleration of each representative slot
+    const FusedSmemLayout L = fused_smem_layout(nw, nv, mr, cw, n1, ma, BULK);
+    bword* act = smem + L.act;
+    bword* Eall = smem + L.E;                             // max_reps * nv * L.e_stride
+    bword* sat = smem + L.sat;                            // max_reps * nw
+    bword* cls = smem + L.cls;                            // max_reps * L.c_stride
+    uint32_t* yts = smem + L.yts;                         // max_reps * L.y_stride
+    uint32_t* reps = smem + L.reps;                       // ma: acceleration of each representative slot
     uint32_t* repw = reps + ma;                           // ma: its v window
     uint32_t* repo = repw + ma;                           // ma: its part of the dilated rows' offset
-    uint32_t* rowchg = repo + ma;                         // max_reps * W1: y rows of a window that lost a cell
+    uint32_t* rowchg = smem + L.rowchg;                   // max_reps * W1: y rows of a window that lost a cell
+    uint32_t* rsh = smem + L.rsh;                         // BULK, ma: leading offsets of a rep's three spans
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + L.mbar);
     const uint32_t W1 = (n1 + 31) / 32;
+    if (BULK && tid == 0) mbar_init(mbar, 1);
 
     const uint64_t pcol = (static_cast<uint64_t>(i2) * g.n[3] + i3) * g.M + static_cast<uint64_t>(ma) * jw;
     // A. One round of loads that depend on the task alone: the active rows
@@ -274,16 +280,48 @@ __device__ __forceinline__ void sat_col_task(const GridInfo& g, const FusedFixAr
     // none stages nothing and skips, and a (representative, row) item whose
     // y range has none is skipped; their states still fail.
     auto stage = [&]() {
-        for (uint32_t e = tid; e < nrep * nw; e += bd) {
-            const uint32_t r = fdiv(e, g.magic_nw), rem = e - r * nw;
-            const uint32_t off = offz + repo[r] + rem;
-            cp_async4(Eall + r * nw * nv + rem, a.dzw + off);
-            if (NV) cp_async4(Eall + r * nw * nv + nw + rem, a.vzw + off);
-        }
-        for (uint32_t r = tid >> 5; r < nrep; r += bd >> 5) {
-            const uint64_t pl = pcol + reps[r];
-            for (uint32_t e = lane; e < cw; e += 32) cp_async4(cls + r * cw + e, a.xcls + pl * cw + e);
-            for (uint32_t e = lane; e < n1; e += 32) cp_async4(yts + r * n1 + e, a.yt + pl * n1 + e);
+        if constexpr (BULK) {
+            // Warp 0: lane r issues representative r's copies after lane 0
+            // has announced every copy's bytes on the barrier.
+            if (tid < 32) {
+                uint32_t bytes = 0;
+                for (uint32_t r = lane; r < nrep; r += 32) {
+                    const uint32_t offe = offz + repo[r];
+                    const uint64_t pl = pcol + reps[r];
+                    const uint32_t she = offe & 3u, shc = static_cast<uint32_t>(pl * cw) & 3u,
+                                   shy = static_cast<uint32_t>(pl * n1) & 3u;
+                    bytes += 4u * (nv * ((nw + she + 3u) & ~3u) + ((cw + shc + 3u) & ~3u) + ((n1 + shy + 3u) & ~3u));
+                }
+                for (int off = 16; off > 0; off >>= 1) bytes += __shfl_down_sync(0xFFFFFFFFu, bytes, off);
+                if (lane == 0) mbar_arrive_expect_tx(mbar, bytes);
+                __syncwarp();
+                for (uint32_t r = lane; r < nrep; r += 32) {
+                    const uint32_t offe = offz + repo[r];
+                    const uint64_t pl = pcol + reps[r];
+                    const uint32_t she = offe & 3u;
+                    const uint64_t offc = pl * cw, offy = pl * n1;
+                    const uint32_t shc = static_cast<uint32_t>(offc) & 3u, shy = static_cast<uint32_t>(offy) & 3u;
+                    bword* e0 = Eall + r * nv * L.e_stride;
+                    const uint32_t ne = 4u * ((nw + she + 3u) & ~3u);
+                    bulk_copy_g2s(e0, a.dzw + (offe - she), ne, mbar);
+                    if (NV) bulk_copy_g2s(e0 + L.e_stride, a.vzw + (offe - she), ne, mbar);
+                    bulk_copy_g2s(cls + r * L.c_stride, a.xcls + (offc - shc), 4u * ((cw + shc + 3u) & ~3u), mbar);
+                    bulk_copy_g2s(yts + r * L.y_stride, a.yt + (offy - shy), 4u * ((n1 + shy + 3u) & ~3u), mbar);
+                    rsh[r] = she | (shc << 8) | (shy << 16);
+                }
+            }
+        } else {
+            for (uint32_t e = tid; e < nrep * nw; e += bd) {
+                const uint32_t r = fdiv(e, g.magic_nw), rem = e - r * nw;
+                const uint32_t off = offz + repo[r] + rem;
+                cp_async4(Eall + r * nw * nv + rem, a.dzw + off);
+                if (NV) cp_async4(Eall + r * nw * nv + nw + rem, a.vzw + off);
+            }
+            for (uint32_t r = tid >> 5; r < nrep; r += bd >> 5) {
+                const uint64_t pl = pcol + reps[r];
+                for (uint32_t e = lane; e < cw; e += 32) cp_async4(cls + r * cw + e, a.xcls + pl * cw + e);
+                for (uint32_t e = lane; e < n1; e += 32) cp_async4(yts + r * n1 + e, a.yt + pl * n1 + e);
+            }
         }
     };
     if (!incremental) stage();
@@ -310,8 +348,24 @@ __device__ __forceinline__ void sat_col_task(const GridInfo& g, const FusedFixAr
         if (!group_sync_or<WARP>(lost)) return;
         stage();
     }
-    cp_async_wait_all();
-    group_sync<WARP>();
+    if constexpr (BULK) {
+        // Bounded wait for the copies.  A wait that gives up (it cannot in a
+        // working device: the copies are a few KB) stops the solve with
+        // kMsgDeviceTimeout, which the host reports as GSC_ERR_TIMEOUT, and
+        // waits once more, again bounded, before the block leaves.
+        bool done = false;
+        for (uint32_t k = 0; k < kBulkWaitProbes && !done; ++k) done = mbar_try_wait(mbar, 0);
+        if (!done) {
+            FixControl* wfc = a.fc;
+            wfc->message = kMsgDeviceTimeout;
+            atomicExch(&wfc->stop, 1u);
+            for (uint32_t k = 0; k < kBulkWaitProbes && !done; ++k) done = mbar_try_wait(mbar, 0);
+        }
+        if (group_sync_or<WARP>(done ? 0 : 1)) return;
+    } else {
+        cp_async_wait_all();
+        group_sync<WARP>();
+    }
     if (tid == 0) atomicAdd(a.stats + kStatsCols * (it + 1) + 3, static_cast<unsigned long long>(nrep));
     // C. the (representative, row) items.
     unsigned long long ntest = 0;
@@ -326,7 +380,8 @@ __device__ __forceinline__ void sat_col_task(const GridInfo& g, const FusedFixAr
             sw[w] = 0;
             anyc |= cm[w];
         }
-        const uint32_t ye = yts[r * n1 + i1];
+        const uint32_t rs = BULK ? rsh[r] : 0u;
+        const uint32_t ye = BULK ? yts[r * L.y_stride + (rs >> 16) + i1] : yts[r * n1 + i1];
         if (anyc && ye != kReject && incremental) {
             // Bits [lo, hi] of the representative's changed-row mask (fused
             // boxes span at most 32 rows): one funnel shift.
@@ -340,7 +395,8 @@ __device__ __forceinline__ void sat_col_task(const GridInfo& g, const FusedFixAr
         if (anyc && ye != kReject) {
 #pragma unroll
             for (int w = 0; w < WMAX; ++w) ntest += __popc(cm[w]);
-            const bword* E = Eall + r * nw * nv;
+            const bword* E = BULK ? Eall + r * nv * L.e_stride + (rs & 0xFFu) : Eall + r * nw * nv;
+            const uint32_t ev = BULK ? L.e_stride : nw;   // the valid rows follow the D' rows
             bword F[WMAX], FV[WMAX];
 #pragma unroll
             for (int w = 0; w < WMAX; ++w) F[w] = FV[w] = 0;
@@ -349,36 +405,41 @@ __device__ __forceinline__ void sat_col_task(const GridInfo& g, const FusedFixAr
                 for (int w = 0; w < WMAX; ++w) {
                     if (!EXACTW && static_cast<uint32_t>(w) >= W) continue;
                     F[w] |= E[y * W + w];
-                    if (NV) FV[w] |= E[nw + y * W + w];
+                    if (NV) FV[w] |= E[ev + y * W + w];
                 }
             }
-            const bword* rec = cls + r * cw;
-            const uint32_t ncls = rec[0] & 0xFFu;
-            if (ncls != 0xFFu) {
-                bword U[WMAX], VA[WMAX], OK[WMAX];
+            const bword* rec = BULK ? cls + r * L.c_stride + ((rs >> 8) & 0xFFu) : cls + r * cw;
+            const bword hdr = rec[0];
+            const uint32_t nd = hdr & 0xFFu;
+            if (nd != 0xFFu) {
+                // U = OR_d ((F >> d) & M_d) over the plane's shifts (and VA
+                // likewise over the valid rows): G is F moved by dmin, one
+                // word longer, so every shift is a right funnel shift by
+                // d - dmin in [0, kShiftMax).
+                const int dmin = static_cast<int8_t>((hdr >> 8) & 0xFFu);
+                bword G[WMAX + 1], GV[WMAX + 1];
 #pragma unroll
-                for (int w = 0; w < WMAX; ++w) U[w] = VA[w] = OK[w] = 0;
-                for (uint32_t c = 0; c < ncls; ++c) {
-                    const int ca = hdr_byte(rec, 1 + c);
-                    const int cb = hdr_byte(rec, 7 + c);
-                    bword win[WMAX], winv[WMAX];
+                for (int w = 0; w <= WMAX; ++w) {
+                    G[w] = moved_word<WMAX>(F, w, dmin);
+                    GV[w] = NV ? moved_word<WMAX>(FV, w, dmin) : 0u;
+                }
+                bword U[WMAX], VA[WMAX];
 #pragma unroll
-                    for (int w = 0; w < WMAX; ++w) win[w] = winv[w] = 0;
-                    for (int d = ca; d <= cb; ++d) {
-                        or_shifted<WMAX>(F, d, win);
-                        if (NV) or_shifted<WMAX>(FV, d, winv);
-                    }
+                for (int w = 0; w < WMAX; ++w) U[w] = VA[w] = 0;
+                for (uint32_t i = 0; i < nd; ++i) {
 #pragma unroll
                     for (int w = 0; w < WMAX; ++w) {
                         if (!EXACTW && static_cast<uint32_t>(w) >= W) continue;
-                        const bword m = rec[4 + c * W + w];
-                        OK[w] |= m;
-                        U[w] |= win[w] & m;
-                        if (NV) VA[w] |= winv[w] & m;
+                        const bword m = rec[4 + i * W + w];
+                        U[w] |= __funnelshift_r(G[w], G[w + 1], i) & m;
+                        if (NV) VA[w] |= __funnelshift_r(GV[w], GV[w + 1], i) & m;
                     }
                 }
 #pragma unroll
-                for (int w = 0; w < WMAX; ++w) sw[w] = cm[w] & OK[w] & ~U[w] & (NV ? VA[w] : ~0u);
+                for (int w = 0; w < WMAX; ++w) {
+                    const bword ok = (EXACTW || static_cast<uint32_t>(w) < W) ? rec[4 + kShiftMax * W + w] : 0u;
+                    sw[w] = cm[w] & ok & ~U[w] & (NV ? VA[w] : ~0u);
+                }
             } else {
                 const uint32_t* xrow = a.xt + (pcol + ja) * n0;
 #pragma unroll

@@ -134,7 +134,9 @@ struct gsc_problem {
     uint32_t max_reps = 0;
     gsc_b200::bword *dzw = nullptr, *vzw = nullptr;
     uint32_t* rowlost = nullptr;
-    uint32_t* slice_ticket = nullptr;
+    // sharded solve (gsc_problem_shard_*): this rank's slices and iterations done
+    uint32_t shard_begin = 0, shard_slices = 0, shard_iter = 0;
+    bool shard_stopped = false;
     uint32_t rl_words = 0;
     uint32_t* offz = nullptr;   // per omega column and theta cell: part of a dilated row's offset
     uint32_t* offv = nullptr;   // per acceleration and v cell: the other part

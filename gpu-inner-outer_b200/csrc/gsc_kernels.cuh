@@ -194,16 +194,52 @@ struct FusedFixArgs {
     // v cell (sums modulo 2^32, as dzw offsets are 32-bit):
     const uint32_t* offz;      // [n2 * mw]: kslot * nl * rows * W + n1 * lz * W
     const uint32_t* offv;      // [n3 * ma]: lslot * rows * W + n1 * n2 * lw * W
-    uint32_t* slice_ticket;    // [slices]: satisfaction blocks of the slice done this iteration
-                               // (one-problem kernel; zero between iterations)
+    // Sharded solve (one rank of several): the satisfaction launch covers
+    // slices [shard_begin, shard_begin + shard_slices) only, and the stop
+    // rules are left to the host, which applies them with the counts of
+    // every rank (gsc_problem_shard_control).  shard_slices == 0: not sharded.
+    uint32_t shard_begin;
+    uint32_t shard_slices;
     cudaGraphConditionalHandle cond;
     int use_cond;
 };
 constexpr int kFusedWarps = 8;   // most warps of a satisfaction block
-constexpr int kClassMax = 6;
+
+// Shared-memory layout of one satisfaction task, in 32-bit words: the
+// active rows, the representatives' dilated D' (and valid) rows, their
+// satisfied masks, class records and y tables, the representatives' index,
+// v window and offset part, the changed-row masks, and with bulk staging
+// the spans' leading offsets and the mbarrier.  Bulk staging gives every
+// staged span a 16-byte aligned slot three words longer than its data.
+struct FusedSmemLayout {
+    uint32_t act, E, sat, cls, yts, reps, rowchg, rsh, mbar, total;
+    uint32_t e_stride, c_stride, y_stride;
+};
+__host__ __device__ inline FusedSmemLayout fused_smem_layout(uint32_t nw, uint32_t nv, uint32_t mr, uint32_t cw,
+                                                             uint32_t n1, uint32_t ma, bool bulk) {
+    auto r4 = [](uint32_t x) { return (x + 3u) & ~3u; };
+    const uint32_t w1 = (n1 + 31) / 32;
+    FusedSmemLayout L;
+    L.act = 0;
+    L.e_stride = bulk ? r4(nw + 3) : nw;
+    L.c_stride = bulk ? r4(cw + 3) : cw;
+    L.y_stride = bulk ? r4(n1 + 3) : n1;
+    L.E = bulk ? r4(nw) : nw;
+    L.sat = L.E + mr * nv * L.e_stride;
+    L.cls = bulk ? r4(L.sat + mr * nw) : L.sat + mr * nw;
+    L.yts = L.cls + mr * L.c_stride;
+    L.reps = L.yts + mr * L.y_stride;
+    L.rowchg = L.reps + 3 * ma;
+    L.rsh = L.rowchg + mr * w1;
+    L.mbar = bulk ? ((L.rsh + ma + 1) & ~1u) : L.rsh;
+    L.total = bulk ? L.mbar + 2 : L.rsh;
+    return L;
+}
+constexpr int kShiftMax = 8;   // most shifts d of a plane's shift-mask record
 constexpr size_t kFusedSmemMax = 200 * 1024;
-// Dynamic shared memory of the fused satisfaction kernel.
-size_t fused_smem_bytes(const GridInfo& g, uint32_t cls_words, int need_valid, uint32_t max_reps);
+// Dynamic shared memory of one fused satisfaction task (bulk: the
+// one-problem kernel's bulk-staged layout; else the batched kernels').
+size_t fused_smem_bytes(const GridInfo& g, uint32_t cls_words, int need_valid, uint32_t max_reps, bool bulk);
 // Threads per satisfaction block for a problem: more when a block has more
 // representative rows to stage and test (max_reps * n1 * W words).
 uint32_t fused_sat_threads(const GridInfo& g, uint32_t max_reps);
@@ -295,11 +331,16 @@ cudaError_t launch_batch_step(const InstanceDesc* descs, const WorkList& small, 
 // task's staging (smem).
 inline size_t batch_sat_smem(const BatchShape& sh, size_t smem) { return sh.warp ? (sh.sat_threads / 32) * smem : smem; }
 
-// Class record words per plane: a 16-byte header + kClassMax * W masks.
-inline uint32_t class_words(const GridInfo& g) { return 4 + kClassMax * g.W; }
-// Per (slice, input) plane: the classes (lo - i0, hi - i0) = (a, b) of its x
-// boxes.  Header bytes: [0] count (0xFF = irregular), [1 + c] a[c], [7 + c]
-// b[c] (int8); then the state mask of each class.  |a|, |b| < 32.
+// Shift-mask record words per plane: a 16-byte header + (kShiftMax + 1) * W masks.
+__host__ __device__ inline uint32_t class_words(const GridInfo& g) { return 4 + (kShiftMax + 1) * g.W; }
+// Per (slice, input) plane, the x boxes [i0 + a, i0 + b] of its states as
+// shift masks: M_d = the states whose box holds i0 + d, for the nd shifts
+// d = dmin .. dmin + nd - 1 (nd <= kShiftMax), and OK = the states with a
+// box.  A state is blocked by a row F exactly when bit i0 of
+// OR_d ((F >> d) & M_d) is set.  Header word 0: byte 0 = nd (0xFF: the plane
+// is irregular and tested state by state), byte 1 = dmin (int8); then M_d
+// for each d (W words each) at word 4 + (d - dmin) * W, and OK at word
+// 4 + kShiftMax * W.  |a|, |b| < 32.
 cudaError_t launch_x_classes(const GridInfo& g, const uint32_t* xt, bword* xcls, cudaStream_t st);
 // Per plane (slice, j = ja + ma * jw): the lowest ja' of the same omega column
 // whose x row, y row and v box equal those of ja, so the two inputs test every
@@ -312,13 +353,20 @@ cudaError_t launch_fused_init(const GridInfo& g, const FusedFixArgs& a, const ui
 // The offz / offv tables of a problem (after its plan: kidx, lidx, nl).
 cudaError_t launch_sat_offsets(const GridInfo& g, const uint32_t* zt, const uint32_t* wt, const uint8_t* kidx,
                                const uint8_t* lidx, uint32_t nl, uint32_t* offz, uint32_t* offv, cudaStream_t st);
-// One iteration is two launches: the dilation, then the satisfaction kernel,
-// whose last block of each (theta, v) slice finalizes the slice and whose
-// last finalizing block applies the stop rules.
+// One iteration is three launches: the dilation, the satisfaction kernel
+// and the finalize kernel (whose last block applies the stop rules).
 // ev (optional, kProfileEvents events): [0] before the dilation, [1..4] after
-// it, [5] and [6] after the satisfaction kernel.
+// it, [5] after the satisfaction kernel, [6] after the finalize kernel.
 cudaError_t launch_fused_iteration(const GridInfo& g, const FusedFixArgs& a, cudaStream_t st, uint32_t* launches,
                                    cudaEvent_t* ev = nullptr);
+
+// Sharded solve: the iteration's dilation (of the whole grid) and
+// satisfaction (of the shard's slices) without the stop rules.
+cudaError_t launch_shard_iteration(const GridInfo& g, const FusedFixArgs& a, cudaStream_t st);
+// Stop rules of a sharded solve's iteration fc->iter + 1 with the counts of
+// every rank; the next iteration is never incremental.
+cudaError_t launch_shard_control(FixControl* fc, unsigned long long* stats, unsigned long long new_reachable,
+                                 unsigned long long new_certified, cudaStream_t st);
 
 // Resets the control block and zeroes the per-iteration counters.
 cudaError_t launch_fix_init(FixControl* fc, uint32_t max_iterations, uint32_t stats_cap,

@@ -462,16 +462,16 @@ __global__ void k_export(GridInfo g, ExportArgs a) {
     }
 }
 
-// Classes of the x boxes of one (slice, input) plane: states whose box is
-// [i0 + a, i0 + b] share the class (a, b).  Up to kClassMax classes with
-// |a|, |b| < 32, else the plane is marked irregular (0xFF) and tested state
-// by state.
+// Shift masks of the x boxes of one (slice, input) plane (class_words): a
+// state whose box is [i0 + a, i0 + b] is in M_d for every d in [a, b].  A
+// box beyond 31 cells of its state, or more than kShiftMax shifts in the
+// plane, marks the plane irregular (0xFF), tested state by state.
 // One thread per plane; a block first copies its planes' x rows (contiguous)
 // into shared memory in one coalesced round, then each thread scans its row
-// there (a row stride of n0 words).
+// there twice (a row stride of n0 words): the shift range, then the masks.
 __global__ void k_x_classes(GridInfo g, const uint32_t* __restrict__ xt, bword* __restrict__ out) {
     extern __shared__ uint32_t s_xrows[];
-    const uint32_t cw = 4 + kClassMax * g.W;
+    const uint32_t cw = class_words(g);
     const uint32_t n0 = g.n[0];
     const uint64_t planes = static_cast<uint64_t>(g.slices) * g.M;
     for (uint64_t first = blockIdx.x * static_cast<uint64_t>(blockDim.x); first < planes;
@@ -484,12 +484,9 @@ __global__ void k_x_classes(GridInfo g, const uint32_t* __restrict__ xt, bword* 
         if (threadIdx.x >= np) continue;
         const uint64_t plane = first + threadIdx.x;
         const uint32_t* row = s_xrows + threadIdx.x * n0;
-        int cnt = 0, A[kClassMax], B[kClassMax];
-        bword masks[kClassMax][kMaxWords];
-        for (int c = 0; c < kClassMax; ++c)
-            for (int w = 0; w < kMaxWords; ++w) masks[c][w] = 0;
+        int dmin = 32, dmax = -32;
         bool irregular = false;
-        for (uint32_t i0 = 0; i0 < g.n[0] && !irregular; ++i0) {
+        for (uint32_t i0 = 0; i0 < n0; ++i0) {
             const uint32_t xe = row[i0];
             if (xe == kReject) continue;
             const int a = static_cast<int>(lo16(xe)) - static_cast<int>(i0);
@@ -498,33 +495,35 @@ __global__ void k_x_classes(GridInfo g, const uint32_t* __restrict__ xt, bword* 
                 irregular = true;
                 break;
             }
-            int c = 0;
-            while (c < cnt && !(A[c] == a && B[c] == b)) ++c;
-            if (c == cnt) {
-                if (cnt == kClassMax) {
-                    irregular = true;
-                    break;
-                }
-                A[cnt] = a;
-                B[cnt] = b;
-                ++cnt;
-            }
-            masks[c][i0 / kBits] |= bword(1) << (i0 % kBits);
+            dmin = min(dmin, a);
+            dmax = max(dmax, b);
         }
-        uint8_t hdr[16] = {};
-        hdr[0] = irregular ? 0xFF : static_cast<uint8_t>(cnt);
-        if (!irregular) {
-            for (int c = 0; c < cnt; ++c) {
-                hdr[1 + c] = static_cast<uint8_t>(static_cast<int8_t>(A[c]));
-                hdr[7 + c] = static_cast<uint8_t>(static_cast<int8_t>(B[c]));
-            }
-        }
+        const int nd = (dmax >= dmin) ? dmax - dmin + 1 : 0;
+        if (nd > kShiftMax) irregular = true;
         bword* o = out + plane * cw;
-        for (int k = 0; k < 4; ++k)
-            o[k] = static_cast<bword>(hdr[4 * k]) | (static_cast<bword>(hdr[4 * k + 1]) << 8) |
-                   (static_cast<bword>(hdr[4 * k + 2]) << 16) | (static_cast<bword>(hdr[4 * k + 3]) << 24);
-        for (int c = 0; c < kClassMax; ++c)
-            for (uint32_t w = 0; w < g.W; ++w) o[4 + c * g.W + w] = irregular ? 0 : masks[c][w];
+        o[0] = irregular ? 0xFFu
+                         : static_cast<bword>(nd) |
+                               (static_cast<bword>(static_cast<uint8_t>(static_cast<int8_t>(nd ? dmin : 0))) << 8);
+        o[1] = o[2] = o[3] = 0;
+        // One x word at a time, its masks in registers.
+        for (uint32_t w = 0; w < g.W; ++w) {
+            bword m[kShiftMax + 1];
+#pragma unroll
+            for (int k = 0; k <= kShiftMax; ++k) m[k] = 0;
+            for (uint32_t i0 = w * kBits; !irregular && i0 < min(n0, (w + 1) * kBits); ++i0) {
+                const uint32_t xe = row[i0];
+                if (xe == kReject) continue;
+                const int a = static_cast<int>(lo16(xe)) - static_cast<int>(i0) - dmin;
+                const int b = static_cast<int>(hi16(xe)) - static_cast<int>(i0) - dmin;
+                const bword bit = bword(1) << (i0 % kBits);
+#pragma unroll
+                for (int k = 0; k < kShiftMax; ++k)
+                    if (k >= a && k <= b) m[k] |= bit;
+                m[kShiftMax] |= bit;
+            }
+#pragma unroll
+            for (int k = 0; k <= kShiftMax; ++k) o[4 + k * g.W + w] = m[k];
+        }
     }
 }
 

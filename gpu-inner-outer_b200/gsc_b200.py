@@ -150,6 +150,11 @@ SIGNATURES = {
     "gsc_problem_export_abstraction": (ctypes.c_int, [_P, _P, _P, _P]),
     "gsc_problem_timings": (ctypes.c_int, [_P, ctypes.POINTER(Timings)]),
     "gsc_problem_phase_timings": (ctypes.c_int, [_P, ctypes.POINTER(PhaseTimings)]),
+    "gsc_problem_shard_begin": (ctypes.c_int, [_P, ctypes.c_uint32, ctypes.c_uint32]),
+    "gsc_problem_shard_step": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_uint64)]),
+    "gsc_problem_shard_words": (ctypes.c_int, [_P, ctypes.POINTER(_P), ctypes.POINTER(ctypes.c_uint64)]),
+    "gsc_problem_shard_control": (ctypes.c_int, [_P, ctypes.c_uint64, ctypes.c_uint64,
+                                                 ctypes.POINTER(ctypes.c_int)]),
     "gsc_problem_iteration_timings": (ctypes.c_int, [_P, ctypes.c_uint32, _P, _P, _P, _P]),
     "gsc_run_case": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ModelDesc), ctypes.POINTER(QueryDesc),
                                     ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(Result),
@@ -266,6 +271,7 @@ class Context:
 
     def __init__(self, device=0, stream=None):
         self._children = weakref.WeakSet()
+        self.device = int(device)
         self._h = ctypes.c_void_p()
         st = lib().gsc_context_create(int(device), ctypes.c_void_p(stream) if stream else None, ctypes.byref(self._h))
         if st != 0:

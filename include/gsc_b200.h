@@ -334,6 +334,31 @@ int gsc_fixpoint_noalloc(const uint32_t shape[4], uint32_t inputs, int32_t wrap_
                          const uint8_t* candidate_mask, uint32_t max_iterations, uint8_t* reachable_mask,
                          uint32_t* controller, uint32_t* reach_step, gsc_result* summary, void* cuda_stream);
 
+/* ---- Sharded fixpoint: one problem over several GPUs ----------------------
+ * No counterpart in the reference (which runs on one GPU).  G ranks, one
+ * process per GPU, each hold the whole problem (its own context, abstraction
+ * and problem, created alike) and iterate only their own contiguous range of
+ * (theta, v) slices [slice_begin, slice_end).  States are x-fastest, so a
+ * slice range is one contiguous slab of every state array, and of the
+ * bit-sliced D' words (words_per_slice words per slice).  Per iteration each
+ * rank calls gsc_problem_shard_step (the dilation of D' over the whole grid,
+ * then the satisfaction test, the exists-input reduction and the finalize of
+ * its own slices; counts[] = its newly reachable and newly certified
+ * states), the ranks all-gather their slabs of D' in place
+ * (gsc_problem_shard_words: device memory, slab k at word
+ * slice_begin_k * words_per_slice) and sum their counts, and every rank
+ * applies the stop rules with the sums (gsc_problem_shard_control, the
+ * reference's rules of reachability.hpp:133-144).  Every iteration of a
+ * sharded solve tests every pair (no row-lost skipping).  After the stop,
+ * gsc_problem_read gives the global iteration count, stop message and set
+ * sizes, and the rank's own slab of every state array; the caller gathers
+ * the slabs.  Fused method only; gsc_problem_solve ends the sharding. */
+int gsc_problem_shard_begin(gsc_problem* p, uint32_t slice_begin, uint32_t slice_end);
+int gsc_problem_shard_step(gsc_problem* p, uint64_t counts[2]);
+int gsc_problem_shard_words(const gsc_problem* p, void** dprime_words, uint64_t* words_per_slice);
+/* *stop = 1 once a stop rule has fired (then further steps do nothing). */
+int gsc_problem_shard_control(gsc_problem* p, uint64_t new_reachable, uint64_t new_certified, int* stop);
+
 /* ---- Closed-loop simulation of the controller ----------------------------
  * The consumer of the controller table, plots/postprocess_controller.py:66-224:
  * trajectories of the continuous unicycle under the problem's controller

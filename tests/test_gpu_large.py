@@ -58,6 +58,28 @@ def test_large_workload_spot_checked_per_iteration(ctx):
     absn.close()
 
 
+@pytest.mark.timeout(900)
+def test_large_workload_stored_equals_fused(ctx):
+    """128x128x72x48 x 144 with both methods side by side: the stored
+    method's 65 GB of one-byte boxes (8 B per pair) streamed every iteration,
+    against the fused method's recomputed boxes, bit for bit over the whole
+    75-iteration fixpoint (the fused solve is spot-checked against the oracle
+    above)."""
+    case = C.large_case()
+    absn = G.Abstraction(ctx, case)
+    out = {}
+    for method in (G.METHOD_FUSED, G.METHOD_STORED):
+        p = G.Problem(ctx, absn, case, method)
+        p.solve(graph=True)
+        out[method] = p.read()
+        assert p.timings()["method"] == method
+        p.close()
+        ctx.trim()
+    assert_same_result(out[G.METHOD_STORED], out[G.METHOD_FUSED], "128x128x72x48 stored vs fused")
+    assert out[G.METHOD_STORED]["iterations"] == out[G.METHOD_FUSED]["iterations"] == 75
+    absn.close()
+
+
 def test_widest_fused_rows(ctx):
     """256 x-cells: eight 32-bit words per row, the fused method's limit."""
     case = C.unicycle_grid_case((256, 16, 8, 6), (3, 3), "wide_256", max_iterations=64)
@@ -97,13 +119,17 @@ def test_wide_grids_take_the_stored_method_with_16_bit_bounds(ctx, shape, demo):
         case = C.unicycle_grid_case(shape, (3, 3), "wide_%dx%dx%dx%d" % shape, max_iterations=64)
     want = O.solve(case)
     absn = G.Abstraction(ctx, case)
-    for graph in (True, False):
-        p = G.Problem(ctx, absn, case, G.METHOD_AUTO)
+    # The automatic choice: stored beyond the fused rows' 256 x-cells, else
+    # fused (whose y, theta and v tables are 16-bit); then the stored method
+    # with 16-bit bounds explicitly, from one CUDA graph and from the host loop.
+    auto = G.METHOD_STORED if shape[0] > 256 else G.METHOD_FUSED
+    for method, graph in ((G.METHOD_AUTO, True), (G.METHOD_STORED, True), (G.METHOD_STORED, False)):
+        p = G.Problem(ctx, absn, case, method)
         p.solve(graph=graph)
         got = p.read()
-        assert p.timings()["method"] == G.METHOD_STORED
+        assert p.timings()["method"] == (auto if method == G.METHOD_AUTO else method)
         p.close()
-        assert_same_result(got, want, "x".join(map(str, shape)))
+        assert_same_result(got, want, "x".join(map(str, shape)) + f" method {method} graph {graph}")
         assert got["iterations"] == want["iterations"] and got["message"] == want["message"]
         assert list(got["iter_new_reachable"]) == list(want["iter_new_reachable"])
     if shape[0] > 256:
