@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--workload", choices=sorted(C.PRESETS) + ["batched", "served", "simulate"], default="demo_scale")
     ap.add_argument("--method", choices=["auto", "stored", "fused"], default="auto")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--shard", action="store_true",
+                    help="one problem over all ranks by slice ranges (strong scaling) instead of replicas")
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="skip the reference's CUDA backend on the published demo beside this library's")
     ap.add_argument("--e2e-steps", type=int, default=5)
@@ -771,6 +773,66 @@ def bench_simulate(args):
     ctx.close()
 
 
+def bench_sharded(args, case):
+    """One problem solved by all ranks together (strong scaling): every rank
+    owns a contiguous range of (theta, v) slices, and each iteration
+    all-gathers D' over NCCL and sums two counts (gsc_shard).  One step = one
+    whole sharded fixpoint; its time is the max over ranks of the device-
+    synchronised wall time of the loop (the loop synchronises with the host
+    every iteration)."""
+    import datetime
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    import gsc_b200 as G
+    import gsc_shard
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+    os.environ.setdefault("MASTER_PORT", "29533")
+    dist.init_process_group("nccl", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    ctx = G.Context(local)
+    absn = G.Abstraction(ctx, case)
+    prob = G.Problem(ctx, absn, case, G.METHOD_FUSED)
+    comm = gsc_shard.TorchComm(dist)
+    shape, ishape = G.grid_shape(case)
+    P = int(np.prod(shape)) * ishape[0] * ishape[1]
+    times, res = [], None
+    for k in range(args.warmup + args.steps):
+        dist.barrier()
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        res = gsc_shard.ShardedFixpoint(gsc_shard.DeviceEngine(prob), comm).run()
+        torch.cuda.synchronize(dev)
+        if k >= args.warmup:
+            times.append((time.perf_counter() - t0) * 1e3)
+    ms = max_over_ranks(dist, [statistics.mean(times)], dev)[0]
+    one = None
+    if rank == 0:
+        prob.solve(graph=True)
+        one = prob.read()
+        same = all(np.array_equal(res[k], one[k]) for k in ("reachable_mask", "controller", "reach_step"))
+        line = {
+            "metric": "fixpoint pair-checks/s", "value": P * res["iterations"] / (ms * 1e-3), "unit": "pair-checks/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": "u32 bit-sliced sets / int32 counts (f64 boxes)", "data": "synthetic",
+            "config": {"workload": case["name"], "pairs": P, "iterations": res["iterations"],
+                       "parallelism": f"slice shards x{world}, NCCL all-gather of D' per iteration",
+                       "same_as_one_gpu_solve": bool(same)},
+        }
+        print(json.dumps(line))
+    prob.close()
+    absn.close()
+    ctx.close()
+    dist.destroy_process_group()
+
+
 def main():
     args = parse()
     if args.workload in ("batched", "served", "simulate") and args.impl != "reference":
@@ -783,6 +845,9 @@ def main():
     case = C.checked(C.PRESETS[args.workload]())
     if args.impl == "reference":
         run_reference_arm(args, case)
+        return
+    if args.shard:
+        bench_sharded(args, case)
         return
 
     import numpy as np

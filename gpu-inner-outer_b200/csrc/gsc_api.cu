@@ -753,7 +753,10 @@ int problem_stage2(gsc_problem* p) {
     GSC_TRY(palloc(p, &p->candb, words));
     GSC_TRY(palloc(p, &p->dp, words));
     GSC_TRY(palloc(p, &p->reach0, words));
-    GSC_TRY(palloc(p, &p->reach1, words));
+    // One reachable set, updated in place by the finalize: no iteration reads
+    // another's reachable words (the satisfaction test reads D' only), so
+    // reach1 names the same buffer and every parity choice picks it.
+    p->reach1 = p->reach0;
     GSC_TRY(palloc(p, &p->active, words));
     GSC_TRY(palloc(p, &p->hit, words));
     GSC_TRY(palloc(p, &p->best, g.S));
@@ -761,6 +764,8 @@ int problem_stage2(gsc_problem* p) {
     GSC_TRY(palloc(p, &p->dzw, combos * words + 4));
     p->rl_words = static_cast<uint32_t>(g.rows / 32 + 2);
     GSC_TRY(palloc(p, &p->rowlost, 2ull * p->rl_words));
+    GSC_TRY(palloc(p, &p->hitrows, p->rl_words));
+    GSC_CU(ctx, cudaMemsetAsync(p->hitrows, 0, static_cast<size_t>(p->rl_words) * sizeof(uint32_t), st));
     GSC_TRY(palloc(p, &p->offz, static_cast<uint64_t>(g.n[2]) * g.mw));
     GSC_TRY(palloc(p, &p->offv, static_cast<uint64_t>(g.n[3]) * g.ma));
     GSC_CU(ctx, launch_sat_offsets(g, p->zt, p->wt, p->kidx, p->lidx, p->dil.nl, p->offz, p->offv, st));
@@ -838,6 +843,7 @@ FusedFixArgs fused_args(const gsc_problem* p, cudaGraphConditionalHandle cond, i
     a.sat_threads = fused_sat_threads(p->g, p->max_reps);
     a.dzw = p->dzw;
     a.rowlost = p->rowlost;
+    a.hitrows = p->hitrows;
     a.shard_begin = p->shard_begin;
     a.shard_slices = p->shard_slices;
     a.rl_words = p->rl_words;
@@ -1291,7 +1297,8 @@ int gsc_problem_phase_timings(const gsc_problem* p, gsc_phase_timings* out) {
     uint64_t prefix = 0;
     for (const void* q : {static_cast<const void*>(p->pd), static_cast<const void*>(p->pvalid),
                           static_cast<const void*>(p->dzw), static_cast<const void*>(p->vzw),
-                          static_cast<const void*>(p->dp), static_cast<const void*>(p->rowlost)})
+                          static_cast<const void*>(p->dp), static_cast<const void*>(p->rowlost),
+                          static_cast<const void*>(p->hitrows)})
         prefix += alloc_bytes(p, q);
     out->abstraction_bytes = p->abs->bytes + boxes;
     out->prefix_bytes = prefix;

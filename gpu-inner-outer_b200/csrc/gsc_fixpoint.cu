@@ -116,18 +116,36 @@ __global__ void __launch_bounds__(128) k_prefix_xy(GridInfo g, int mode, const u
     const uint32_t n0 = g.n[0], n1 = g.n[1];
     const uint32_t slice = blockIdx.x;   // theta + n2 * v
     const uint32_t z = slice % g.n[2], w = slice / g.n[2];
-    const uint64_t src = static_cast<uint64_t>(slice) * n0 * n1;
+    const uint32_t cells = n0 * n1;
+    const uint64_t src = static_cast<uint64_t>(slice) * cells;
+    // The slice's set (one byte per state, contiguous) into shared memory,
+    // eight loads in flight per thread.
+    constexpr int kU = 8;
+    for (uint32_t i0 = threadIdx.x; i0 < cells; i0 += kU * blockDim.x) {
+        int32_t v[kU];
+#pragma unroll
+        for (int k = 0; k < kU; ++k) {
+            const uint32_t i = i0 + k * blockDim.x;
+            v[k] = 0;
+            if (i < cells) {
+                const uint64_t s = src + i;
+                v[k] = (mode == 0) ? (a[s] != 0) : (mode == 1) ? (a[s] != 0 && b[s] == 0) : (a[s] == 0);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < kU; ++k) {
+            const uint32_t i = i0 + k * blockDim.x;
+            if (i < cells) sxy[i] = v[k];
+        }
+    }
+    __syncthreads();
+    // Rows along x: one warp per row, warp-shuffle scans with a carry.
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     for (uint32_t y = warp; y < n1; y += nwarps) {
-        const uint64_t row = src + static_cast<uint64_t>(y) * n0;
         int32_t carry = 0;
         for (uint32_t x0 = 0; x0 < n0; x0 += 32) {
             const uint32_t x = x0 + lane;
-            int32_t v = 0;
-            if (x < n0) {
-                const uint64_t s = row + x;
-                v = (mode == 0) ? (a[s] != 0) : (mode == 1) ? (a[s] != 0 && b[s] == 0) : (a[s] == 0);
-            }
+            int32_t v = (x < n0) ? sxy[y * n0 + x] : 0;
 #pragma unroll
             for (int off = 1; off < 32; off <<= 1) {
                 const int32_t t = __shfl_up_sync(0xFFFFFFFFu, v, off);
@@ -139,6 +157,7 @@ __global__ void __launch_bounds__(128) k_prefix_xy(GridInfo g, int mode, const u
         }
     }
     __syncthreads();
+    // Columns along y: one thread per x, writing the table rows.
     const uint64_t base = static_cast<uint64_t>(z + 1) * g.ps[2] + static_cast<uint64_t>(w + 1) * g.ps[3] + 1;
     for (uint32_t x = threadIdx.x; x < n0; x += blockDim.x) {
         int32_t acc = 0;
@@ -166,13 +185,26 @@ __global__ void __launch_bounds__(256) k_prefix_zw(GridInfo g, uint32_t lt, int3
     const uint32_t x0 = (blockIdx.x - y * tiles) << lt;
     const uint32_t nx = min(tw, n0 - x0);
     const uint64_t base = static_cast<uint64_t>(y + 1) * g.ps[1] + x0 + 1;
-    const uint32_t lines = n2 * n3;
-    for (uint32_t i = threadIdx.x; i < (lines << lt); i += blockDim.x) {
-        const uint32_t tx = i & (tw - 1);
-        const uint32_t zw = i >> lt;
-        const uint32_t w = zw / n2, z = zw - w * n2;
-        szw[i] = (tx < nx) ? T[base + tx + static_cast<uint64_t>(z + 1) * g.ps[2] + static_cast<uint64_t>(w + 1) * g.ps[3]]
-                           : 0;
+    const uint32_t cells = (n2 * n3) << lt;
+    // The tile into shared memory, eight loads in flight per thread.
+    constexpr int kU = 8;
+    for (uint32_t i0 = threadIdx.x; i0 < cells; i0 += kU * blockDim.x) {
+        int32_t v[kU];
+#pragma unroll
+        for (int k = 0; k < kU; ++k) {
+            const uint32_t i = i0 + k * blockDim.x;
+            const uint32_t tx = i & (tw - 1);
+            const uint32_t zw = i >> lt;
+            const uint32_t w = zw / n2, z = zw - w * n2;
+            v[k] = (i < cells && tx < nx)
+                       ? T[base + tx + static_cast<uint64_t>(z + 1) * g.ps[2] + static_cast<uint64_t>(w + 1) * g.ps[3]]
+                       : 0;
+        }
+#pragma unroll
+        for (int k = 0; k < kU; ++k) {
+            const uint32_t i = i0 + k * blockDim.x;
+            if (i < cells) szw[i] = v[k];
+        }
     }
     __syncthreads();
     for (uint32_t l = threadIdx.x; l < (n3 << lt); l += blockDim.x) {

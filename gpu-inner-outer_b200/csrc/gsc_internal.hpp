@@ -134,6 +134,7 @@ struct gsc_problem {
     uint32_t max_reps = 0;
     gsc_b200::bword *dzw = nullptr, *vzw = nullptr;
     uint32_t* rowlost = nullptr;
+    uint32_t* hitrows = nullptr;
     // sharded solve (gsc_problem_shard_*): this rank's slices and iterations done
     uint32_t shard_begin = 0, shard_slices = 0, shard_iter = 0;
     bool shard_stopped = false;
