@@ -764,8 +764,6 @@ int problem_stage2(gsc_problem* p) {
     GSC_TRY(palloc(p, &p->dzw, combos * words + 4));
     p->rl_words = static_cast<uint32_t>(g.rows / 32 + 2);
     GSC_TRY(palloc(p, &p->rowlost, 2ull * p->rl_words));
-    GSC_TRY(palloc(p, &p->hitrows, p->rl_words));
-    GSC_CU(ctx, cudaMemsetAsync(p->hitrows, 0, static_cast<size_t>(p->rl_words) * sizeof(uint32_t), st));
     GSC_TRY(palloc(p, &p->offz, static_cast<uint64_t>(g.n[2]) * g.mw));
     GSC_TRY(palloc(p, &p->offv, static_cast<uint64_t>(g.n[3]) * g.ma));
     GSC_CU(ctx, launch_sat_offsets(g, p->zt, p->wt, p->kidx, p->lidx, p->dil.nl, p->offz, p->offv, st));
@@ -843,7 +841,6 @@ FusedFixArgs fused_args(const gsc_problem* p, cudaGraphConditionalHandle cond, i
     a.sat_threads = fused_sat_threads(p->g, p->max_reps);
     a.dzw = p->dzw;
     a.rowlost = p->rowlost;
-    a.hitrows = p->hitrows;
     a.shard_begin = p->shard_begin;
     a.shard_slices = p->shard_slices;
     a.rl_words = p->rl_words;
@@ -955,7 +952,6 @@ int gsc_problem_create(gsc_context* ctx, const gsc_abstraction* abs, const gsc_q
     p->timings.abstraction_ms = abs->build_ms;
     if (cudaEventElapsedTime(&ms, pev[0], pev[1]) == cudaSuccess) p->h2d_ms = ms;
     cudaGetLastError();
-    p->peak_used = device_used_bytes();
     p->timings.device_bytes = p->bytes;
     p->timings.method = p->method;
     if (p->method == GSC_METHOD_FUSED) {
@@ -1068,7 +1064,6 @@ int gsc_problem_solve(gsc_problem* p, uint32_t flags) {
     if (flags & GSC_SOLVE_GRAPH && !(flags & GSC_SOLVE_PROFILE))
         launches = 2 + per_iter * std::max<uint32_t>(hfc.iter, 1);   // init child graph + loop bodies
     p->timings.kernel_launches = launches;
-    p->peak_used = std::max(p->peak_used, device_used_bytes());
     if (flags & GSC_SOLVE_PROFILE) {
         p->timings.sat_kernel_ms = sat_ms;
         p->timings.scan_kernel_ms = scan_ms;
@@ -1297,14 +1292,15 @@ int gsc_problem_phase_timings(const gsc_problem* p, gsc_phase_timings* out) {
     uint64_t prefix = 0;
     for (const void* q : {static_cast<const void*>(p->pd), static_cast<const void*>(p->pvalid),
                           static_cast<const void*>(p->dzw), static_cast<const void*>(p->vzw),
-                          static_cast<const void*>(p->dp), static_cast<const void*>(p->rowlost),
-                          static_cast<const void*>(p->hitrows)})
+                          static_cast<const void*>(p->dp), static_cast<const void*>(p->rowlost)})
         prefix += alloc_bytes(p, q);
     out->abstraction_bytes = p->abs->bytes + boxes;
     out->prefix_bytes = prefix;
     out->iteration_bytes = p->bytes - boxes - prefix;
     out->total_allocated_bytes = p->abs->bytes + p->bytes;
-    out->peak_usage_bytes = p->peak_used;
+    // Sampled here, on demand, rather than on the create / solve path: the
+    // query of the driver costs more than a small problem's whole solve.
+    out->peak_usage_bytes = std::max(p->peak_used, device_used_bytes());
     out->result_bytes = 11 * p->g.S + 16ull * t.iterations;
     out->profiled_iterations = static_cast<uint32_t>(p->iter_prof.size());
     return GSC_OK;

@@ -122,20 +122,20 @@ __global__ void __launch_bounds__(128) k_prefix_xy(GridInfo g, int mode, const u
     // eight loads in flight per thread.
     constexpr int kU = 8;
     for (uint32_t i0 = threadIdx.x; i0 < cells; i0 += kU * blockDim.x) {
-        int32_t v[kU];
+        // Both masks' bytes are loaded before either is tested, so no load
+        // waits on another.
+        uint32_t av[kU], bv[kU];
 #pragma unroll
         for (int k = 0; k < kU; ++k) {
             const uint32_t i = i0 + k * blockDim.x;
-            v[k] = 0;
-            if (i < cells) {
-                const uint64_t s = src + i;
-                v[k] = (mode == 0) ? (a[s] != 0) : (mode == 1) ? (a[s] != 0 && b[s] == 0) : (a[s] == 0);
-            }
+            av[k] = (i < cells) ? a[src + i] : 0u;
+            bv[k] = (mode == 1 && i < cells) ? b[src + i] : 0u;
         }
 #pragma unroll
         for (int k = 0; k < kU; ++k) {
             const uint32_t i = i0 + k * blockDim.x;
-            if (i < cells) sxy[i] = v[k];
+            const int32_t v = (mode == 0) ? (av[k] != 0) : (mode == 1) ? ((av[k] != 0) & (bv[k] == 0)) : (av[k] == 0);
+            if (i < cells) sxy[i] = v;
         }
     }
     __syncthreads();

@@ -44,54 +44,25 @@ __global__ void k_fused_init(GridInfo g, FusedFixArgs a, const uint8_t* __restri
     for (uint64_t s = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; s < g.S;
          s += static_cast<uint64_t>(gridDim.x) * blockDim.x)
         init_state(a, cand, s);
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < a.rl_words; k += gridDim.x * blockDim.x)
-        a.hitrows[k] = 0;
 }
 
-// (theta, v)-dilated copies of a bit-sliced set.  Before the first iteration
-// (or without row-lost records) every word position is computed, one thread
-// each.  After it, only positions whose widest window holds a row that lost
-// a D' cell can change: when the last iteration added few states (the
-// incremental test of sat_col_task) and the widest window is at most 4
-// (theta, v) cells, one thread per row checks whether its row lost a cell
-// and, if so, recomputes every position whose window holds it
-// (neighbouring lost rows may recompute a position twice, writing the same
-// words); otherwise one thread per position tests its window
-// (dilate_position).  The kernel also clears the row bits the next finalize
-// writes and the rows the satisfaction kernel will mark.
+// (theta, v)-dilated copies of a bit-sliced set, one thread per word
+// position (dilate_position): after the first iteration, with the row-lost
+// records, only positions whose widest window holds a row that lost a D'
+// cell are recomputed.  The kernel also clears the row bits the next
+// finalize writes.
 __global__ void k_dilate(GridInfo g, const bword* __restrict__ src, bword* __restrict__ dst, DilateArgs d,
-                         const FixControl* fc, uint32_t* rowlost, uint32_t rl_words, uint32_t* hitrows) {
+                         const FixControl* fc, uint32_t* rowlost, uint32_t rl_words) {
     pdl_wait();
     if (fc && fc->stop) return;
     const uint32_t c = fc ? fc->iter : 0;
     const uint32_t* lost = (rowlost && c > 0) ? rowlost + (c & 1) * rl_words : nullptr;
     uint32_t* next = rowlost ? rowlost + ((c + 1) & 1) * rl_words : nullptr;
-    const uint32_t W = g.W;
-    const uint32_t pos = static_cast<uint32_t>(g.rows * W);
-    const uint32_t span = (next || hitrows) ? max(pos, rl_words) : pos;
-    // By row only for small windows: a lost row's thread recomputes
-    // kmax * lmax * W positions of kmax * lmax loads each.
-    const bool by_row = lost && fc && d.kval[d.nk - 1] * d.lval[d.nl - 1] <= 4 &&
-                        static_cast<unsigned long long>(fc->last_new) * kIncrementalRows <= g.rows;
+    const uint32_t pos = static_cast<uint32_t>(g.rows * g.W);
+    const uint32_t span = next ? max(pos, rl_words) : pos;
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < span; p += gridDim.x * blockDim.x) {
         if (next && p < rl_words) next[p] = 0;
-        if (hitrows && p < rl_words) hitrows[p] = 0;
-        if (!by_row) {
-            if (p < pos) dilate_position(g, src, dst, d, p, lost);
-            continue;
-        }
-        if (p >= g.rows || !((lost[p >> 5] >> (p & 31)) & 1u)) continue;
-        const uint32_t n1 = g.n[1], n2 = g.n[2];
-        const uint32_t y = p % n1, q = p / n1;
-        const uint32_t z = q % n2, v = q / n2;
-        const uint32_t kmax = d.kval[d.nk - 1], lmax = d.lval[d.nl - 1];
-        for (uint32_t i = 0; i < kmax; ++i) {
-            const uint32_t z0 = (z >= i) ? z - i : z + n2 - i;   // windows z0 .. z0 + kmax - 1 hold z
-            for (uint32_t j = 0; j < lmax && j <= v; ++j) {
-                const uint32_t r0 = y + n1 * (z0 + n2 * (v - j));
-                for (uint32_t w = 0; w < W; ++w) dilate_position(g, src, dst, d, r0 * W + w, nullptr);
-            }
-        }
+        if (p < pos) dilate_position(g, src, dst, d, p, lost);
     }
 }
 
@@ -217,11 +188,9 @@ __global__ void __launch_bounds__(kFusedWarps * 32) k_sat_col(GridInfo g, FusedF
 
 // Apply the iteration's hits, build next iteration's D', count, and let the
 // last block to finish apply the stop rules (reachability.hpp:133-144).  One
-// thread per x-row: only rows that the satisfaction kernel marked in hitrows
-// hold a hit, and a row without one keeps its reachable, active and D' words
-// (the reachable set is updated in place).  A sharded solve finalizes the
-// shard's rows only and leaves the stop rules to the host, which applies
-// them with every rank's counts.
+// thread per word; the reachable set is updated in place.  A sharded solve
+// finalizes the shard's words only and leaves the stop rules to the host,
+// which applies them with every rank's counts.
 __global__ void __launch_bounds__(256) k_fused_finalize(GridInfo g, FusedFixArgs a) {
     pdl_wait();
     FixControl* fc = a.fc;
@@ -231,14 +200,13 @@ __global__ void __launch_bounds__(256) k_fused_finalize(GridInfo g, FusedFixArgs
         return;
     }
     const uint32_t it = fc->iter + 1;
-    const uint64_t first = static_cast<uint64_t>(a.shard_begin) * g.n[1];
-    const uint64_t rows = a.shard_slices ? static_cast<uint64_t>(a.shard_slices) * g.n[1] : g.rows;
+    const uint64_t nw = static_cast<uint64_t>(g.n[1]) * g.W;
+    const uint64_t first = static_cast<uint64_t>(a.shard_begin) * nw;
+    const uint64_t words = a.shard_slices ? a.shard_slices * nw : g.rows * g.W;
     unsigned long long nr = 0, nc = 0;
-    for (uint64_t k = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; k < rows;
+    for (uint64_t k = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; k < words;
          k += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        const uint64_t r = first + k;
-        if (!((a.hitrows[r >> 5] >> (r & 31)) & 1u)) continue;
-        for (uint32_t w = 0; w < g.W; ++w) finalize_word(g, a, a.reach0, a.reach0, r * g.W + w, it, nr, nc);
+        finalize_word(g, a, a.reach0, a.reach0, first + k, it, nr, nc);
     }
     unsigned long long* row = a.stats + kStatsCols * it;
     add_counters(row, nr, nc);
@@ -316,12 +284,12 @@ cudaError_t launch_plan(const GridInfo& g, const uint32_t* zt, const uint32_t* w
 }
 
 cudaError_t launch_dilate(const GridInfo& g, const bword* src, bword* dst, const DilateArgs& d, const FixControl* fc,
-                          uint32_t* rowlost, uint32_t rl_words, cudaStream_t st, uint32_t* hitrows) {
+                          uint32_t* rowlost, uint32_t rl_words, cudaStream_t st) {
     const uint64_t pos = g.rows * g.W;
     uint64_t b = (pos + 255) / 256;
     if (b > 8192) b = 8192;
     return launch_pdl(k_dilate, dim3(static_cast<unsigned int>(b ? b : 1)), dim3(256), 0, st, g, src, dst, d, fc,
-                      rowlost, rl_words, hitrows);
+                      rowlost, rl_words);
 }
 
 cudaError_t launch_sat_offsets(const GridInfo& g, const uint32_t* zt, const uint32_t* wt, const uint8_t* kidx,
@@ -351,8 +319,7 @@ cudaError_t launch_fused_iteration(const GridInfo& g, const FusedFixArgs& a, cud
     if (ev) cudaEventRecord(ev[0], st);
     // A sharded solve dilates the whole grid every iteration: the other
     // ranks' D' slabs arrive without row-lost records.
-    cudaError_t derr = launch_dilate(g, a.dp, a.dzw, a.dil, a.fc, a.shard_slices ? nullptr : a.rowlost, a.rl_words, st,
-                                     a.hitrows);
+    cudaError_t derr = launch_dilate(g, a.dp, a.dzw, a.dil, a.fc, a.shard_slices ? nullptr : a.rowlost, a.rl_words, st);
     if (derr != cudaSuccess) return derr;
     if (ev)
         for (int k = 1; k <= 4; ++k) cudaEventRecord(ev[k], st);
@@ -377,8 +344,8 @@ cudaError_t launch_fused_iteration(const GridInfo& g, const FusedFixArgs& a, cud
 #undef GSC_SAT_CASE
     if (err != cudaSuccess) return err;
     if (ev) cudaEventRecord(ev[5], st);
-    const uint64_t rows = a.shard_slices ? static_cast<uint64_t>(a.shard_slices) * g.n[1] : g.rows;
-    uint64_t fb = (rows + 255) / 256;
+    const uint64_t words = a.shard_slices ? static_cast<uint64_t>(a.shard_slices) * g.n[1] * g.W : g.rows * g.W;
+    uint64_t fb = (words + 255) / 256;
     if (fb > 4096) fb = 4096;
     if (launches) *launches += 3;
     err = launch_pdl(k_fused_finalize, dim3(static_cast<unsigned int>(fb ? fb : 1)), dim3(256), 0, st, g, a);

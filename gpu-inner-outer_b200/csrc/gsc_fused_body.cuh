@@ -484,13 +484,7 @@ __device__ __forceinline__ void sat_col_task(const GridInfo& g, const FusedFixAr
                 atomicMin(a.best + srow + b, j);
             }
         }
-        if (got) {
-            atomicOr(a.hit + wbase + e, got);
-            if (a.hitrows) {
-                const uint32_t row = slice * n1 + y;
-                atomicOr(a.hitrows + (row >> 5), 1u << (row & 31));
-            }
-        }
+        if (got) atomicOr(a.hit + wbase + e, got);
     }
     for (int off = 16; off > 0; off >>= 1) ntest += __shfl_down_sync(0xFFFFFFFFu, ntest, off);
     if ((tid & 31) == 0 && ntest) atomicAdd(a.stats + kStatsCols * (it + 1) + 2, ntest);

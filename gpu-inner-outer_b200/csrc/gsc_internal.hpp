@@ -134,7 +134,6 @@ struct gsc_problem {
     uint32_t max_reps = 0;
     gsc_b200::bword *dzw = nullptr, *vzw = nullptr;
     uint32_t* rowlost = nullptr;
-    uint32_t* hitrows = nullptr;
     // sharded solve (gsc_problem_shard_*): this rank's slices and iterations done
     uint32_t shard_begin = 0, shard_slices = 0, shard_iter = 0;
     bool shard_stopped = false;
@@ -166,7 +165,7 @@ struct gsc_problem {
     double pass_ms[4] = {0, 0, 0, 0};
     double prof_sat_ms = 0.0, prof_reduce_ms = 0.0, prof_memcpy_ms = 0.0;
     std::vector<std::array<float, 4>> iter_prof;
-    uint64_t peak_used = 0;      // device memory in use on the GPU, highest sample
+    uint64_t peak_used = 0;      // device memory in use on the GPU when last sampled
     ~gsc_problem();
 };
 

@@ -184,8 +184,6 @@ struct FusedFixArgs {
     uint32_t* rowlost;         // [2][rl_words] bit per x-row: the row lost a D' cell in the iteration
                                // (iter & 1) just finalised
     uint32_t rl_words;         // rows / 32 + 2
-    uint32_t* hitrows;         // [rl_words] bit per x-row: a state of the row was satisfied this iteration
-                               // (set by the satisfaction kernel, cleared by the next dilation)
     const bword* vzw;          // (theta, v)-dilated valid set (when validity is more than safety)
     const uint8_t* kidx;       // [n2 + 1]: theta width -> its slot in dil.kval
     const uint8_t* lidx;       // [n3 + 1]: v width -> its slot in dil.lval
@@ -250,7 +248,7 @@ uint32_t fused_sat_threads(const GridInfo& g, uint32_t max_reps);
 // lost a D' cell are recomputed; it also clears the row bits the next
 // finalize writes.
 cudaError_t launch_dilate(const GridInfo& g, const bword* src, bword* dst, const DilateArgs& d, const FixControl* fc,
-                          uint32_t* rowlost, uint32_t rl_words, cudaStream_t st, uint32_t* hitrows = nullptr);
+                          uint32_t* rowlost, uint32_t rl_words, cudaStream_t st);
 // Fills a PlanRecord from the counts, flags and (when xrep is set) the
 // theta / v tables and plane representatives; writes kidx / lidx.
 cudaError_t launch_plan(const GridInfo& g, const uint32_t* zt, const uint32_t* wt, const uint8_t* xrep,

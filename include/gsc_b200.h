@@ -273,7 +273,7 @@ typedef struct {
     double total_compute_ms;          /* kernel + memcpy (kernels.cu:850-851)                          */
     uint64_t total_allocated_bytes;   /* device memory of the abstraction and the problem              */
     uint64_t peak_usage_bytes;        /* device memory in use on the GPU (cudaMemGetInfo), highest
-                                         sample after creation and after each solve                    */
+                                         sample taken by this call on the problem                      */
     uint64_t abstraction_bytes;       /* abstraction tables + the problem's boxes, classes, safe tables */
     uint64_t prefix_bytes;            /* stored: prefix tables; fused: D' and its dilated copies       */
     uint64_t iteration_bytes;         /* masks, sets, controller, reach_step, counters, control        */
