@@ -106,9 +106,9 @@ __global__ void k_prefix_axis(GridInfo g, int dim, int32_t* __restrict__ T, cons
 // warp shuffles into shared memory; then one thread per x column scans along
 // y and writes the slice's table rows (coalesced along x).
 constexpr uint32_t kPrefixXYSmemMax = 96u << 10;
-constexpr uint32_t kPrefixZWSmemMax = 64u << 10;
+constexpr uint32_t kPrefixZWSmemMax = 32u << 10;
 
-__global__ void __launch_bounds__(128) k_prefix_xy(GridInfo g, int mode, const uint8_t* __restrict__ a,
+__global__ void __launch_bounds__(256) k_prefix_xy(GridInfo g, int mode, const uint8_t* __restrict__ a,
                                                    const uint8_t* __restrict__ b, int32_t* __restrict__ T,
                                                    const FixControl* fc) {
     if (fc && fc->stop) return;
@@ -493,7 +493,7 @@ cudaError_t launch_prefix4(const GridInfo& g, int mode, const uint8_t* a, const 
         }
         uint32_t lt = 5;
         while (lt > 0 && (zw_line << lt) > kPrefixZWSmemMax) --lt;
-        k_prefix_xy<<<g.slices, 128, static_cast<size_t>(xy_bytes), st>>>(g, mode, a, b, table, ctl);
+        k_prefix_xy<<<g.slices, 256, static_cast<size_t>(xy_bytes), st>>>(g, mode, a, b, table, ctl);
         if (ev) cudaEventRecord(ev[0], st);
         const uint32_t tiles = (g.n[0] + (1u << lt) - 1) >> lt;
         k_prefix_zw<<<tiles * g.n[1], 256, static_cast<size_t>(zw_line << lt), st>>>(g, lt, table, ctl);

@@ -266,7 +266,7 @@ cudaError_t launch_sat_col_t(const GridInfo& g, const FusedFixArgs& a, size_t sm
 
 uint32_t fused_sat_threads(const GridInfo& g, uint32_t max_reps) {
     const uint64_t work = static_cast<uint64_t>(max_reps) * g.n[1] * g.W;
-    return work <= 1024 ? 64u : work <= 2304 ? 128u : 256u;
+    return work <= 2304 ? 128u : 256u;
 }
 
 size_t fused_smem_bytes(const GridInfo& g, uint32_t cls_words, int need_valid, uint32_t max_reps, bool bulk) {
