@@ -492,15 +492,16 @@ __device__ __forceinline__ void sat_col_task(const GridInfo& g, const FusedFixAr
 
 // Apply the iteration's hits to word e and build next iteration's D';
 // nr / nc collect newly reachable states and newly certified candidates.
-// L2: read hit and best[] from L2 (inside the satisfaction kernel, where
-// other blocks of the same launch wrote them with atomics and this SM's L1
-// may hold an older copy of their lines).
-template <bool L2 = false>
+// The reachable set is updated in place (rprev and rnext name one buffer),
+// and D' = (valid & ~reachable) | unsafe holds for every word between
+// iterations, so a word without a hit keeps all of its bits: its thread
+// reads the hit word and stops.
 __device__ __forceinline__ void finalize_word(const GridInfo& g, const FusedFixArgs& a, const bword* rprev,
                                               bword* rnext, uint64_t e, uint32_t it, unsigned long long& nr,
                                               unsigned long long& nc) {
+    const bword h = a.hit[e];
+    if (!h) return;
     const bword rp = rprev[e];
-    const bword h = L2 ? __ldcg(a.hit + e) : a.hit[e];
     const bword rn = rp | h;
     rnext[e] = rn;
     const bword dn = (a.validb[e] & ~rn) | a.unsafeb[e];
@@ -509,34 +510,31 @@ __device__ __forceinline__ void finalize_word(const GridInfo& g, const FusedFixA
         atomicOr(a.rowlost + (it & 1) * a.rl_words + (r >> 5), 1u << (r & 31));
     }
     a.dp[e] = dn;
-    if (h) {
-        a.hit[e] = 0;
-        a.active[e] &= ~h;
-        const bword c = a.candb[e];
-        nr += __popc(h & ~rp);
-        nc += __popc(h & c);
-        const uint64_t r = e / g.W;
-        const uint64_t sbase = r * g.n[0] + (e - r * g.W) * kBits;
-        bword m = h;
-        while (m) {
-            // Four states at a time: their best[] loads in flight together.
-            uint32_t b[4], j[4];
+    a.hit[e] = 0;
+    a.active[e] &= ~h;
+    const bword c = a.candb[e];
+    nr += __popc(h & ~rp);
+    nc += __popc(h & c);
+    const uint64_t r = e / g.W;
+    const uint64_t sbase = r * g.n[0] + (e - r * g.W) * kBits;
+    bword m = h;
+    while (m) {
+        // Four states at a time: their best[] loads in flight together.
+        uint32_t b[4], j[4];
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                b[k] = m ? static_cast<uint32_t>(__ffs(m) - 1) : kBits;
-                m &= m - 1;
-            }
+        for (int k = 0; k < 4; ++k) {
+            b[k] = m ? static_cast<uint32_t>(__ffs(m) - 1) : kBits;
+            m &= m - 1;
+        }
 #pragma unroll
-            for (int k = 0; k < 4; ++k)
-                j[k] = b[k] < kBits ? (L2 ? __ldcg(a.best + sbase + b[k]) : a.best[sbase + b[k]]) : kInvalid32;
+        for (int k = 0; k < 4; ++k) j[k] = b[k] < kBits ? a.best[sbase + b[k]] : kInvalid32;
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                if (b[k] >= kBits) continue;
-                const uint64_t s = sbase + b[k];
-                a.controller[s] = j[k];
-                a.best[s] = kInvalid32;
-                if (!((c >> b[k]) & 1u)) a.reach_step[s] = it;
-            }
+        for (int k = 0; k < 4; ++k) {
+            if (b[k] >= kBits) continue;
+            const uint64_t s = sbase + b[k];
+            a.controller[s] = j[k];
+            a.best[s] = kInvalid32;
+            if (!((c >> b[k]) & 1u)) a.reach_step[s] = it;
         }
     }
 }
