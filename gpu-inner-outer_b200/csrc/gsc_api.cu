@@ -275,6 +275,50 @@ cudaError_t profile_events(gsc_context* ctx, cudaEvent_t** out) {
     return cudaSuccess;
 }
 
+// How long a profiled iteration's launches wait behind launch_hold: more
+// than the host takes to queue an iteration's kernels, events and copy.
+constexpr uint64_t kProfileHoldNs = 60000;
+
+// The pinned control-record slots and events of host-loop solves.
+static cudaError_t loop_resources(gsc_context* ctx) {
+    if (!ctx->loop_fc) {
+        void* h = nullptr;
+        const cudaError_t err = cudaMallocHost(&h, 2 * sizeof(FixControl));
+        if (err != cudaSuccess) return err;
+        ctx->loop_fc = static_cast<FixControl*>(h);
+    }
+    for (auto& e : ctx->loop_ev)
+        if (!e) {
+            const cudaError_t err = cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+            if (err != cudaSuccess) return err;
+        }
+    return cudaSuccess;
+}
+
+// True for page-locked (or registered) host memory.
+static bool is_pinned(const void* ptr) {
+    cudaPointerAttributes at{};
+    if (cudaPointerGetAttributes(&at, ptr) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return at.type == cudaMemoryTypeHost;
+}
+
+// The side stream of overlapped copies and its two ordering events.
+static cudaError_t side_resources(gsc_context* ctx) {
+    if (!ctx->side) {
+        const cudaError_t err = cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking);
+        if (err != cudaSuccess) return err;
+    }
+    for (auto& e : ctx->side_ev)
+        if (!e) {
+            const cudaError_t err = cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+            if (err != cudaSuccess) return err;
+        }
+    return cudaSuccess;
+}
+
 // Device memory in use on the current GPU (all processes), as the reference
 // samples it (kernels.cu:30-42).
 uint64_t device_used_bytes() {
@@ -474,6 +518,15 @@ void gsc_context_destroy(gsc_context* ctx) {
         }
     for (auto e : ctx->setup_ev)
         if (e) cudaEventDestroy(e);
+    for (auto e : ctx->loop_ev)
+        if (e) cudaEventDestroy(e);
+    for (auto e : ctx->side_ev)
+        if (e) cudaEventDestroy(e);
+    if (ctx->side) {
+        cudaStreamSynchronize(ctx->side);
+        cudaStreamDestroy(ctx->side);
+    }
+    if (ctx->loop_fc) cudaFreeHost(ctx->loop_fc);
     ctx->pool.reset();
     pinned_trim(ctx);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -744,6 +797,8 @@ int problem_stage2(gsc_problem* p) {
         GSC_CU(ctx, launch_stored_build(g, sb, st));
         GSC_TRY(palloc(p, &p->pd, g.tsize));
         GSC_CU(ctx, cudaMemsetAsync(p->pd, 0, g.tsize * 4, st));
+        p->rl_words = static_cast<uint32_t>(g.rows / 32 + 2);
+        GSC_TRY(palloc(p, &p->rowlost, 2ull * p->rl_words));
         return GSC_OK;
     }
     const uint64_t words = g.rows * g.W;
@@ -806,6 +861,8 @@ StoredFixArgs stored_args(const gsc_problem* p, cudaGraphConditionalHandle cond,
     a.stats = p->stats;
     a.cond = cond;
     a.use_cond = use_cond;
+    a.rowlost = p->rowlost;
+    a.rl_words = p->rl_words;
     return a;
 }
 
@@ -985,6 +1042,7 @@ int gsc_problem_solve(gsc_problem* p, uint32_t flags) {
         launches += 2;
         cudaEvent_t* ev = nullptr;
         GSC_CU(ctx, profile_events(ctx, &ev));
+        const int npass = p->method == GSC_METHOD_STORED ? static_cast<int>(prefix4_launches(p->g)) : 1;
         for (double& v : p->pass_ms) v = 0.0;
         p->prof_sat_ms = p->prof_reduce_ms = p->prof_memcpy_ms = 0.0;
         p->iter_prof.clear();
@@ -995,13 +1053,20 @@ int gsc_problem_solve(gsc_problem* p, uint32_t flags) {
             // The stop rules fire by iteration stats_cap - 1 at the latest.
             if (++guard > p->stats_cap + 2)
                 return fail(ctx, GSC_ERR_TIMEOUT, "fixpoint did not stop within its iteration bound");
-            err = enqueue_iteration(p, 0, 0, &launches, ev);
+            // The hold lets the host queue the iteration and its events
+            // before any of them runs.
+            err = launch_hold(st, kProfileHoldNs);
+            if (err == cudaSuccess) err = enqueue_iteration(p, 0, 0, &launches, ev);
             if (err == cudaSuccess) err = cudaMemcpyAsync(&hfc, p->fc, sizeof(hfc), cudaMemcpyDeviceToHost, st);
             if (err == cudaSuccess) err = cudaEventRecord(ev[7], st);
             if (err == cudaSuccess) err = cudaStreamSynchronize(st);
+            // Events 1 .. npass follow the prefix passes (or the dilation);
+            // the satisfaction phase is timed from the last of them.
             float d[kProfileEvents - 1] = {};
-            for (int k = 0; err == cudaSuccess && k < kProfileEvents - 1; ++k)
-                err = cudaEventElapsedTime(&d[k], ev[k], ev[k + 1]);
+            for (int k = 0; err == cudaSuccess && k < kProfileEvents - 1; ++k) {
+                if (k >= npass && k < 4) continue;
+                err = cudaEventElapsedTime(&d[k], ev[k == 4 ? npass : k], ev[k + 1]);
+            }
             if (err != cudaSuccess) break;
             float prefix = 0.f;
             for (int k = 0; k < 4; ++k) {
@@ -1022,22 +1087,37 @@ int gsc_problem_solve(gsc_problem* p, uint32_t flags) {
         if (!p->exec) GSC_TRY(build_graph(p));
         GSC_CU(ctx, cudaGraphLaunch(p->exec, st));
     } else {
+        // Chunks of kLoopChunk iterations, two in flight: after enqueueing
+        // chunk k+1 the host waits for chunk k's copy of the control record,
+        // so the device does not idle on the host's check, and at most one
+        // chunk of iterations (kernels that return at once on the stop flag)
+        // runs past the stop.
+        constexpr uint32_t kLoopChunk = 2;
+        GSC_CU(ctx, loop_resources(ctx));
         GSC_CU(ctx, enqueue_init(p));
         launches += 2;
-        uint32_t host_stop = 0, chunk = 4, done = 0;
-        FixControl hfc;
-        while (true) {
-            for (uint32_t i = 0; i < chunk; ++i) GSC_CU(ctx, enqueue_iteration(p, 0, 0, &launches));
-            done += chunk;
-            GSC_CU(ctx, cudaMemcpyAsync(&hfc, p->fc, sizeof(hfc), cudaMemcpyDeviceToHost, st));
-            GSC_CU(ctx, cudaStreamSynchronize(st));
-            host_stop = hfc.stop;
-            if (host_stop) break;
-            if (done > p->stats_cap + 64)
+        uint32_t done = 0;
+        auto enqueue_chunk = [&](uint32_t slot) -> cudaError_t {
+            for (uint32_t i = 0; i < kLoopChunk; ++i) {
+                const cudaError_t e = enqueue_iteration(p, 0, 0, &launches);
+                if (e != cudaSuccess) return e;
+            }
+            done += kLoopChunk;
+            const cudaError_t e =
+                cudaMemcpyAsync(ctx->loop_fc + slot, p->fc, sizeof(FixControl), cudaMemcpyDeviceToHost, st);
+            return e == cudaSuccess ? cudaEventRecord(ctx->loop_ev[slot], st) : e;
+        };
+        GSC_CU(ctx, enqueue_chunk(0));
+        for (uint32_t k = 0;; ++k) {
+            // The slot of chunk k+1 is chunk k-1's, whose record was read.
+            GSC_CU(ctx, enqueue_chunk((k + 1) & 1));
+            GSC_CU(ctx, cudaEventSynchronize(ctx->loop_ev[k & 1]));
+            if (ctx->loop_fc[k & 1].stop) break;
+            if (done > p->stats_cap + 4 * kLoopChunk) {
+                cudaStreamSynchronize(st);
                 return fail(ctx, GSC_ERR_TIMEOUT, "fixpoint did not stop within its iteration bound");
-            if (chunk < 64) chunk *= 2;
+            }
         }
-        (void)done;
     }
     GSC_CU(ctx, cudaEventRecord(ctx->ev[1], st));
     GSC_CU(ctx, cudaEventSynchronize(ctx->ev[1]));
@@ -1345,8 +1425,36 @@ int gsc_run_case(int device, const gsc_model_desc* model, const gsc_query_desc* 
     gsc_problem* p = nullptr;
     int s = gsc_abstraction_create(ctx, model, &abs);
     if (s == GSC_OK) s = gsc_problem_create(ctx, abs, query, method, &p);
+    // The valid and candidate masks are final once the problem is built:
+    // into page-locked host arrays they are copied on the side stream while
+    // the fixpoint runs.  (A copy into pageable memory would hold the host
+    // until it is done, so those are read after the solve as usual.)
+    bool side = false;
+    if (s == GSC_OK && out->valid_mask && out->candidate_mask && is_pinned(out->valid_mask) &&
+        is_pinned(out->candidate_mask)) {
+        cudaError_t e = side_resources(ctx);
+        if (e == cudaSuccess) e = cudaEventRecord(ctx->side_ev[0], ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->side, ctx->side_ev[0], 0);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(out->valid_mask, p->valid, p->g.S, cudaMemcpyDeviceToHost, ctx->side);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(out->candidate_mask, p->cand, p->g.S, cudaMemcpyDeviceToHost, ctx->side);
+        if (e == cudaSuccess) e = cudaEventRecord(ctx->side_ev[1], ctx->side);
+        side = e == cudaSuccess;
+        if (!side) s = fail(ctx, GSC_ERR_CUDA, cudaGetErrorString(e));
+    }
     if (s == GSC_OK) s = gsc_problem_solve(p, flags);
-    if (s == GSC_OK) s = gsc_problem_read(p, out);
+    if (s == GSC_OK) {
+        gsc_result r = *out;
+        if (side) r.valid_mask = r.candidate_mask = nullptr;
+        s = gsc_problem_read(p, &r);
+        r.valid_mask = out->valid_mask;
+        r.candidate_mask = out->candidate_mask;
+        *out = r;
+    }
+    // The side copies read the problem's masks: they end before it is freed.
+    if (side) {
+        const cudaError_t e = cudaStreamSynchronize(ctx->side);
+        if (e != cudaSuccess && s == GSC_OK) s = fail(ctx, GSC_ERR_CUDA, cudaGetErrorString(e));
+    }
     if (s == GSC_OK && timings) gsc_problem_timings(p, timings);
     gsc_problem_destroy(p);
     gsc_abstraction_destroy(abs);

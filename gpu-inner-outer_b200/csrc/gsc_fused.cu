@@ -321,8 +321,7 @@ cudaError_t launch_fused_iteration(const GridInfo& g, const FusedFixArgs& a, cud
     // ranks' D' slabs arrive without row-lost records.
     cudaError_t derr = launch_dilate(g, a.dp, a.dzw, a.dil, a.fc, a.shard_slices ? nullptr : a.rowlost, a.rl_words, st);
     if (derr != cudaSuccess) return derr;
-    if (ev)
-        for (int k = 1; k <= 4; ++k) cudaEventRecord(ev[k], st);
+    if (ev) cudaEventRecord(ev[1], st);
     const size_t sm = fused_smem_bytes(g, a.cls_words, a.need_valid, a.max_reps, true);
     cudaError_t err;
 #define GSC_SAT_CASE(Wn)                                                                         \

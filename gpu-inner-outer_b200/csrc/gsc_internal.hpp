@@ -67,6 +67,15 @@ struct gsc_context {
     // taking a cached block.  Freed by gsc_context_trim and at destruction.
     std::mutex pin_mu;
     std::multimap<size_t, void*> pin_free;
+    // Host-loop solves: two pinned copies of the control record and an event
+    // per copy, so that one chunk of iterations runs while the host reads
+    // the stop flag of the previous one (created at first use).
+    gsc_b200::FixControl* loop_fc = nullptr;
+    cudaEvent_t loop_ev[2] = {nullptr, nullptr};
+    // A second stream for copies that overlap a solve (gsc_run_case), with
+    // the events that order it against `stream` (created at first use).
+    cudaStream_t side = nullptr;
+    cudaEvent_t side_ev[2] = {nullptr, nullptr};
 };
 
 struct gsc_abstraction {

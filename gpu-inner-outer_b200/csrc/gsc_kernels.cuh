@@ -73,8 +73,8 @@ cudaError_t launch_unpack_reach(const GridInfo& g, const FixControl* fc, const b
 // mode 0: valid; 1: valid && !reach (b = reach); 2: !safe (4-D safe mask).
 // Built in two passes (x-y per (theta, v) slice, then theta-v per (x tile,
 // y)) when a slice and a theta-v plane fit shared memory, else one pass per
-// dimension.  ev (optional, 4 events): ev[k] is recorded after pass k + 1; a
-// two-pass build records ev[1..3] after its second pass.
+// dimension.  ev (optional, prefix4_launches(g) events): ev[k] is recorded
+// after pass k + 1.
 cudaError_t launch_prefix4(const GridInfo& g, int mode, const uint8_t* a, const uint8_t* b, int32_t* table,
                            const FixControl* ctl, cudaStream_t st, cudaEvent_t* ev = nullptr);
 // Kernels launch_prefix4 launches for this grid.
@@ -128,14 +128,30 @@ struct StoredFixArgs {
     unsigned long long* stats;   // [stats_cap][kStatsCols]
     cudaGraphConditionalHandle cond;
     int use_cond;
+    // [2][rl_words] bitmaps over the rows (y, theta, v): iteration it marks
+    // in bitmap it & 1 the rows of the states it made reachable.  When the
+    // previous iteration added few states, iteration it tests only the pairs
+    // whose box holds a row marked in bitmap (it - 1) & 1: the others failed
+    // before and their boxes still hold the same D cells.  The control
+    // kernel of iteration it clears bitmap (it + 1) & 1 for the next one.
+    // rl_words includes one word of padding.
+    uint32_t* rowlost;
+    uint32_t rl_words;
 };
 cudaError_t launch_stored_init(const GridInfo& g, const StoredFixArgs& a, cudaStream_t st);
 // ev (optional, kProfileEvents events): [0] before the prefix rebuild,
-// [1..4] after its passes (launch_prefix4), [5] after the satisfaction kernel,
-// [6] after the control kernel.
+// [1..n] after its n passes (launch_prefix4: n = prefix4_launches(g); events
+// n+1 .. 4 are not recorded), [5] after the satisfaction kernel, [6] after
+// the control kernel.  The fused iteration records [0], [1] after the
+// dilation, [5] and [6] alike.
 constexpr int kProfileEvents = 8;
 cudaError_t launch_stored_iteration(const GridInfo& g, const StoredFixArgs& a, cudaStream_t st, uint32_t* launches,
                                     cudaEvent_t* ev = nullptr);
+// One thread that holds the stream for about `ns` nanoseconds (bounded by
+// the global timer and by an iteration cap), so that what the host queues
+// behind it meanwhile runs back to back: profiled phases then time the
+// kernels rather than the host's enqueueing.
+cudaError_t launch_hold(cudaStream_t st, uint64_t ns);
 
 // Box widths present in a problem: theta widths kval[0..nk) and v widths
 // lval[0..nl), ascending; combo (ki, li) indexes the dilated copies.
