@@ -797,8 +797,6 @@ int problem_stage2(gsc_problem* p) {
         GSC_CU(ctx, launch_stored_build(g, sb, st));
         GSC_TRY(palloc(p, &p->pd, g.tsize));
         GSC_CU(ctx, cudaMemsetAsync(p->pd, 0, g.tsize * 4, st));
-        p->rl_words = static_cast<uint32_t>(g.rows / 32 + 2);
-        GSC_TRY(palloc(p, &p->rowlost, 2ull * p->rl_words));
         return GSC_OK;
     }
     const uint64_t words = g.rows * g.W;
@@ -861,8 +859,6 @@ StoredFixArgs stored_args(const gsc_problem* p, cudaGraphConditionalHandle cond,
     a.stats = p->stats;
     a.cond = cond;
     a.use_cond = use_cond;
-    a.rowlost = p->rowlost;
-    a.rl_words = p->rl_words;
     return a;
 }
 

@@ -265,66 +265,14 @@ __device__ __forceinline__ uint32_t dcount16(const int32_t* __restrict__ P, cons
     return q16(P, g, l0, l1, l2, l3, r0, r1, g.n[2], r3) + q16(P, g, l0, l1, 0, l3, r0, r1, h2 + 1, r3);
 }
 
-// Whether the box with y cells [l1, h1], theta cells l2 .. h2 (wrapping
-// when l2 > h2) and v cells [l3, h3] holds a row (y, theta, v) marked in
-// `lost`.  A box more than 32 rows high is reported as holding one.
-__device__ __forceinline__ bool box_rows_lost(const uint32_t* __restrict__ lost, const GridInfo& g, uint32_t l1,
-                                              uint32_t h1, uint32_t l2, uint32_t h2, uint32_t l3, uint32_t h3) {
-    const uint32_t len = h1 - l1 + 1;
-    if (len > 32) return true;
-    const uint32_t n1 = g.n[1], n2 = g.n[2];
-    const uint32_t mask = len == 32 ? 0xFFFFFFFFu : (1u << len) - 1;
-    const uint32_t nz = (l2 <= h2) ? h2 - l2 + 1 : n2 - l2 + h2 + 1;
-    uint32_t z = l2;
-    for (uint32_t i = 0; i < nz; ++i) {
-        for (uint32_t v = l3; v <= h3; ++v) {
-            const uint32_t bit = l1 + n1 * (z + n2 * v);
-            const uint32_t w = bit >> 5;
-            if (__funnelshift_r(__ldg(lost + w), __ldg(lost + w + 1), bit & 31) & mask) return true;
-        }
-        z = (z + 1 == n2) ? 0 : z + 1;
-    }
-    return false;
-}
-
-// The same for a packed box (one byte per bound).
-__device__ __forceinline__ bool box_rows_lost8(const uint32_t* __restrict__ lost, const GridInfo& g, uint32_t lo,
-                                               uint32_t hi) {
-    return box_rows_lost(lost, g, (lo >> 8) & 255u, (hi >> 8) & 255u, (lo >> 16) & 255u, (hi >> 16) & 255u, lo >> 24,
-                         hi >> 24);
-}
-
-// The bitmap of rows that lost a D cell in the previous iteration, when this
-// iteration tests only the pairs whose box holds one of them: from the
-// second iteration on, once the previous iteration added at most one state
-// per kStoredIncrementalRows rows (with more, nearly every box holds such a
-// row and the test of the bitmap costs more than it saves); else nullptr.
-constexpr unsigned long long kStoredIncrementalRows = 16;
-
-__device__ __forceinline__ const uint32_t* stored_lost_rows(const GridInfo& g, const StoredFixArgs& a,
-                                                            const FixControl* fc, uint32_t it) {
-    if (!a.rowlost || it < 2 || static_cast<unsigned long long>(fc->last_new) * kStoredIncrementalRows > g.rows)
-        return nullptr;
-    return a.rowlost + ((it - 1) & 1) * a.rl_words;
-}
-
-// Marks the row of state s in the bitmap `mark`.
-__device__ __forceinline__ void mark_row(uint32_t* mark, const GridInfo& g, uint64_t s) {
-    const uint32_t row = static_cast<uint32_t>(s / g.n[0]);
-    atomicOr(mark + (row >> 5), 1u << (row & 31));
-}
-
 __global__ void k_stored_init(GridInfo g, StoredFixArgs a) {
-    const uint64_t t0 = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
-    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
-    for (uint64_t s = t0; s < g.S; s += stride) {
+    for (uint64_t s = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; s < g.S;
+         s += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
         const uint8_t c = a.cand[s];
         a.reach[s] = c ? 1 : 0;
         a.controller[s] = kInvalid32;
         a.reach_step[s] = c ? 0u : kInvalid32;
     }
-    if (a.rowlost)
-        for (uint64_t i = t0; i < 2ull * a.rl_words; i += stride) a.rowlost[i] = 0;
 }
 
 // One thread per two consecutive states: a 16-byte load brings both states'
@@ -338,7 +286,6 @@ __global__ void __launch_bounds__(256) k_sat_stored(GridInfo g, StoredFixArgs a)
     const uint32_t it = fc->iter + 1;
     const uint64_t half = a.S_pad >> 1;
     const uint64_t t = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
-    const uint32_t* lost = stored_lost_rows(g, a, fc, it);
     unsigned long long nr = 0, nc = 0, nload = 0, ncount = 0;
     if (t < half) {
         bool act[2], isc[2], rch[2], cert[2], found[2] = {false, false};
@@ -362,25 +309,14 @@ __global__ void __launch_bounds__(256) k_sat_stored(GridInfo g, StoredFixArgs a)
                 const uint4 b = nb;
                 nload += 2;   // one 16-byte load carries two pairs' boxes
                 if (j + 1 < g.M) nb = ld_stream(bx + static_cast<uint64_t>(j + 1) * half);
-                const bool p0 = act[0] && !found[0] && b.x != kBoxSentinel;
-                const bool p1 = act[1] && !found[1] && b.z != kBoxSentinel;
-                bool t0 = p0, t1 = p1;
-                if (lost && (p0 || p1)) {
-                    // Neighbouring states usually share their y, theta and
-                    // v bounds, and with them the answer.
-                    if (p0) t0 = box_rows_lost8(lost, g, b.x, b.y);
-                    if (p1)
-                        t1 = (p0 && ((b.z ^ b.x) >> 8) == 0 && ((b.w ^ b.y) >> 8) == 0) ? t0
-                                                                                       : box_rows_lost8(lost, g, b.z, b.w);
-                }
-                if (t0) {
+                if (act[0] && !found[0] && b.x != kBoxSentinel) {
                     ++ncount;
                     if (dcount(a.pd, g, b.x, b.y) == 0) {
                         found[0] = true;
                         chosen[0] = j;
                     }
                 }
-                if (t1) {
+                if (act[1] && !found[1] && b.z != kBoxSentinel) {
                     ++ncount;
                     if (dcount(a.pd, g, b.z, b.w) == 0) {
                         found[1] = true;
@@ -397,7 +333,6 @@ __global__ void __launch_bounds__(256) k_sat_stored(GridInfo g, StoredFixArgs a)
             if (!rch[k]) {
                 a.reach[s] = 1;
                 ++nr;
-                if (a.rowlost) mark_row(a.rowlost + (it & 1) * a.rl_words, g, s);
             }
             if (!cert[k]) {
                 a.controller[s] = chosen[k];
@@ -430,7 +365,6 @@ __global__ void __launch_bounds__(256) k_sat_stored_wide(GridInfo g, StoredFixAr
     if (fc->stop) return;
     const uint32_t it = fc->iter + 1;
     const uint64_t s = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
-    const uint32_t* lost = stored_lost_rows(g, a, fc, it);
     unsigned long long nr = 0, nc = 0, nload = 0, ncount = 0;
     if (s < g.S) {
         const bool v = a.valid[s] != 0;
@@ -448,8 +382,6 @@ __global__ void __launch_bounds__(256) k_sat_stored_wide(GridInfo g, StoredFixAr
                 ++nload;
                 if (j + 1 < g.M) nb = ld_stream(bx + static_cast<uint64_t>(j + 1) * g.S);
                 if (b.x == kBoxSentinel) continue;
-                if (lost && !box_rows_lost(lost, g, hi16(b.x), hi16(b.z), lo16(b.y), lo16(b.w), hi16(b.y), hi16(b.w)))
-                    continue;
                 ++ncount;
                 if (dcount16(a.pd, g, b) == 0) {
                     found = true;
@@ -462,7 +394,6 @@ __global__ void __launch_bounds__(256) k_sat_stored_wide(GridInfo g, StoredFixAr
             if (!rch) {
                 a.reach[s] = 1;
                 ++nr;
-                if (a.rowlost) mark_row(a.rowlost + (it & 1) * a.rl_words, g, s);
             }
             if (!cert) {
                 a.controller[s] = chosen;
@@ -511,25 +442,13 @@ __global__ void k_fix_init(FixControl* fc, uint32_t max_iterations, uint32_t sta
 }
 
 __global__ void k_control(FixControl* fc, const unsigned long long* stats, cudaGraphConditionalHandle cond,
-                          int use_cond, uint32_t* rowlost, uint32_t rl_words) {
-    if (rowlost) {
-        // The bitmap that the next iteration marks; the one this iteration
-        // marked is read by the next.
-        const uint32_t stopped = fc->stop, it = fc->iter + 1;
-        __syncthreads();
-        if (!stopped) {
-            uint32_t* nxt = rowlost + ((it + 1) & 1) * rl_words;
-            for (uint32_t i = threadIdx.x; i < rl_words; i += blockDim.x) nxt[i] = 0;
-        }
-    }
-    if (threadIdx.x != 0) return;
+                          int use_cond) {
     if (!fc->stop) {
         const uint32_t it = fc->iter + 1;
         const unsigned long long nr = stats[kStatsCols * it];
         const unsigned long long nc = stats[kStatsCols * it + 1];
         fc->certified += nc;
         fc->reachable += nr;
-        fc->last_new = nr > 0xFFFFFFFFull ? 0xFFFFFFFFu : static_cast<uint32_t>(nr);
         fc->iter = it;
         if (fc->certified == fc->candidate_count) {
             fc->converged = 1;
@@ -624,7 +543,7 @@ cudaError_t launch_stored_iteration(const GridInfo& g, const StoredFixArgs& a, c
     else
         k_sat_stored<<<blocks_for(a.S_pad / 2, 256), 256, 0, st>>>(g, a);
     if (ev) cudaEventRecord(ev[5], st);
-    k_control<<<1, a.rowlost ? 256 : 1, 0, st>>>(a.fc, a.stats, a.cond, a.use_cond, a.rowlost, a.rl_words);
+    k_control<<<1, 1, 0, st>>>(a.fc, a.stats, a.cond, a.use_cond);
     if (ev) cudaEventRecord(ev[6], st);
     if (launches) *launches += prefix4_launches(g) + 2;
     return cudaGetLastError();

@@ -128,15 +128,6 @@ struct StoredFixArgs {
     unsigned long long* stats;   // [stats_cap][kStatsCols]
     cudaGraphConditionalHandle cond;
     int use_cond;
-    // [2][rl_words] bitmaps over the rows (y, theta, v): iteration it marks
-    // in bitmap it & 1 the rows of the states it made reachable.  When the
-    // previous iteration added few states, iteration it tests only the pairs
-    // whose box holds a row marked in bitmap (it - 1) & 1: the others failed
-    // before and their boxes still hold the same D cells.  The control
-    // kernel of iteration it clears bitmap (it + 1) & 1 for the next one.
-    // rl_words includes one word of padding.
-    uint32_t* rowlost;
-    uint32_t rl_words;
 };
 cudaError_t launch_stored_init(const GridInfo& g, const StoredFixArgs& a, cudaStream_t st);
 // ev (optional, kProfileEvents events): [0] before the prefix rebuild,
