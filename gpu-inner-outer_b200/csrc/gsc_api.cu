@@ -279,20 +279,28 @@ cudaError_t profile_events(gsc_context* ctx, cudaEvent_t** out) {
 // than the host takes to queue an iteration's kernels, events and copy.
 constexpr uint64_t kProfileHoldNs = 60000;
 
-// The pinned control-record slots and events of host-loop solves.
+// The mapped mirror word of host-loop solves.
 static cudaError_t loop_resources(gsc_context* ctx) {
-    if (!ctx->loop_fc) {
-        void* h = nullptr;
-        const cudaError_t err = cudaMallocHost(&h, 2 * sizeof(FixControl));
-        if (err != cudaSuccess) return err;
-        ctx->loop_fc = static_cast<FixControl*>(h);
+    if (ctx->loop_word) return cudaSuccess;
+    void* h = nullptr;
+    cudaError_t err = cudaHostAlloc(&h, 64, cudaHostAllocMapped | cudaHostAllocPortable);
+    if (err != cudaSuccess) return err;
+    void* d = nullptr;
+    err = cudaHostGetDevicePointer(&d, h, 0);
+    if (err != cudaSuccess) {
+        cudaFreeHost(h);
+        return err;
     }
-    for (auto& e : ctx->loop_ev)
-        if (!e) {
-            const cudaError_t err = cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
-            if (err != cudaSuccess) return err;
-        }
+    ctx->loop_word = static_cast<unsigned long long*>(h);
+    ctx->loop_word_dev = static_cast<unsigned long long*>(d);
     return cudaSuccess;
+}
+
+// One pause of a host spin-wait.
+static inline void cpu_relax() {
+#if defined(__x86_64__) || defined(__i386__)
+    __builtin_ia32_pause();
+#endif
 }
 
 // True for page-locked (or registered) host memory.
@@ -518,15 +526,13 @@ void gsc_context_destroy(gsc_context* ctx) {
         }
     for (auto e : ctx->setup_ev)
         if (e) cudaEventDestroy(e);
-    for (auto e : ctx->loop_ev)
-        if (e) cudaEventDestroy(e);
     for (auto e : ctx->side_ev)
         if (e) cudaEventDestroy(e);
     if (ctx->side) {
         cudaStreamSynchronize(ctx->side);
         cudaStreamDestroy(ctx->side);
     }
-    if (ctx->loop_fc) cudaFreeHost(ctx->loop_fc);
+    if (ctx->loop_word) cudaFreeHost(ctx->loop_word);
     ctx->pool.reset();
     pinned_trim(ctx);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -859,6 +865,7 @@ StoredFixArgs stored_args(const gsc_problem* p, cudaGraphConditionalHandle cond,
     a.stats = p->stats;
     a.cond = cond;
     a.use_cond = use_cond;
+    a.mirror = p->mirror;
     return a;
 }
 
@@ -906,6 +913,7 @@ FusedFixArgs fused_args(const gsc_problem* p, cudaGraphConditionalHandle cond, i
     a.offv = p->offv;
     a.cond = cond;
     a.use_cond = use_cond;
+    a.mirror = p->mirror;
     return a;
 }
 
@@ -1083,37 +1091,56 @@ int gsc_problem_solve(gsc_problem* p, uint32_t flags) {
         if (!p->exec) GSC_TRY(build_graph(p));
         GSC_CU(ctx, cudaGraphLaunch(p->exec, st));
     } else {
-        // Chunks of kLoopChunk iterations, two in flight: after enqueueing
-        // chunk k+1 the host waits for chunk k's copy of the control record,
-        // so the device does not idle on the host's check, and at most one
-        // chunk of iterations (kernels that return at once on the stop flag)
-        // runs past the stop.
-        constexpr uint32_t kLoopChunk = 2;
+        // The host keeps kLoopAhead iterations queued beyond the last one
+        // finished, which it reads from the mirror word (written by each
+        // iteration's last kernel, no copy in the stream), so the device
+        // never waits for the host, and at most kLoopAhead iterations
+        // (kernels that return at once on the stop flag) run past the stop.
+        // When the stream has drained and the word shows no stop (a stop set
+        // by a bounded device wait that gave up), the record in device memory
+        // decides.
+        constexpr uint32_t kLoopAhead = 2;
         GSC_CU(ctx, loop_resources(ctx));
+        volatile unsigned long long* word = ctx->loop_word;
+        *word = (p->q.max_iterations == 0) ? (1ull << 32) : 0ull;
         GSC_CU(ctx, enqueue_init(p));
         launches += 2;
-        uint32_t done = 0;
-        auto enqueue_chunk = [&](uint32_t slot) -> cudaError_t {
-            for (uint32_t i = 0; i < kLoopChunk; ++i) {
-                const cudaError_t e = enqueue_iteration(p, 0, 0, &launches);
-                if (e != cudaSuccess) return e;
+        p->mirror = ctx->loop_word_dev;
+        uint32_t enq = 0, polls = 0;
+        cudaError_t err = cudaSuccess;
+        bool timeout = false;
+        while (err == cudaSuccess) {
+            const unsigned long long m = *word;
+            if (m >> 32) break;
+            if (enq < static_cast<uint32_t>(m) + kLoopAhead) {
+                // The stop rules end the solve by iteration stats_cap - 1.
+                if (enq > p->stats_cap + kLoopAhead) {
+                    timeout = true;
+                    break;
+                }
+                err = enqueue_iteration(p, 0, 0, &launches);
+                ++enq;
+                continue;
             }
-            done += kLoopChunk;
-            const cudaError_t e =
-                cudaMemcpyAsync(ctx->loop_fc + slot, p->fc, sizeof(FixControl), cudaMemcpyDeviceToHost, st);
-            return e == cudaSuccess ? cudaEventRecord(ctx->loop_ev[slot], st) : e;
-        };
-        GSC_CU(ctx, enqueue_chunk(0));
-        for (uint32_t k = 0;; ++k) {
-            // The slot of chunk k+1 is chunk k-1's, whose record was read.
-            GSC_CU(ctx, enqueue_chunk((k + 1) & 1));
-            GSC_CU(ctx, cudaEventSynchronize(ctx->loop_ev[k & 1]));
-            if (ctx->loop_fc[k & 1].stop) break;
-            if (done > p->stats_cap + 4 * kLoopChunk) {
-                cudaStreamSynchronize(st);
-                return fail(ctx, GSC_ERR_TIMEOUT, "fixpoint did not stop within its iteration bound");
+            if ((++polls & 63) == 0) {
+                const cudaError_t q = cudaStreamQuery(st);
+                if (q == cudaErrorNotReady) continue;
+                if (q != cudaSuccess) {
+                    err = q;
+                    break;
+                }
+                FixControl f;
+                err = cudaMemcpy(&f, p->fc, sizeof(f), cudaMemcpyDeviceToHost);
+                if (err != cudaSuccess || f.stop) break;
+                *word = f.iter;
+                continue;
             }
+            cpu_relax();
         }
+        p->mirror = nullptr;
+        if (err != cudaSuccess || timeout) cudaStreamSynchronize(st);
+        GSC_CU(ctx, err);
+        if (timeout) return fail(ctx, GSC_ERR_TIMEOUT, "fixpoint did not stop within its iteration bound");
     }
     GSC_CU(ctx, cudaEventRecord(ctx->ev[1], st));
     GSC_CU(ctx, cudaEventSynchronize(ctx->ev[1]));

@@ -442,7 +442,7 @@ __global__ void k_fix_init(FixControl* fc, uint32_t max_iterations, uint32_t sta
 }
 
 __global__ void k_control(FixControl* fc, const unsigned long long* stats, cudaGraphConditionalHandle cond,
-                          int use_cond) {
+                          int use_cond, unsigned long long* mirror) {
     if (!fc->stop) {
         const uint32_t it = fc->iter + 1;
         const unsigned long long nr = stats[kStatsCols * it];
@@ -463,6 +463,12 @@ __global__ void k_control(FixControl* fc, const unsigned long long* stats, cudaG
         }
     }
     if (use_cond) cudaGraphSetConditional(cond, fc->stop ? 0u : 1u);
+    if (mirror) {
+        // iter | stop << 32 for a host loop that polls it.
+        *reinterpret_cast<volatile unsigned long long*>(mirror) =
+            fc->iter | (static_cast<unsigned long long>(fc->stop ? 1u : 0u) << 32);
+        __threadfence_system();
+    }
 }
 
 __global__ void k_set_condition(const FixControl* fc, cudaGraphConditionalHandle cond) {
@@ -543,7 +549,7 @@ cudaError_t launch_stored_iteration(const GridInfo& g, const StoredFixArgs& a, c
     else
         k_sat_stored<<<blocks_for(a.S_pad / 2, 256), 256, 0, st>>>(g, a);
     if (ev) cudaEventRecord(ev[5], st);
-    k_control<<<1, 1, 0, st>>>(a.fc, a.stats, a.cond, a.use_cond);
+    k_control<<<1, 1, 0, st>>>(a.fc, a.stats, a.cond, a.use_cond, a.mirror);
     if (ev) cudaEventRecord(ev[6], st);
     if (launches) *launches += prefix4_launches(g) + 2;
     return cudaGetLastError();

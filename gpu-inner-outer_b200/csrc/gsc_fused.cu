@@ -197,6 +197,7 @@ __global__ void __launch_bounds__(256) k_fused_finalize(GridInfo g, FusedFixArgs
     if (fc->stop) {
         // Already stopped (e.g. max_iterations == 0): the graph loop must still end.
         if (a.use_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(a.cond, 0u);
+        if (a.mirror && blockIdx.x == 0 && threadIdx.x == 0) write_mirror(a.mirror, fc);
         return;
     }
     const uint32_t it = fc->iter + 1;
@@ -228,6 +229,7 @@ __global__ void __launch_bounds__(256) k_fused_finalize(GridInfo g, FusedFixArgs
         if (a.shard_slices) return;
         control_step(fc, row, it);
         if (a.use_cond) cudaGraphSetConditional(a.cond, fc->stop ? 0u : 1u);
+        if (a.mirror) write_mirror(a.mirror, fc);
     }
 }
 

@@ -551,6 +551,14 @@ __device__ __forceinline__ void add_counters(unsigned long long* row, unsigned l
     }
 }
 
+// iter | stop << 32 of the control record into the host's mirror word, for
+// a host loop that polls it instead of copying the record back.
+__device__ __forceinline__ void write_mirror(unsigned long long* mirror, const FixControl* fc) {
+    *reinterpret_cast<volatile unsigned long long*>(mirror) =
+        fc->iter | (static_cast<unsigned long long>(fc->stop ? 1u : 0u) << 32);
+    __threadfence_system();
+}
+
 // The stop rules after iteration `it` (reachability.hpp:133-144), by one
 // thread once every counter of the iteration is in.
 // Its loads are one round, from L2 (where the other blocks' counter atomics

@@ -67,11 +67,11 @@ struct gsc_context {
     // taking a cached block.  Freed by gsc_context_trim and at destruction.
     std::mutex pin_mu;
     std::multimap<size_t, void*> pin_free;
-    // Host-loop solves: two pinned copies of the control record and an event
-    // per copy, so that one chunk of iterations runs while the host reads
-    // the stop flag of the previous one (created at first use).
-    gsc_b200::FixControl* loop_fc = nullptr;
-    cudaEvent_t loop_ev[2] = {nullptr, nullptr};
+    // Host-loop solves: a page-locked word, mapped for the device, into which
+    // each iteration's last kernel writes iter | stop << 32, so that the host
+    // follows the solve without copies in the stream (created at first use).
+    unsigned long long* loop_word = nullptr;
+    unsigned long long* loop_word_dev = nullptr;
     // A second stream for copies that overlap a solve (gsc_run_case), with
     // the events that order it against `stream` (created at first use).
     cudaStream_t side = nullptr;
@@ -145,6 +145,8 @@ struct gsc_problem {
     uint32_t* rowlost = nullptr;
     // sharded solve (gsc_problem_shard_*): this rank's slices and iterations done
     uint32_t shard_begin = 0, shard_slices = 0, shard_iter = 0;
+    // The context's mirror word while a host-loop solve runs, else nullptr.
+    unsigned long long* mirror = nullptr;
     bool shard_stopped = false;
     uint32_t rl_words = 0;
     uint32_t* offz = nullptr;   // per omega column and theta cell: part of a dilated row's offset

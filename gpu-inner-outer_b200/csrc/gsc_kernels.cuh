@@ -128,6 +128,10 @@ struct StoredFixArgs {
     unsigned long long* stats;   // [stats_cap][kStatsCols]
     cudaGraphConditionalHandle cond;
     int use_cond;
+    // Host-loop solves: a word of page-locked host memory, mapped for the
+    // device, that receives iter | stop << 32 after each iteration's stop
+    // rules (write_mirror), or nullptr.
+    unsigned long long* mirror;
 };
 cudaError_t launch_stored_init(const GridInfo& g, const StoredFixArgs& a, cudaStream_t st);
 // ev (optional, kProfileEvents events): [0] before the prefix rebuild,
@@ -209,6 +213,7 @@ struct FusedFixArgs {
     uint32_t shard_slices;
     cudaGraphConditionalHandle cond;
     int use_cond;
+    unsigned long long* mirror;   // as StoredFixArgs::mirror
 };
 constexpr int kFusedWarps = 8;   // most warps of a satisfaction block
 
