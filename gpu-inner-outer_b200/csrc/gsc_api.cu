@@ -303,29 +303,7 @@ static inline void cpu_relax() {
 #endif
 }
 
-// True for page-locked (or registered) host memory.
-static bool is_pinned(const void* ptr) {
-    cudaPointerAttributes at{};
-    if (cudaPointerGetAttributes(&at, ptr) != cudaSuccess) {
-        cudaGetLastError();
-        return false;
-    }
-    return at.type == cudaMemoryTypeHost;
-}
 
-// The side stream of overlapped copies and its two ordering events.
-static cudaError_t side_resources(gsc_context* ctx) {
-    if (!ctx->side) {
-        const cudaError_t err = cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking);
-        if (err != cudaSuccess) return err;
-    }
-    for (auto& e : ctx->side_ev)
-        if (!e) {
-            const cudaError_t err = cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
-            if (err != cudaSuccess) return err;
-        }
-    return cudaSuccess;
-}
 
 // Device memory in use on the current GPU (all processes), as the reference
 // samples it (kernels.cu:30-42).
@@ -526,12 +504,6 @@ void gsc_context_destroy(gsc_context* ctx) {
         }
     for (auto e : ctx->setup_ev)
         if (e) cudaEventDestroy(e);
-    for (auto e : ctx->side_ev)
-        if (e) cudaEventDestroy(e);
-    if (ctx->side) {
-        cudaStreamSynchronize(ctx->side);
-        cudaStreamDestroy(ctx->side);
-    }
     if (ctx->loop_word) cudaFreeHost(ctx->loop_word);
     ctx->pool.reset();
     pinned_trim(ctx);
@@ -1448,36 +1420,8 @@ int gsc_run_case(int device, const gsc_model_desc* model, const gsc_query_desc* 
     gsc_problem* p = nullptr;
     int s = gsc_abstraction_create(ctx, model, &abs);
     if (s == GSC_OK) s = gsc_problem_create(ctx, abs, query, method, &p);
-    // The valid and candidate masks are final once the problem is built:
-    // into page-locked host arrays they are copied on the side stream while
-    // the fixpoint runs.  (A copy into pageable memory would hold the host
-    // until it is done, so those are read after the solve as usual.)
-    bool side = false;
-    if (s == GSC_OK && out->valid_mask && out->candidate_mask && is_pinned(out->valid_mask) &&
-        is_pinned(out->candidate_mask)) {
-        cudaError_t e = side_resources(ctx);
-        if (e == cudaSuccess) e = cudaEventRecord(ctx->side_ev[0], ctx->stream);
-        if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->side, ctx->side_ev[0], 0);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(out->valid_mask, p->valid, p->g.S, cudaMemcpyDeviceToHost, ctx->side);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(out->candidate_mask, p->cand, p->g.S, cudaMemcpyDeviceToHost, ctx->side);
-        if (e == cudaSuccess) e = cudaEventRecord(ctx->side_ev[1], ctx->side);
-        side = e == cudaSuccess;
-        if (!side) s = fail(ctx, GSC_ERR_CUDA, cudaGetErrorString(e));
-    }
     if (s == GSC_OK) s = gsc_problem_solve(p, flags);
-    if (s == GSC_OK) {
-        gsc_result r = *out;
-        if (side) r.valid_mask = r.candidate_mask = nullptr;
-        s = gsc_problem_read(p, &r);
-        r.valid_mask = out->valid_mask;
-        r.candidate_mask = out->candidate_mask;
-        *out = r;
-    }
-    // The side copies read the problem's masks: they end before it is freed.
-    if (side) {
-        const cudaError_t e = cudaStreamSynchronize(ctx->side);
-        if (e != cudaSuccess && s == GSC_OK) s = fail(ctx, GSC_ERR_CUDA, cudaGetErrorString(e));
-    }
+    if (s == GSC_OK) s = gsc_problem_read(p, out);
     if (s == GSC_OK && timings) gsc_problem_timings(p, timings);
     gsc_problem_destroy(p);
     gsc_abstraction_destroy(abs);

@@ -72,10 +72,6 @@ struct gsc_context {
     // follows the solve without copies in the stream (created at first use).
     unsigned long long* loop_word = nullptr;
     unsigned long long* loop_word_dev = nullptr;
-    // A second stream for copies that overlap a solve (gsc_run_case), with
-    // the events that order it against `stream` (created at first use).
-    cudaStream_t side = nullptr;
-    cudaEvent_t side_ev[2] = {nullptr, nullptr};
 };
 
 struct gsc_abstraction {
@@ -145,8 +141,6 @@ struct gsc_problem {
     uint32_t* rowlost = nullptr;
     // sharded solve (gsc_problem_shard_*): this rank's slices and iterations done
     uint32_t shard_begin = 0, shard_slices = 0, shard_iter = 0;
-    // The context's mirror word while a host-loop solve runs, else nullptr.
-    unsigned long long* mirror = nullptr;
     bool shard_stopped = false;
     uint32_t rl_words = 0;
     uint32_t* offz = nullptr;   // per omega column and theta cell: part of a dilated row's offset
@@ -155,6 +149,8 @@ struct gsc_problem {
     gsc_b200::DilateArgs dil{};
     int need_valid = 0;
     // common fixpoint state
+    // The context's mirror word while a host-loop solve runs, else nullptr.
+    unsigned long long* mirror = nullptr;
     uint32_t* controller = nullptr;
     uint32_t* reach_step = nullptr;
     gsc_b200::FixControl* fc = nullptr;
