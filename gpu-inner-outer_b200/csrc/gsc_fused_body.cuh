@@ -175,7 +175,13 @@ __device__ __forceinline__ int group_sync_or(int p) {
 // words into a 16-byte aligned slot, and readers add the span's leading
 // offset (fused_smem_layout).
 // Every early return is taken by the whole group.
-constexpr unsigned long long kIncrementalRows = 16;
+// An iteration runs incrementally when the previous one added at most one
+// state per kIncrementalRows x-rows.  Measured at 128x128x72x48: 16 -> 4
+// took the fixpoint from 42.8 to 40.9 ms; 1 took it to 40.6 ms but slowed
+// the published demo by 0.5 %, and testing incrementally in every iteration
+// slowed it by 6 %.  A sharded solve sets last_new to 2^32 - 1, which no
+// threshold of 1 or more admits.
+constexpr unsigned long long kIncrementalRows = 4;
 
 template <int WMAX, bool EXACTW, int NVMODE, bool WARP = false, bool BULK = false>
 __device__ __forceinline__ void sat_col_task(const GridInfo& g, const FusedFixArgs& a, uint32_t task,
@@ -255,8 +261,8 @@ __device__ __forceinline__ void sat_col_task(const GridInfo& g, const FusedFixAr
         // in the previous one, and D' only loses cells, so a state can newly
         // pass only if its box holds a cell that left D' in the previous
         // iteration.  When that iteration added few states (at most one per
-        // kIncrementalRows x-rows; a new state touches the items of about
-        // that many rows), the iteration runs incrementally (phase B).
+        // kIncrementalRows x-rows), the iteration runs incrementally (phase
+        // B).
         const uint32_t stop = fc->stop, it = fc->iter, last = fc->last_new;
         const bool inc = it > 0 && static_cast<unsigned long long>(last) * kIncrementalRows <= g.rows;
         s_meta[1] = a.zt[i2 * mw + jw];
