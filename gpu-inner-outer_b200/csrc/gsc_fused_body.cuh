@@ -337,14 +337,28 @@ __device__ __forceinline__ void sat_col_task(const GridInfo& g, const FusedFixAr
         for (uint32_t e = tid; e < nrep * W1; e += bd) {
             const uint32_t r = e / W1, yw = e - r * W1;
             const uint32_t we = repw[r];
-            uint32_t m = 0, z = lz;
-            for (uint32_t i = 0; i < nz; ++i) {
-                for (uint32_t v = lo16(we); v <= hi16(we); ++v) {
-                    const uint32_t bit = n1 * (z + n2 * v) + yw * 32;
-                    m |= __funnelshift_r(rl[bit >> 5], rl[(bit >> 5) + 1], bit & 31);
+            const uint32_t v0 = lo16(we), v1 = hi16(we);
+            // The window's (theta, v) rows with the next row's loads issued
+            // before the current row's words are used (two in flight).
+            uint32_t z = lz, v = v0;
+            uint32_t bit = n1 * (z + n2 * v) + yw * 32;
+            uint32_t c0 = __ldg(rl + (bit >> 5)), c1 = __ldg(rl + (bit >> 5) + 1), cs = bit & 31;
+            uint32_t m = 0;
+            for (uint32_t q = 1; q < nz * (v1 - v0 + 1); ++q) {
+                if (v == v1) {
+                    v = v0;
+                    z = (z + 1 == n2) ? 0 : z + 1;
+                } else {
+                    ++v;
                 }
-                z = (z + 1 == n2) ? 0 : z + 1;
+                bit = n1 * (z + n2 * v) + yw * 32;
+                const uint32_t d0 = __ldg(rl + (bit >> 5)), d1 = __ldg(rl + (bit >> 5) + 1);
+                m |= __funnelshift_r(c0, c1, cs);
+                c0 = d0;
+                c1 = d1;
+                cs = bit & 31;
             }
+            m |= __funnelshift_r(c0, c1, cs);
             if (yw == W1 - 1 && (n1 & 31)) m &= (1u << (n1 & 31)) - 1;
             rowchg[r * W1 + yw] = m;
             lost |= m != 0;
