@@ -200,6 +200,11 @@ const char* gsc_message_string(int message);
 int gsc_grid_shape(const gsc_model_desc* model, uint32_t shape[4], uint32_t input_shape[2]);
 
 /* A context binds a device and a stream (NULL stream = a private stream).
+ * A context and the handles made from it are used from one host thread at
+ * a time (its timing events and its host-loop stop word are its own);
+ * threads that solve at the same time use a context each.  gsc_run_case
+ * keeps one context per device and serialises its calls; the gsc_server_*
+ * calls are thread-safe.
  * Mirrors the device checks of kernels.cu:496-502.  Problems and
  * abstractions of a context take their device memory from the context's
  * caching pool (regions of 64 MB or more, sub-allocated first-fit), so a
