@@ -521,26 +521,16 @@ __device__ __forceinline__ void finalize_word(const GridInfo& g, const FusedFixA
                                               unsigned long long& nc) {
     const bword h = a.hit[e];
     if (!h) return;
+    // Every load the word needs, issued before any of its stores (one round
+    // trip): its sets and the best[] entries of its first four new states.
     const bword rp = rprev[e];
-    const bword rn = rp | h;
-    rnext[e] = rn;
-    const bword dn = (a.validb[e] & ~rn) | a.unsafeb[e];
-    if (a.dp[e] & ~dn) {   // the row lost a D' cell in iteration `it`
-        const uint32_t r = static_cast<uint32_t>(e / g.W);
-        atomicOr(a.rowlost + (it & 1) * a.rl_words + (r >> 5), 1u << (r & 31));
-    }
-    a.dp[e] = dn;
-    a.hit[e] = 0;
-    a.active[e] &= ~h;
-    const bword c = a.candb[e];
-    nr += __popc(h & ~rp);
-    nc += __popc(h & c);
+    const bword vb = a.validb[e], ub = a.unsafeb[e], dpo = a.dp[e], c = a.candb[e], act = a.active[e];
     const uint64_t r = e / g.W;
     const uint64_t sbase = r * g.n[0] + (e - r * g.W) * kBits;
     bword m = h;
-    while (m) {
-        // Four states at a time: their best[] loads in flight together.
-        uint32_t b[4], j[4];
+    uint32_t b[4], j[4];
+    // Four states at a time: their best[] loads in flight together.
+    auto load4 = [&]() {
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             b[k] = m ? static_cast<uint32_t>(__ffs(m) - 1) : kBits;
@@ -548,6 +538,21 @@ __device__ __forceinline__ void finalize_word(const GridInfo& g, const FusedFixA
         }
 #pragma unroll
         for (int k = 0; k < 4; ++k) j[k] = b[k] < kBits ? a.best[sbase + b[k]] : kInvalid32;
+    };
+    load4();
+    const bword rn = rp | h;
+    rnext[e] = rn;
+    const bword dn = (vb & ~rn) | ub;
+    if (dpo & ~dn) {   // the row lost a D' cell in iteration `it`
+        const uint32_t row = static_cast<uint32_t>(r);
+        atomicOr(a.rowlost + (it & 1) * a.rl_words + (row >> 5), 1u << (row & 31));
+    }
+    a.dp[e] = dn;
+    a.hit[e] = 0;
+    a.active[e] = act & ~h;
+    nr += __popc(h & ~rp);
+    nc += __popc(h & c);
+    for (;;) {
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             if (b[k] >= kBits) continue;
@@ -556,6 +561,8 @@ __device__ __forceinline__ void finalize_word(const GridInfo& g, const FusedFixA
             a.best[s] = kInvalid32;
             if (!((c >> b[k]) & 1u)) a.reach_step[s] = it;
         }
+        if (!m) break;
+        load4();
     }
 }
 
