@@ -793,7 +793,7 @@ int problem_stage2(gsc_problem* p) {
     GSC_TRY(palloc(p, &p->best, g.S));
     const uint64_t combos = static_cast<uint64_t>(p->dil.nk) * p->dil.nl;
     GSC_TRY(palloc(p, &p->dzw, combos * words + 4));
-    p->rl_words = static_cast<uint32_t>(g.rows / 32 + 2);
+    p->rl_words = g.slices * ((g.n[1] + 31) / 32) + 1;
     GSC_TRY(palloc(p, &p->rowlost, 2ull * p->rl_words));
     GSC_TRY(palloc(p, &p->offz, static_cast<uint64_t>(g.n[2]) * g.mw));
     GSC_TRY(palloc(p, &p->offv, static_cast<uint64_t>(g.n[3]) * g.ma));

@@ -90,15 +90,17 @@ __device__ __forceinline__ void dilate_position(const GridInfo& g, const bword* 
     const uint32_t lfit = min(lmax, n3 - v);   // v windows that stay inside the grid
     if (lost) {
         // Every bit of the window is read (no early exit), so the loads of
-        // several theta cells are in flight together.
+        // several theta cells are in flight together.  The row-lost words
+        // hold W1 = ceil(n1 / 32) words per (theta, v) slice, bit y % 32 of
+        // word y / 32 for row y.
+        const uint32_t W1 = (n1 + 31) / 32, yw = y >> 5, yb = y & 31;
         uint32_t hit = 0, zz = z;
 #pragma unroll 4
         for (uint32_t i = 0; i < kmax; ++i) {
 #pragma unroll
             for (uint32_t j = 0; j < kMaxDilate; ++j) {
                 if (j < lfit) {
-                    const uint32_t rr = y + n1 * (zz + n2 * (v + j));
-                    hit |= (lost[rr >> 5] >> (rr & 31)) & 1u;
+                    hit |= (lost[(zz + n2 * (v + j)) * W1 + yw] >> yb) & 1u;
                 }
             }
             zz = (zz + 1 == n2) ? 0 : zz + 1;
@@ -338,11 +340,10 @@ __device__ __forceinline__ void sat_col_task(const GridInfo& g, const FusedFixAr
             const uint32_t r = e / W1, yw = e - r * W1;
             const uint32_t we = repw[r];
             const uint32_t v0 = lo16(we), v1 = hi16(we);
-            // The window's (theta, v) rows with the next row's loads issued
-            // before the current row's words are used (two in flight).
+            // The window's (theta, v) slices' row-lost words (W1 per slice),
+            // the next slice's load issued before the current one is used.
             uint32_t z = lz, v = v0;
-            uint32_t bit = n1 * (z + n2 * v) + yw * 32;
-            uint32_t c0 = __ldg(rl + (bit >> 5)), c1 = __ldg(rl + (bit >> 5) + 1), cs = bit & 31;
+            uint32_t c0 = __ldg(rl + (z + n2 * v) * W1 + yw);
             uint32_t m = 0;
             for (uint32_t q = 1; q < nz * (v1 - v0 + 1); ++q) {
                 if (v == v1) {
@@ -351,15 +352,11 @@ __device__ __forceinline__ void sat_col_task(const GridInfo& g, const FusedFixAr
                 } else {
                     ++v;
                 }
-                bit = n1 * (z + n2 * v) + yw * 32;
-                const uint32_t d0 = __ldg(rl + (bit >> 5)), d1 = __ldg(rl + (bit >> 5) + 1);
-                m |= __funnelshift_r(c0, c1, cs);
+                const uint32_t d0 = __ldg(rl + (z + n2 * v) * W1 + yw);
+                m |= c0;
                 c0 = d0;
-                c1 = d1;
-                cs = bit & 31;
             }
-            m |= __funnelshift_r(c0, c1, cs);
-            if (yw == W1 - 1 && (n1 & 31)) m &= (1u << (n1 & 31)) - 1;
+            m |= c0;
             rowchg[r * W1 + yw] = m;
             lost |= m != 0;
         }
@@ -543,9 +540,10 @@ __device__ __forceinline__ void finalize_word(const GridInfo& g, const FusedFixA
     const bword rn = rp | h;
     rnext[e] = rn;
     const bword dn = (vb & ~rn) | ub;
-    if (dpo & ~dn) {   // the row lost a D' cell in iteration `it`
-        const uint32_t row = static_cast<uint32_t>(r);
-        atomicOr(a.rowlost + (it & 1) * a.rl_words + (row >> 5), 1u << (row & 31));
+    if (dpo & ~dn) {   // the row lost a D' cell in iteration `it`: word y / 32 of its slice
+        const uint32_t row = static_cast<uint32_t>(r), n1 = g.n[1];
+        const uint32_t sl = row / n1, y = row - sl * n1;
+        atomicOr(a.rowlost + (it & 1) * a.rl_words + sl * ((n1 + 31) / 32) + (y >> 5), 1u << (y & 31));
     }
     a.dp[e] = dn;
     a.hit[e] = 0;

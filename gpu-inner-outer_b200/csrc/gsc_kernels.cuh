@@ -193,6 +193,7 @@ struct FusedFixArgs {
     uint32_t sat_threads;      // threads per satisfaction block (64, 128 or 256)
     bword* dzw;                // (theta, v)-dilated D' [combo][rows * W], brought up to date each iteration
     uint32_t* rowlost;         // [2][rl_words] bit per x-row: the row lost a D' cell in the iteration
+                               // (W1 = ceil(n1 / 32) words per (theta, v) slice, bit y % 32 of word y / 32)
                                // (iter & 1) just finalised
     uint32_t rl_words;         // rows / 32 + 2
     const bword* vzw;          // (theta, v)-dilated valid set (when validity is more than safety)
