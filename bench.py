@@ -332,9 +332,9 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def ncu_traffic(kernel, workload):
-    """DRAM bytes per launch of `kernel` on `workload` from a committed ncu
-    summary (profiles/*.txt lines 'traffic kernel=<k> workload=<w> bytes_per_launch=<n>')."""
+def ncu_figure(tag, field, kernel, workload):
+    """A per-launch figure of `kernel` on `workload` from a committed ncu
+    summary (profiles/*.md lines '<tag> kernel=<k> workload=<w> <field>=<n>')."""
     pdir = os.path.join(ROOT, "profiles")
     if not os.path.isdir(pdir):
         return None
@@ -343,11 +343,30 @@ def ncu_traffic(kernel, workload):
             continue
         with open(os.path.join(pdir, fn)) as f:
             for ln in f:
-                if ln.startswith("traffic ") and f"kernel={kernel} " in ln and f"workload={workload} " in ln:
+                if ln.startswith(tag + " ") and f"kernel={kernel} " in ln and f"workload={workload} " in ln:
                     for tok in ln.split():
-                        if tok.startswith("bytes_per_launch="):
+                        if tok.startswith(field + "="):
                             return float(tok.split("=")[1])
     return None
+
+
+def ncu_traffic(kernel, workload):
+    """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum)."""
+    return ncu_figure("traffic", "bytes_per_launch", kernel, workload)
+
+
+def issue_roofline(kernel, workload, per_launch_ms, sm_mhz, sms):
+    """The kernel against its issue rate: warp instructions per launch
+    (smsp__inst_executed.sum averaged over one fixpoint's launches, from a
+    committed ncu summary) over the live launch time, against 4 schedulers
+    per SM issuing one warp instruction per cycle at the sampled SM clock."""
+    inst = ncu_figure("instructions", "warp_instructions_per_launch", kernel, workload)
+    if not inst or not sm_mhz or not per_launch_ms:
+        return None
+    achieved = inst / (per_launch_ms * 1e-3) / 1e12
+    peak = 4 * sms * sm_mhz * 1e6 / 1e12
+    return {"achieved": achieved, "peak": peak, "unit": "T warp instructions/s", "frac": achieved / peak,
+            "warp_instructions_per_launch": inst}
 
 
 def algorithmic_bytes(method, g, timings):
@@ -929,6 +948,8 @@ def main():
     peak, peak_kind = measured_peak()
     achieved = alg / (per_launch_ms * 1e-3) / 1e9
     traffic = ncu_traffic(kname, case["name"])
+    issue = issue_roofline(kname, case["name"], per_launch_ms, clocks.summary().get("sm_mhz"),
+                           torch.cuda.get_device_properties(dev).multi_processor_count)
 
     # End to end through the public one-shot call: host description in, pinned host arrays out.
     e2e_ms = []
@@ -980,7 +1001,7 @@ def main():
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "kernel": kname,
                      "kernel_ms_per_launch": per_launch_ms, "algorithmic_bytes_per_launch": alg,
-                     "peak_kind": peak_kind},
+                     "peak_kind": peak_kind, "issue": issue},
         "cpu_baseline": cpu,
         "e2e": {"value": replica_value(world, P * r["iterations"], e2e_step), "unit": "pair-checks/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_step},
