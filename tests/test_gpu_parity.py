@@ -157,6 +157,23 @@ def test_resolve_same_problem_twice(ctx):
         assert_same_result(r3, r1, "host loop after graph")
 
 
+@pytest.mark.parametrize("cap", [1, 2, 3, 5, 8, 13, 33, 34, 35])
+def test_max_iterations_stop_against_oracle(ctx, cap):
+    """A solve cut off by max_iterations (reachability.hpp:141-144) at every
+    stage of hyperbolic_mid_b's 34 iterations: the host loop (which queues
+    iterations ahead of the stop word) and the graph give the oracle's bits,
+    iteration count and message, for both methods."""
+    case = dict(INDEX["hyperbolic_mid_b"]["case"], max_iterations=cap)
+    want = O.solve(case)
+    assert want["iterations"] == min(cap, 34)
+    for method in METHODS.values():
+        for graph in (False, True):
+            got = solve(ctx, case, method, graph)
+            assert_same_result(got, want, f"cap {cap}/{method}/graph={graph}")
+            assert got["iterations"] == want["iterations"] and got["message"] == want["message"]
+            assert got["converged"] == want["converged"]
+
+
 def test_context_pool_reuse_budget_and_trim():
     """Problems of a context draw on its caching pool: a second create/destroy
     cycle needs no new device memory, trim returns every unused region, and a
