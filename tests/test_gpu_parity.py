@@ -174,6 +174,21 @@ def test_max_iterations_stop_against_oracle(ctx, cap):
             assert got["converged"] == want["converged"]
 
 
+def test_context_on_a_caller_stream():
+    """A context bound to the caller's CUDA stream (a torch stream here): both
+    loops run on it and give the fixture's result, for both methods."""
+    torch = pytest.importorskip("torch")
+    s = torch.cuda.Stream(device=0)
+    name = "hyperbolic_mid_b"
+    with G.Context(0, stream=s.cuda_stream) as c:
+        for method in METHODS.values():
+            for graph in (False, True):
+                got = solve(c, INDEX[name]["case"], method, graph)
+                assert_same_result(got, golden_arrays(name), f"caller stream {method} graph={graph}")
+                assert got["iterations"] == INDEX[name]["iterations"]
+    torch.cuda.synchronize(0)
+
+
 def test_context_pool_reuse_budget_and_trim():
     """Problems of a context draw on its caching pool: a second create/destroy
     cycle needs no new device memory, trim returns every unused region, and a
