@@ -110,6 +110,34 @@ def test_random_instances_against_oracle(ctx, index):
         assert got["iterations"] == want["iterations"] and got["message"] == want["message"]
 
 
+def demo_variant(i):
+    """The published demo's geometry and dynamics on a seeded grid (20–72 x
+    20–72 x 16–48 x 5–12 cells), input steps and substep count: fixpoints of
+    6 to 44 iterations on rows of one to three words."""
+    rng = np.random.default_rng([4242, i])
+    c = dict(C.hyperbolic_demo_case())
+    n = [int(rng.integers(20, 73)), int(rng.integers(20, 73)), int(rng.integers(16, 49)), int(rng.integers(5, 13))]
+    c["name"] = "demo_variant_%d" % i
+    c["state_eta"] = [(c["state_ub"][d] - c["state_lb"][d]) / n[d] for d in range(4)]
+    c["input_eta"] = [float(rng.choice([0.4, 0.5, 2.0 / 3.0])), float(rng.choice([0.4, 0.5, 2.0 / 3.0]))]
+    c["integration_substeps"] = int(rng.choice([4, 8, 16]))
+    c["expect_shape"] = n
+    return C.checked(c)
+
+
+@pytest.mark.parametrize("index", range(8))
+def test_demo_variants_against_oracle(ctx, index):
+    """Deep fixpoints on odd grid shapes (incremental iterations, row-lost
+    tests, several words per row) through both methods and both loops."""
+    case = demo_variant(index)
+    want = O.solve(case)
+    for method in METHODS.values():
+        for graph in (False, True):
+            got = solve(ctx, case, method, graph)
+            assert_same_result(got, want, f"{case['name']}/{method}/graph={graph}")
+            assert got["iterations"] == want["iterations"] and got["message"] == want["message"]
+
+
 def test_safe_mask_overrides(ctx):
     """A custom constraint (ConstraintType::kCustom) arrives as a host mask:
     rank 2 over (x, y) and rank 4 over all cells give the oracle's result."""
