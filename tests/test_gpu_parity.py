@@ -138,6 +138,34 @@ def test_demo_variants_against_oracle(ctx, index):
             assert got["iterations"] == want["iterations"] and got["message"] == want["message"]
 
 
+@pytest.mark.parametrize("shape", [(1, 9, 8, 3), (9, 1, 8, 3), (33, 5, 1, 3), (17, 6, 8, 1), (1, 1, 1, 1),
+                                   (32, 32, 2, 2), (64, 33, 3, 2)])
+def test_degenerate_grids_against_oracle(ctx, shape):
+    """Grids of one cell along a dimension (one theta cell: every box wraps
+    the whole circle), one-cell grids and rows of exactly one or two words:
+    each method that takes the grid gives the oracle's result."""
+    c = dict(C.hyperbolic_demo_case())
+    c["name"] = "degenerate_%dx%dx%dx%d" % shape
+    c["state_eta"] = [(c["state_ub"][d] - c["state_lb"][d]) / shape[d] for d in range(4)]
+    c["input_eta"] = [2.0 / 3.0, 2.0 / 3.0]
+    c["integration_substeps"] = 4
+    c["expect_shape"] = list(shape)
+    case = C.checked(c)
+    want = O.solve(case)
+    solved = 0
+    for method in (G.METHOD_AUTO, G.METHOD_STORED, G.METHOD_FUSED):
+        for graph in (False, True):
+            try:
+                got = solve(ctx, case, method, graph)
+            except G.GscError as e:
+                assert method == G.METHOD_FUSED and e.status == 4, e   # fused refuses: stored takes it
+                continue
+            assert_same_result(got, want, f"{c['name']}/{method}/graph={graph}")
+            assert got["iterations"] == want["iterations"] and got["message"] == want["message"]
+            solved += 1
+    assert solved >= 4
+
+
 def test_safe_mask_overrides(ctx):
     """A custom constraint (ConstraintType::kCustom) arrives as a host mask:
     rank 2 over (x, y) and rank 4 over all cells give the oracle's result."""
