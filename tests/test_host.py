@@ -73,3 +73,21 @@ def test_no_device_fails_loudly():
     assert e.value.status == 5
     with pytest.raises(G.GscError):
         G.run_case(C.default_case())
+
+
+def test_bench_reads_the_committed_kernel_figures():
+    """bench.py's roofline takes the dominant kernel's DRAM traffic and warp
+    instructions per launch from the committed ncu summaries; both are there
+    for the default workload, and the issue roofline computes from them."""
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("bench_module", os.path.join(ROOT, "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    workload = C.PRESETS["demo_scale"]()["name"]
+    traffic = bench.ncu_traffic("k_sat_col", workload)
+    assert traffic and 1e6 < traffic < 1e9
+    issue = bench.issue_roofline("k_sat_col", workload, 0.03, 1965.0, 148)
+    assert issue and 1e6 < issue["warp_instructions_per_launch"] < 1e9
+    assert abs(issue["peak"] - 4 * 148 * 1.965e9 / 1e12) < 1e-9 and 0 < issue["frac"] < 1.5
+    assert bench.issue_roofline("k_sat_col", "no_such_workload", 0.03, 1965.0, 148) is None
